@@ -1,0 +1,180 @@
+/*
+ * jaccpot_b200 — C ABI of the Blackwell (sm_100a) FMM evaluation pass.
+ *
+ * The reference (jaccpot, Python/JAX) has no native seam: its kernels are JAX
+ * functions called from the engine.  Each entry point below replaces one of
+ * those functions and is what a jax.ffi custom call (or the ctypes host code in
+ * jaccpot_b200/) binds.  Reference paths are relative to the jaccpot project.
+ *
+ * Conventions (all GPU entry points):
+ *   - every array argument is a DEVICE pointer owned by the caller; nothing
+ *     here allocates device memory;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream);
+ *   - calls are asynchronous and stream-ordered; the return value reports only
+ *     argument validation and launch errors (JB_OK = 0);
+ *   - particles are Morton-sorted float4 (x, y, z, mass); node centres are
+ *     float4 (x, y, z, total mass);
+ *   - coefficient rows (multipoles, locals) hold (p+1)^2 floats in the packed
+ *     real (Dehnen, no-sqrt2) layout, degree n at [n^2, n^2+2n+1) with
+ *     m = -n..n (operators/_sh_indexing.py:36-118), padded to a row stride of
+ *     jb_coeff_stride(p) floats;
+ *   - topology arrays are the ones jb_tree_build produces (int32 node ids,
+ *     int64 CSR offsets), see jaccpot_b200/tree.py.
+ */
+#ifndef JACCPOT_B200_H
+#define JACCPOT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JB_API __attribute__((visibility("default")))
+
+enum {
+  JB_OK = 0,
+  JB_ERR_ARG = 1,         /* null pointer, negative size, bad enum */
+  JB_ERR_ORDER = 2,       /* expansion order outside [1, JB_MAX_ORDER] */
+  JB_ERR_CUDA = 3,        /* launch or runtime error (see jb_last_cuda_error) */
+  JB_ERR_INDEX = 4,       /* a list entry is out of range (jb_validate_lists) */
+  JB_ERR_WORKSPACE = 5,   /* caller buffer too small */
+  JB_ERR_ALLOC = 6,       /* host allocation failed (tree build) */
+  JB_ERR_NONFINITE = 7,   /* non-finite input (tree build) */
+  JB_ERR_UNSUPPORTED = 8  /* mode not built for this order */
+};
+
+#define JB_MAX_ORDER 10
+
+/* M2L arithmetic modes (jb_m2l). */
+enum {
+  JB_M2L_FP32 = 0,       /* rotate + scale, FP32 CUDA cores */
+  JB_M2L_SPLIT_BF16 = 1  /* constant factors on tcgen05, BF16 hi/lo 3-product */
+};
+
+/* Near-field accumulation modes (jb_leaf_eval). */
+enum {
+  JB_P2P_FP32 = 0,
+  JB_P2P_KAHAN = 1  /* compensated per-target sums */
+};
+
+/* ------------------------------------------------------------------------ */
+/* Host-side prepare: tree + interaction lists (stand-in for yggdrax).      */
+/* ------------------------------------------------------------------------ */
+typedef struct jb_tree jb_tree;
+
+typedef struct {
+  int64_t num_particles;
+  int32_t num_nodes, num_internal, num_leaves, num_levels;
+  int64_t num_far_pairs, num_near_pairs;
+  int32_t max_leaf_occupancy;
+} jb_tree_info_t;
+
+enum {
+  JB_TREE_PERMUTATION = 0,      /* int64[N]: sorted slot -> input index */
+  JB_TREE_NODE_RANGES = 1,      /* int32[2*num_nodes], inclusive */
+  JB_TREE_LEFT_CHILD = 2,       /* int32[num_internal] */
+  JB_TREE_RIGHT_CHILD = 3,      /* int32[num_internal] */
+  JB_TREE_PARENT = 4,           /* int32[num_nodes], root -1 */
+  JB_TREE_NODE_LEVEL = 5,       /* int32[num_nodes] */
+  JB_TREE_LEVEL_OFFSETS = 6,    /* int32[num_levels+1], internal nodes by depth */
+  JB_TREE_LEAF_OF_PARTICLE = 7, /* int32[N] (sorted slot -> leaf index) */
+  JB_TREE_FAR_OFFSETS = 8,      /* int64[num_nodes+1] */
+  JB_TREE_FAR_SOURCES = 9,      /* int32[num_far_pairs] */
+  JB_TREE_NEAR_OFFSETS = 10,    /* int64[num_leaves+1] */
+  JB_TREE_NEAR_SOURCES = 11,    /* int32[num_near_pairs] (leaf indices) */
+  JB_TREE_CENTERS_F64 = 12,     /* double[3*num_nodes], COM */
+  JB_TREE_RADII_F64 = 13        /* double[num_nodes], bounding radius about COM */
+};
+
+/* Morton sort + radix tree with leaves of <= leaf_size particles + dual
+ * traversal with opening angle theta.  Replaces yggdrax's tree build and
+ * build_well_separated_interactions / neighbour lists as called from
+ * runtime/fmm_prepare.py:823 (_build_tree_with_config) and :1411
+ * (_build_dual_tree_artifacts). Host memory; pos is (n,3), mass (n,). */
+JB_API int jb_tree_build(int64_t n, const double* pos, const double* mass, int leaf_size,
+                         double theta, jb_tree** out);
+JB_API int jb_tree_info(const jb_tree* t, jb_tree_info_t* info);
+JB_API int jb_tree_copy(const jb_tree* t, int field, void* dst);
+JB_API void jb_tree_free(jb_tree* t);
+
+/* ------------------------------------------------------------------------ */
+/* Device pass.                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* Row stride (floats) of a coefficient array of order p: (p+1)^2 rounded up
+ * to a multiple of 4.  Returns 0 for an unsupported order. */
+JB_API int jb_coeff_stride(int p);
+
+/* Last CUDA error string seen by this thread (empty if none). */
+JB_API const char* jb_last_cuda_error(void);
+
+/* Builds sorted float4 particles from the caller's (N,3) positions and (N,)
+ * masses: out[i] = (pos[perm[i]], mass[perm[i]]).  The Morton-order gather
+ * at runtime/fmm_prepare.py (positions_sorted / masses_sorted). */
+JB_API int jb_gather_sorted(int64_t n, const float* pos, const float* mass, const int64_t* perm,
+                            float* out_pos4, void* stream);
+
+/* Checks every list entry against its range on the device (one-off, at
+ * prepare time); writes the number of bad entries to *bad_count_dev (int32).
+ * The hot kernels below trust validated lists. */
+JB_API int jb_validate_lists(int num_nodes, int num_internal, const int* left, const int* right,
+                             const int64_t* far_off, const int* far_src, int64_t num_far,
+                             const int64_t* near_off, const int* near_src, int64_t num_near,
+                             int* bad_count_dev, void* stream);
+
+/* Upward sweep, leaf stage: COM centre (yggdrax compute_tree_mass_moments,
+ * upward/real_tree_expansions.py:439) and P2M (:89-213, p2m_real_direct,
+ * operators/real_p2m_l2p.py:51) for every leaf.  Writes centers[leaf] and
+ * mult[leaf]. */
+JB_API int jb_p2m(int p, const float* pos4, int num_nodes, int num_internal, const int* node_ranges,
+                  float* centers, float* mult, void* stream);
+
+/* Upward sweep, one level: COM of each internal node in [first, last) from
+ * its children and M2M (m2m_real, operators/real_translations.py:531;
+ * aggregate_m2m_real_by_level, upward/real_tree_expansions.py:216-364). */
+JB_API int jb_m2m_level(int p, int first, int last, const int* left, const int* right,
+                        float* centers, float* mult, void* stream);
+
+/* Far field: for each target in `targets` (node ids, any order), sums the
+ * M2L of every source in its CSR list into locals[target] (overwrites).
+ * Replaces _accumulate_m2l_fullbatch/_chunked_scan + m2l_rot_scale_real_batch
+ * (runtime/kernels/_m2l.py:1483-1793, operators/m2l_real_rot_scale.py:392). */
+JB_API int jb_m2l(int p, int mode, int num_targets, const int* targets, const float* mult,
+                  const float* centers, const int64_t* far_off, const int* far_src, float* locals,
+                  void* stream);
+
+/* Downward sweep, one level: for each internal node in [first, last), adds
+ * l2l(parent) to both children (l2l_real, operators/real_translations.py:604;
+ * _propagate_solidfmm_locals_by_level, runtime/kernels/_l2l.py:210-404). */
+JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* right,
+                        const float* centers, float* locals, void* stream);
+
+/* Leaf evaluation: per target leaf, L2P of its local at every particle
+ * (runtime/kernels/_evaluate.py:2106-2484, evaluate_local_real_with_grad)
+ * plus the near field over the self leaf and its CSR neighbour leaves
+ * (nearfield/near_field.py:916, nearfield/_kernels.py:40-338), assembled as
+ * acc = near - G * grad (runtime/kernels/_evaluate.py:1157-1172).
+ * out_acc4[i] = (ax, ay, az, potential) in sorted order. */
+JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_leaves,
+                        const int* node_ranges, const float* centers, const float* locals,
+                        const int64_t* near_off, const int* near_src, float G, float eps2,
+                        float* out_acc4, void* stream);
+
+/* Target subset (runtime/kernels/_evaluate.py:1941-2095): targets_sorted are
+ * sorted-slot indices; out_acc4[q] in target order. */
+JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int* node_ranges,
+                           const float* centers, const float* locals, const int64_t* near_off,
+                           const int* near_src, const int* leaf_of, int64_t num_targets,
+                           const int* targets_sorted, float G, float eps2, float* out_acc4,
+                           void* stream);
+
+/* Un-permute (runtime/fmm_evaluate.py:526-538): out_acc[perm[i]] = acc4[i].xyz,
+ * out_pot (optional) likewise. */
+JB_API int jb_scatter_unsorted(int64_t n, const float* acc4, const int64_t* perm, float* out_acc,
+                               float* out_pot, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JACCPOT_B200_H */

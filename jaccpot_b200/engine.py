@@ -1,0 +1,183 @@
+"""Device-side evaluation pass: uploads a topology once, then runs
+P2M -> M2M (by level) -> M2L -> L2L (by level) -> L2P + P2P on one stream.
+
+This is the B200 replacement for the reference engine's sweep/evaluate seam
+(jaccpot/runtime/fmm_sweeps.py:221 prepare_upward_sweep, :442
+prepare_downward_sweep, runtime/kernels/_evaluate.py:769
+_evaluate_tree_compiled_impl).  Torch provides device memory and streams
+only; every arithmetic step is a kernel of libjaccpot_b200.so.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .tree import Topology
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream_handle(stream: torch.cuda.Stream | None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+class DeviceTopology:
+    """The topology arrays resident in HBM (int32 ids, int64 CSR offsets)."""
+
+    def __init__(self, topo: Topology, device: torch.device | str = "cuda"):
+        dev = torch.device(device)
+        if dev.type != "cuda":
+            raise ValueError("DeviceTopology needs a CUDA device (there is no CPU path)")
+        self.topo = topo
+        self.device = dev
+        up = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)
+        self.node_ranges = up(topo.node_ranges.reshape(-1), torch.int32)
+        self.left = up(topo.left_child if topo.num_internal else np.zeros(1, np.int32), torch.int32)
+        self.right = up(topo.right_child if topo.num_internal else np.zeros(1, np.int32), torch.int32)
+        self.far_off = up(topo.far_offsets, torch.int64)
+        self.far_src = up(topo.far_sources if topo.num_far_pairs else np.zeros(1, np.int32), torch.int32)
+        self.near_off = up(topo.near_offsets, torch.int64)
+        self.near_src = up(topo.near_leaves if topo.num_near_pairs else np.zeros(1, np.int32), torch.int32)
+        self.leaf_of = up(topo.leaf_of_particle, torch.int32)
+        self.perm = up(topo.permutation, torch.int64)
+        self.m2l_targets = up(topo.m2l_targets if topo.m2l_targets.size else np.zeros(1, np.int32), torch.int32)
+        self.num_m2l_targets = int(topo.m2l_targets.size)
+        self.level_offsets = [int(x) for x in topo.level_offsets]
+
+    def validate(self) -> None:
+        """Device-side range check of every list entry (jb_validate_lists)."""
+        t = self.topo
+        bad = torch.zeros(1, dtype=torch.int32, device=self.device)
+        _lib.check(_lib.lib().jb_validate_lists(
+            t.num_nodes, t.num_internal, _ptr(self.left), _ptr(self.right), _ptr(self.far_off),
+            _ptr(self.far_src), t.num_far_pairs, _ptr(self.near_off), _ptr(self.near_src),
+            t.num_near_pairs, _ptr(bad), _stream_handle(None)), "jb_validate_lists")
+        nbad = int(bad.item())
+        if nbad:
+            raise _lib.JBError(f"topology has {nbad} out-of-range list entries")
+
+
+@dataclass
+class Workspace:
+    p: int
+    stride: int
+    pos4: torch.Tensor  # (N, 4) sorted particles
+    centers: torch.Tensor  # (nodes, 4)
+    mult: torch.Tensor  # (nodes, stride)
+    locals: torch.Tensor  # (nodes, stride)
+    acc4: torch.Tensor  # (N, 4)
+
+    @staticmethod
+    def allocate(dt: DeviceTopology, p: int) -> "Workspace":
+        t = dt.topo
+        cs = _lib.coeff_stride(p)
+        kw = dict(device=dt.device, dtype=torch.float32)
+        return Workspace(
+            p=p,
+            stride=cs,
+            pos4=torch.empty((t.num_particles, 4), **kw),
+            centers=torch.empty((t.num_nodes, 4), **kw),
+            mult=torch.empty((t.num_nodes, cs), **kw),
+            locals=torch.empty((t.num_nodes, cs), **kw),
+            acc4=torch.empty((t.num_particles, 4), **kw),
+        )
+
+
+class Pass:
+    """One evaluation pass over a resident topology; every method enqueues
+    kernels on `stream` (default: torch's current stream) and returns."""
+
+    def __init__(self, dt: DeviceTopology, p: int, *, G: float = 1.0, eps2: float = 0.0,
+                 m2l_mode: int = _lib.JB_M2L_FP32, p2p_mode: int = _lib.JB_P2P_FP32):
+        if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
+            raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
+        self.dt = dt
+        self.p = int(p)
+        self.G = float(G)
+        self.eps2 = float(eps2)
+        self.m2l_mode = int(m2l_mode)
+        self.p2p_mode = int(p2p_mode)
+        self.ws = Workspace.allocate(dt, self.p)
+        self.lib = _lib.lib()
+
+    # -- stages -------------------------------------------------------------
+    def load_particles(self, positions: torch.Tensor, masses: torch.Tensor, stream=None) -> None:
+        """Morton-order gather of (N,3) positions and (N,) masses (device)."""
+        n = self.dt.topo.num_particles
+        pos = positions.to(device=self.dt.device, dtype=torch.float32).contiguous()
+        mass = masses.to(device=self.dt.device, dtype=torch.float32).contiguous()
+        if pos.shape != (n, 3) or mass.shape != (n,):
+            raise ValueError("positions must be (N,3) and masses (N,) matching the prepared topology")
+        _lib.check(self.lib.jb_gather_sorted(n, _ptr(pos), _ptr(mass), _ptr(self.dt.perm),
+                                             _ptr(self.ws.pos4), _stream_handle(stream)), "jb_gather_sorted")
+
+    def upward(self, stream=None) -> None:
+        t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)
+        _lib.check(self.lib.jb_p2m(self.p, _ptr(ws.pos4), t.num_nodes, t.num_internal, _ptr(dt.node_ranges),
+                                   _ptr(ws.centers), _ptr(ws.mult), s), "jb_p2m")
+        lo = dt.level_offsets
+        for lev in range(t.num_levels - 1, -1, -1):
+            _lib.check(self.lib.jb_m2m_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
+                                             _ptr(ws.centers), _ptr(ws.mult), s), "jb_m2m_level")
+
+    def m2l(self, stream=None) -> None:
+        dt, ws, s = self.dt, self.ws, _stream_handle(stream)
+        ws.locals.zero_()
+        _lib.check(self.lib.jb_m2l(self.p, self.m2l_mode, dt.num_m2l_targets, _ptr(dt.m2l_targets),
+                                   _ptr(ws.mult), _ptr(ws.centers), _ptr(dt.far_off), _ptr(dt.far_src),
+                                   _ptr(ws.locals), s), "jb_m2l")
+
+    def l2l(self, stream=None) -> None:
+        t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)
+        lo = dt.level_offsets
+        for lev in range(t.num_levels):
+            _lib.check(self.lib.jb_l2l_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
+                                             _ptr(ws.centers), _ptr(ws.locals), s), "jb_l2l_level")
+
+    def evaluate(self, stream=None) -> torch.Tensor:
+        t, dt, ws = self.dt.topo, self.dt, self.ws
+        _lib.check(self.lib.jb_leaf_eval(self.p, self.p2p_mode, _ptr(ws.pos4), t.num_internal, t.num_leaves,
+                                         _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.locals),
+                                         _ptr(dt.near_off), _ptr(dt.near_src), self.G, self.eps2,
+                                         _ptr(ws.acc4), _stream_handle(stream)), "jb_leaf_eval")
+        return ws.acc4
+
+    def evaluate_targets(self, targets_sorted: torch.Tensor, out: torch.Tensor | None = None,
+                         stream=None) -> torch.Tensor:
+        t, dt, ws = self.dt.topo, self.dt, self.ws
+        ts = targets_sorted.to(device=dt.device, dtype=torch.int32).contiguous()
+        nt = int(ts.shape[0])
+        if out is None:
+            out = torch.empty((nt, 4), device=dt.device, dtype=torch.float32)
+        _lib.check(self.lib.jb_eval_targets(self.p, _ptr(ws.pos4), t.num_internal, _ptr(dt.node_ranges),
+                                            _ptr(ws.centers), _ptr(ws.locals), _ptr(dt.near_off),
+                                            _ptr(dt.near_src), _ptr(dt.leaf_of), nt, _ptr(ts), self.G, self.eps2,
+                                            _ptr(out), _stream_handle(stream)), "jb_eval_targets")
+        return out
+
+    def unsort(self, acc: torch.Tensor, pot: torch.Tensor | None, stream=None) -> None:
+        n = self.dt.topo.num_particles
+        _lib.check(self.lib.jb_scatter_unsorted(n, _ptr(self.ws.acc4), _ptr(self.dt.perm), _ptr(acc),
+                                                _ptr(pot), _stream_handle(stream)), "jb_scatter_unsorted")
+
+    def downward(self, stream=None) -> None:
+        self.m2l(stream)
+        self.l2l(stream)
+
+    def run(self, stream=None) -> torch.Tensor:
+        """Whole pass on the particles already in ws.pos4; returns sorted acc4."""
+        self.upward(stream)
+        self.downward(stream)
+        return self.evaluate(stream)
+
+    def launches_per_run(self) -> int:
+        t = self.dt.topo
+        # p2m + m2m levels + zero + m2l + l2l levels + leaf_eval
+        return 1 + t.num_levels + 1 + 1 + t.num_levels + 1

@@ -1,0 +1,172 @@
+"""``FastMultipoleMethod`` facade with the reference's public signature.
+
+Mirrors jaccpot/solver.py:540-1400 (``FastMultipoleMethod.__init__`` :664,
+``compute_accelerations`` :917, ``prepare_state`` :1012,
+``evaluate_prepared_state`` :1292) for the real basis.  ``prepare_state``
+builds the tree and lists on the host (the yggdrax stand-in) and runs the
+upward and downward sweeps on the GPU; ``evaluate_prepared_state`` runs L2P +
+P2P for all particles or for ``target_indices`` -- the same split of work the
+reference makes (runtime/fmm_prepare.py:3742 / runtime/fmm_evaluate.py:325).
+
+Arrays may be numpy or torch; results come back as the same kind (torch
+results stay on the GPU).  Everything runs on CUDA: there is no CPU path.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Any, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import DeviceTopology, Pass
+from .tree import Topology, build_topology
+
+# Preset defaults: (theta, leaf_size hint); solver.py:27-118 + config.py presets.
+_PRESETS = {"fast": 0.6, "balanced": 0.6, "accurate": 0.5, "large_n_gpu": 0.6}
+_M2L_IMPLS = {None: _lib.JB_M2L_FP32, "rot_scale": _lib.JB_M2L_FP32, "fp32": _lib.JB_M2L_FP32,
+              "split_bf16": _lib.JB_M2L_SPLIT_BF16, "tcgen05": _lib.JB_M2L_SPLIT_BF16}
+
+
+@dataclass
+class FMMPreparedState:
+    """What the reference's FMMPreparedState (runtime/fmm_state.py:870-897)
+    carries, resident on the GPU: topology + lists, centres, multipoles and
+    locals, the Morton permutation and the run parameters."""
+
+    topology: Topology
+    device_topology: DeviceTopology
+    pass_: Pass
+    max_order: int
+    theta: float
+    leaf_size: int
+    num_particles: int
+    input_dtype: Any
+
+    @property
+    def inverse_permutation(self) -> np.ndarray:
+        return self.topology.inverse_permutation
+
+    @property
+    def max_leaf_size(self) -> int:
+        return self.topology.max_leaf_occupancy
+
+
+def _to_torch(a, device, dtype) -> torch.Tensor:
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype)
+    return torch.as_tensor(np.asarray(a), dtype=dtype, device=device)
+
+
+class FastMultipoleMethod:
+    """Real-basis FMM on one B200 behind jaccpot's public API."""
+
+    def __init__(
+        self,
+        *,
+        preset: str = "fast",
+        basis: str = "real",
+        m2l_impl: Optional[str] = None,
+        adaptive_order: bool = False,
+        p_gears: Optional[Sequence[int]] = None,
+        use_pallas: Optional[bool] = None,
+        theta: float = 0.6,
+        G: float = 1.0,
+        softening: float = 1e-3,
+        precision: Optional[str] = None,
+        working_dtype: Any = None,
+        nearfield_compensated: bool = False,
+        device: str | torch.device = "cuda",
+        advanced: Any = None,
+        **legacy_kwargs: Any,
+    ):
+        preset = str(getattr(preset, "value", preset)).lower()
+        if preset not in _PRESETS:
+            raise ValueError(f"unknown preset {preset!r}")
+        basis = str(basis).lower()
+        if basis != "real":
+            raise ValueError(f"basis {basis!r} is not provided: this implementation covers the real basis only")
+        if precision not in (None, "fp32"):
+            raise ValueError("only fp32 evaluation is provided on the GPU")
+        if m2l_impl not in _M2L_IMPLS:
+            raise ValueError(f"unknown m2l_impl {m2l_impl!r}")
+        if use_pallas:
+            raise ValueError("use_pallas is not available: the kernels are native sm_100a CUDA")
+        if legacy_kwargs:
+            raise TypeError(f"unexpected keyword arguments: {sorted(legacy_kwargs)}")
+        if not (0.0 < float(theta) < 1.0):
+            raise ValueError("theta must be in (0, 1)")
+        self.preset = preset
+        self.basis = basis
+        self.theta = float(theta)
+        self.G = float(G)
+        self.softening = float(softening)
+        self.m2l_mode = _M2L_IMPLS[m2l_impl]
+        self.p2p_mode = _lib.JB_P2P_KAHAN if nearfield_compensated else _lib.JB_P2P_FP32
+        self.adaptive_order = bool(adaptive_order)
+        self.p_gears = tuple(p_gears) if p_gears is not None else None
+        self.device = torch.device(device)
+        self._last_state: Optional[FMMPreparedState] = None
+
+    # ------------------------------------------------------------------ prepare
+    def prepare_state(self, positions, masses, *, bounds=None, leaf_size: int = 16, max_order: int = 4,
+                      theta: Optional[float] = None, **_ignored) -> FMMPreparedState:
+        th = self.theta if theta is None else float(theta)
+        pos_np = positions.detach().cpu().numpy() if isinstance(positions, torch.Tensor) else np.asarray(positions)
+        mass_np = masses.detach().cpu().numpy() if isinstance(masses, torch.Tensor) else np.asarray(masses)
+        if pos_np.ndim != 2 or pos_np.shape[1] != 3 or mass_np.shape != (pos_np.shape[0],):
+            raise ValueError("positions must be (N, 3) and masses (N,)")
+        topo = build_topology(pos_np, mass_np, leaf_size=int(leaf_size), theta=th)
+        dt = DeviceTopology(topo, self.device)
+        dt.validate()
+        ps = Pass(dt, int(max_order), G=self.G, eps2=self.softening ** 2, m2l_mode=self.m2l_mode,
+                  p2p_mode=self.p2p_mode)
+        ps.load_particles(_to_torch(positions, self.device, torch.float32),
+                          _to_torch(masses, self.device, torch.float32))
+        ps.upward()
+        ps.downward()
+        st = FMMPreparedState(topology=topo, device_topology=dt, pass_=ps, max_order=int(max_order), theta=th,
+                              leaf_size=int(leaf_size), num_particles=int(pos_np.shape[0]),
+                              input_dtype=positions.dtype if hasattr(positions, "dtype") else np.float64)
+        self._last_state = st
+        return st
+
+    # ----------------------------------------------------------------- evaluate
+    def evaluate_prepared_state(self, state: FMMPreparedState, *, target_indices=None,
+                                return_potential: bool = False, jit_traversal=None,
+                                max_acc_derivative_order: int = 0, as_numpy: Optional[bool] = None):
+        if max_acc_derivative_order:
+            raise ValueError("acceleration derivative towers are not provided")
+        ps = state.pass_
+        dev = state.device_topology.device
+        want_np = as_numpy if as_numpy is not None else not isinstance(target_indices, torch.Tensor)
+        if target_indices is None:
+            ps.evaluate()
+            acc = torch.empty((state.num_particles, 3), device=dev, dtype=torch.float32)
+            pot = torch.empty((state.num_particles,), device=dev, dtype=torch.float32) if return_potential else None
+            ps.unsort(acc, pot)
+        else:
+            ti = _to_torch(target_indices, dev, torch.int64).reshape(-1)
+            if ti.numel() and (int(ti.min()) < 0 or int(ti.max()) >= state.num_particles):
+                raise IndexError("target_indices out of range")
+            inv = torch.from_numpy(state.topology.inverse_permutation).to(dev)
+            ts = inv[ti].to(torch.int32)
+            out = ps.evaluate_targets(ts)
+            acc = out[:, :3].contiguous()
+            pot = out[:, 3].contiguous() if return_potential else None
+        if want_np:
+            acc = acc.cpu().numpy()
+            pot = pot.cpu().numpy() if pot is not None else None
+        return (acc, pot) if return_potential else acc
+
+    def compute_accelerations(self, positions, masses, *, target_indices=None, bounds=None, leaf_size: int = 16,
+                              max_order: int = 4, return_potential: bool = False, theta: Optional[float] = None,
+                              reuse_prepared_state: bool = False, max_acc_derivative_order: int = 0):
+        st = self.prepare_state(positions, masses, bounds=bounds, leaf_size=leaf_size, max_order=max_order,
+                                theta=theta)
+        return self.evaluate_prepared_state(
+            st, target_indices=target_indices, return_potential=return_potential,
+            max_acc_derivative_order=max_acc_derivative_order,
+            as_numpy=not isinstance(positions, torch.Tensor))

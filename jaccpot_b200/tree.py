@@ -1,0 +1,131 @@
+"""Host prepare: tree topology and interaction lists (yggdrax stand-in).
+
+``build_topology`` calls ``jb_tree_build`` (csrc/tree_build.cpp) and returns a
+:class:`Topology` of numpy arrays in the layout the reference's kernels read
+from yggdrax artefacts (``Tree.node_ranges/left_child/right_child``,
+``NodeInteractionList``, ``NodeNeighborList``, the Morton permutation), see
+jaccpot/runtime/fmm_state.py:870-897 for the state that carries them.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+
+@dataclass
+class Topology:
+    num_particles: int
+    num_nodes: int
+    num_internal: int
+    num_leaves: int
+    num_levels: int
+    max_leaf_occupancy: int
+    leaf_size: int
+    theta: float
+    permutation: np.ndarray  # int64[N] sorted slot -> input index
+    inverse_permutation: np.ndarray  # int64[N] input index -> sorted slot
+    node_ranges: np.ndarray  # int32[num_nodes, 2] inclusive
+    left_child: np.ndarray  # int32[num_internal]
+    right_child: np.ndarray  # int32[num_internal]
+    parent: np.ndarray  # int32[num_nodes]
+    node_level: np.ndarray  # int32[num_nodes]
+    level_offsets: np.ndarray  # int32[num_levels + 1]
+    leaf_of_particle: np.ndarray  # int32[N]
+    far_offsets: np.ndarray  # int64[num_nodes + 1]
+    far_sources: np.ndarray  # int32[num_far]
+    near_offsets: np.ndarray  # int64[num_leaves + 1]
+    near_leaves: np.ndarray  # int32[num_near]
+    centers_f64: np.ndarray  # float64[num_nodes, 3] (host COM used by the MAC)
+    radii_f64: np.ndarray  # float64[num_nodes]
+    m2l_targets: np.ndarray = field(default=None)  # int32, nodes with >= 1 far pair, longest list first
+
+    @property
+    def num_far_pairs(self) -> int:
+        return int(self.far_sources.shape[0])
+
+    @property
+    def num_near_pairs(self) -> int:
+        return int(self.near_leaves.shape[0])
+
+    def near_pair_interactions(self) -> int:
+        """Particle-particle interactions of the near field (self blocks included)."""
+        cnt = (self.node_ranges[:, 1] - self.node_ranges[:, 0] + 1).astype(np.int64)
+        leaf_cnt = cnt[self.num_internal:]
+        src_cnt = leaf_cnt[self.near_leaves]
+        per_edge_t = np.repeat(leaf_cnt, np.diff(self.near_offsets))
+        return int((per_edge_t * src_cnt).sum() + (leaf_cnt * (leaf_cnt - 1)).sum())
+
+
+def build_topology(positions, masses, *, leaf_size: int = 16, theta: float = 0.6) -> Topology:
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+    mass = np.ascontiguousarray(np.asarray(masses, dtype=np.float64).reshape(-1))
+    n = pos.shape[0]
+    if mass.shape[0] != n:
+        raise ValueError("positions and masses disagree in length")
+    lb = _lib.lib()
+    h = ctypes.c_void_p()
+    _lib.check(lb.jb_tree_build(n, pos.ctypes.data, mass.ctypes.data, int(leaf_size), float(theta),
+                                ctypes.byref(h)), "jb_tree_build")
+    try:
+        info = _lib.TreeInfo()
+        _lib.check(lb.jb_tree_info(h, ctypes.byref(info)), "jb_tree_info")
+        sizes = {
+            "permutation": n,
+            "node_ranges": 2 * info.num_nodes,
+            "left_child": info.num_internal,
+            "right_child": info.num_internal,
+            "parent": info.num_nodes,
+            "node_level": info.num_nodes,
+            "level_offsets": info.num_levels + 1,
+            "leaf_of_particle": n,
+            "far_offsets": info.num_nodes + 1,
+            "far_sources": info.num_far_pairs,
+            "near_offsets": info.num_leaves + 1,
+            "near_leaves": info.num_near_pairs,
+            "centers_f64": 3 * info.num_nodes,
+            "radii_f64": info.num_nodes,
+        }
+        arrs = {}
+        for name, (fid, dt) in _lib.TREE_FIELDS.items():
+            a = np.empty(max(sizes[name], 1), dtype=dt)
+            _lib.check(lb.jb_tree_copy(h, fid, a.ctypes.data), f"jb_tree_copy({name})")
+            arrs[name] = a[: sizes[name]]
+    finally:
+        lb.jb_tree_free(h)
+    perm = arrs["permutation"]
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(n, dtype=np.int64)
+    counts = np.diff(arrs["far_offsets"])
+    tg = np.nonzero(counts)[0]
+    order = np.argsort(-counts[tg], kind="stable")
+    return Topology(
+        num_particles=n,
+        num_nodes=info.num_nodes,
+        num_internal=info.num_internal,
+        num_leaves=info.num_leaves,
+        num_levels=info.num_levels,
+        max_leaf_occupancy=info.max_leaf_occupancy,
+        leaf_size=int(leaf_size),
+        theta=float(theta),
+        permutation=perm,
+        inverse_permutation=inv,
+        node_ranges=arrs["node_ranges"].reshape(-1, 2),
+        left_child=arrs["left_child"],
+        right_child=arrs["right_child"],
+        parent=arrs["parent"],
+        node_level=arrs["node_level"],
+        level_offsets=arrs["level_offsets"],
+        leaf_of_particle=arrs["leaf_of_particle"],
+        far_offsets=arrs["far_offsets"],
+        far_sources=arrs["far_sources"],
+        near_offsets=arrs["near_offsets"],
+        near_leaves=arrs["near_leaves"],
+        centers_f64=arrs["centers_f64"].reshape(-1, 3),
+        radii_f64=arrs["radii_f64"],
+        m2l_targets=tg[order].astype(np.int32),
+    )
