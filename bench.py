@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Benchmark of the FMM evaluation pass on B200 (one JSON line on rank 0).
+
+Workload: 64-clump Plummer mixture, N = 4,194,304, real basis, order p = 8,
+leaf size 32 (the split-precision configuration the headline metric is quoted
+on).  A step is one evaluation pass over the prepared topology: Morton gather
+of the resident inputs, P2M -> M2M -> M2L -> L2L -> L2P + P2P, un-permute into
+input order.  The host tree build / traversal (prepare) is done once, outside
+the timed region, as in the reference's prepare_state / evaluate split.
+
+`value` is particles/s of the timed form with inputs resident in HBM; `e2e`
+is the same metric through the public API (FastMultipoleMethod.
+differentiable_accelerations on the prepared state) from pinned host buffers,
+H2D + pass + D2H inside the timed region.  L2 is flushed (256 MiB write)
+between timed steps; each step is timed with CUDA events on its stream.
+
+`--impl reference` times the CPU restatement of the same pass (the reference
+itself is JAX, which is not installed) on the host cores.
+
+With torchrun (N > 1 ranks) the target leaves are split into N Morton ranges;
+every rank runs the (cheap, replicated) upward sweep and evaluates its own
+range: no data-path collective.  Timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particles/s for accelerations at N=4M, rel err ≤1e-4: chosen vs plain, 1 B200"
+WORKLOAD = {
+    "workload": "clustered 64-clump Plummer mixture, N=4194304, real basis p=8, leaf 32",
+    "generator": "clustered",
+    "N": 4194304,
+    "order": 8,
+    "leaf_size": 32,
+    "theta": 0.6,
+    "seed": 0,
+}
+ERR_TARGETS = 4096
+ERR_BOUND = 1e-4
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows: list[list[str]] = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "bf16_tflops": d.get("bf16_tflops", 1590.0),
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained", 1400.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+def _traffic(kernel: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get(kernel)
+    return None
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args) -> None:
+    """CPU restatement of the pass (oracle port), all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    from jaccpot_b200 import tree, workloads
+
+    oracle.build()
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    n = args.cpu_sample
+    pos, mass = workloads.GENERATORS[WORKLOAD["generator"]](n, WORKLOAD["seed"])
+    topo = tree.build_topology(pos, mass, leaf_size=WORKLOAD["leaf_size"], theta=WORKLOAD["theta"])
+    ps, ms = pos[topo.permutation], mass[topo.permutation]
+    P = oracle.Pass(topo, np.float32)
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        P.run(WORKLOAD["order"], ps, ms, G=1.0, eps2=0.0)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+    ms_step = 1e3 * statistics.mean(times)
+    val = n / (ms_step / 1e3)
+    sample = f"clustered N={n} (same generator, p=8, leaf 32, theta {WORKLOAD['theta']}), float32 pass, one pass per step"
+    cfg = dict(WORKLOAD)
+    cfg["cpu_sample_N"] = n
+    print(json.dumps({
+        "metric": METRIC, "value": val, "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference", "config": cfg,
+        "cpu_baseline": {"value": val, "unit": "particles/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=WORKLOAD["N"], help="particle count (default: the headline 4M)")
+    ap.add_argument("--cpu-sample", type=int, default=1048576, help="CPU baseline sample size")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from jaccpot_b200 import _lib, engine, tree, workloads
+    from jaccpot_b200.solver import FastMultipoleMethod
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    n = args.n
+    cfg = dict(WORKLOAD)
+    cfg["N"] = n
+    pos, mass = workloads.GENERATORS[cfg["generator"]](n, cfg["seed"])
+    fmm = FastMultipoleMethod(theta=cfg["theta"], G=1.0, softening=0.0, device=dev)
+    t0 = time.perf_counter()
+    state = fmm.prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
+    torch.cuda.synchronize()
+    prep_s = time.perf_counter() - t0
+    topo = state.topology
+    dt = state.device_topology
+
+    # leaf range of this rank (Morton order); ranks > 1 evaluate a slice
+    L = topo.num_leaves
+    leaf_lo, leaf_hi = (L * rank) // world, (L * (rank + 1)) // world
+
+    forms = {
+        "plain": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_FP32),
+        "chosen": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_KAHAN),
+    }
+    passes = {k: engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, leaf_range=(leaf_lo, leaf_hi), **v)
+              for k, v in forms.items()}
+    d_pos = torch.from_numpy(pos).to(dev)
+    d_mass = torch.from_numpy(mass).to(dev)
+    acc_out = torch.empty((n, 3), device=dev, dtype=torch.float32)
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
+    stream = torch.cuda.current_stream()
+
+    def step(ps: engine.Pass, ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        ps.load_particles(d_pos, d_mass)
+        ps.upward()
+        if ev is not None:
+            ev[1].record(stream)
+        ps.m2l()
+        if ev is not None:
+            ev[2].record(stream)
+        ps.l2l()
+        if ev is not None:
+            ev[3].record(stream)
+        ps.evaluate()
+        if ev is not None:
+            ev[4].record(stream)
+        ps.unsort(acc_out, None)
+        if ev is not None:
+            ev[5].record(stream)
+
+    def timed(ps: engine.Pass, steps: int, sampler=None):
+        per_step, stage = [], np.zeros(5)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(steps):
+            flush.fill_(1.0)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+            step(ps, ev)
+            torch.cuda.synchronize()
+            per_step.append(ev[0].elapsed_time(ev[5]))
+            stage += [ev[i].elapsed_time(ev[i + 1]) for i in range(5)]
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return float(np.mean(per_step)), stage / steps
+
+    results = {}
+    for name, ps in passes.items():
+        for _ in range(args.warmup):
+            step(ps)
+        torch.cuda.synchronize()
+    # plain, then chosen (clocks sampled over the chosen form's timed region)
+    ms_plain, stage_plain = timed(passes["plain"], args.steps)
+    with ClockSampler(local) as cs:
+        ms_chosen, stage_chosen = timed(passes["chosen"], args.steps)
+    clocks = cs.summary()
+
+    def reduce_max(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_plain = reduce_max(ms_plain)
+    ms_chosen = reduce_max(ms_chosen)
+
+    # accuracy of both forms against an FP64 direct sum on sampled targets
+    rng = np.random.default_rng(12345)
+    tg = rng.choice(n, size=min(ERR_TARGETS, n), replace=False)
+    ts = torch.from_numpy(topo.inverse_permutation[tg].astype(np.int32)).to(dev)
+    ref = torch.empty((tg.size, 4), device=dev, dtype=torch.float64)
+    ps0 = passes["chosen"]
+    _lib.check(_lib.lib().jb_direct_f64(n, ps0.ws.pos4.data_ptr(), tg.size, ts.data_ptr(), 1.0, 0.0,
+                                        ref.data_ptr(), stream.cuda_stream), "jb_direct_f64")
+    errs = {}
+    for name, ps in passes.items():
+        step(ps)
+        torch.cuda.synchronize()
+        got = acc_out[torch.from_numpy(tg).to(dev)].double().cpu().numpy()
+        e = workloads.relative_errors(got, ref[:, :3].cpu().numpy())
+        errs[name] = {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+
+    # e2e through the public API from pinned host buffers
+    h_pos = torch.from_numpy(pos).pin_memory()
+    h_mass = torch.from_numpy(mass).pin_memory()
+    h_out = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    state.pass_ = passes["chosen"]
+    for _ in range(args.warmup):
+        fmm.differentiable_accelerations(state, h_pos, h_mass, out=h_out)
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fmm.differentiable_accelerations(state, h_pos, h_mass, out=h_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e = reduce_max(float(np.mean(e2e_ms)))
+
+    # roofline of the dominant kernel (largest stage time of the chosen form)
+    peaks = _peaks()
+    near_inter = topo.near_pair_interactions()
+    p2p_flops = 20.0 * near_inter
+    m2l_flops = {4: 718.0, 6: 1964.0, 8: 4166.0}.get(cfg["order"], 4166.0) * topo.num_far_pairs
+    # measured FP32 FMA peak (in-run probe, 148 SMs x 8 blocks x 256 thr)
+    sink = torch.empty(256, device=dev)
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = 4096
+    _lib.lib().jb_probe_throughput(148 * 8, 64, 0, sink.data_ptr(), stream.cuda_stream)
+    pe0.record(stream)
+    _lib.lib().jb_probe_throughput(148 * 8, iters, 0, sink.data_ptr(), stream.cuda_stream)
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    fp32_peak = 2.0 * 148 * 8 * 256 * iters * 8 / (pe0.elapsed_time(pe1) / 1e3) / 1e12
+    stage_names = ["upward", "m2l", "l2l", "leaf_eval", "unsort"]
+    dom = int(np.argmax(stage_chosen))
+    if stage_names[dom] == "m2l":
+        ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
+        roof = {"kernel": "k_m2l_fp32<8>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_m2l_fp32")}
+    else:
+        ach = p2p_flops / (stage_chosen[3] / 1e3) / 1e12
+        roof = {"kernel": "k_leaf_eval<8,kahan>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_leaf_eval")}
+    roof["peak_source"] = "in-run FP32 FMA probe (MEASURED_PEAKS.json has HBM and bf16 only)"
+    roof["algorithmic"] = "P2P 20 flop/pair x near pairs; M2L 2*(2*sum(2l+1)^2 + z-terms) flop/pair"
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+        oracle.build()
+        thr = oracle.set_threads(os.cpu_count() or 1)
+        ns = args.cpu_sample
+        cpos, cmass = workloads.GENERATORS[cfg["generator"]](ns, cfg["seed"])
+        ctopo = tree.build_topology(cpos, cmass, leaf_size=cfg["leaf_size"], theta=cfg["theta"])
+        P = oracle.Pass(ctopo, np.float32)
+        t0 = time.perf_counter()
+        P.run(cfg["order"], cpos[ctopo.permutation], cmass[ctopo.permutation])
+        cdt = time.perf_counter() - t0
+        cpu = {"value": ns / cdt, "unit": "particles/s", "cores": thr, "kind": "port",
+               "sample": f"one float32 pass of the oracle on clustered N={ns} (same generator/order/leaf/theta)"}
+
+    launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
+    if rank == 0:
+        cfg.update({
+            "form": "chosen = FP32 rotate+scale M2L + Kahan-compensated P2P; plain = FP32 M2L + FP32 P2P",
+            "plain_particles_per_s": n / (ms_plain / 1e3),
+            "plain_ms_per_step": ms_plain,
+            "stage_ms_chosen": dict(zip(stage_names, [float(x) for x in stage_chosen])),
+            "stage_ms_plain": dict(zip(stage_names, [float(x) for x in stage_plain])),
+            "err_vs_fp64_direct": errs,
+            "err_targets": int(tg.size),
+            "err_bound_met": bool(errs["chosen"]["p99"] <= ERR_BOUND),
+            "prepare_s": prep_s,
+            "num_nodes": topo.num_nodes,
+            "far_pairs": topo.num_far_pairs,
+            "near_leaf_pairs": topo.num_near_pairs,
+            "near_interactions": near_inter,
+            "l2": "flushed (256 MiB write) between timed steps",
+            "parallelism": f"target-leaf ranges over {world} rank(s)",
+            "timing": "CUDA events per step on the launching stream; max over ranks",
+        })
+        line = {
+            "metric": METRIC, "value": n / (ms_chosen / 1e3), "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_chosen, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": n / (e2e / 1e3), "unit": "particles/s", "h2d_bytes_per_step": n * 16,
+                    "d2h_bytes_per_step": n * 12, "ms_per_step": e2e},
+            "gpu_launches": launches * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -155,8 +155,9 @@ JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* 
  * plus the near field over the self leaf and its CSR neighbour leaves
  * (nearfield/near_field.py:916, nearfield/_kernels.py:40-338), assembled as
  * acc = near - G * grad (runtime/kernels/_evaluate.py:1157-1172).
- * out_acc4[i] = (ax, ay, az, potential) in sorted order. */
-JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_leaves,
+ * Evaluates leaves [leaf_first, leaf_last) (leaf indices, node id minus
+ * num_internal); out_acc4[i] = (ax, ay, az, potential) in sorted order. */
+JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int leaf_first, int leaf_last,
                         const int* node_ranges, const float* centers, const float* locals,
                         const int64_t* near_off, const int* near_src, float G, float eps2,
                         float* out_acc4, void* stream);
@@ -173,6 +174,22 @@ JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int
  * out_pot (optional) likewise. */
 JB_API int jb_scatter_unsorted(int64_t n, const float* acc4, const int64_t* perm, float* out_acc,
                                float* out_pot, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Verification and measurement helpers (no reference counterpart in the    */
+/* hot path; they back the error report and the roofline denominators).    */
+/* ------------------------------------------------------------------------ */
+
+/* FP64 direct sum on sampled targets over all n sorted particles, self pair
+ * excluded: runtime/reference.py:292 (direct_sum) and
+ * bench/validation/mac_error_distribution.py:140-186 (targets subset).
+ * out4[4q..4q+3] = (ax, ay, az, potential) in float64. */
+JB_API int jb_direct_f64(int64_t n, const float* pos4, int64_t num_targets, const int* targets_sorted, double G,
+                         double eps2, double* out4, void* stream);
+
+/* Pipe-throughput probe: blocks x 256 threads x iters x 8 dependent-chain
+ * FMAs (use_mufu = 0) or rsqrt (use_mufu = 1).  Time it with events. */
+JB_API int jb_probe_throughput(int blocks, int iters, int use_mufu, float* sink, void* stream);
 
 #ifdef __cplusplus
 }

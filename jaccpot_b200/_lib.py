@@ -85,9 +85,11 @@ _SIGNATURES = {
     "jb_m2m_level": [_I, _I, _I, _P, _P, _P, _P, _P],
     "jb_m2l": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P],
     "jb_l2l_level": [_I, _I, _I, _P, _P, _P, _P, _P],
-    "jb_leaf_eval": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _F, _F, _P, _P],
+    "jb_leaf_eval": [_I, _I, _P, _I, _I, _I, _P, _P, _P, _P, _P, _F, _F, _P, _P],
     "jb_eval_targets": [_I, _P, _I, _P, _P, _P, _P, _P, _P, _I64, _P, _F, _F, _P, _P],
     "jb_scatter_unsorted": [_I64, _P, _P, _P, _P, _P],
+    "jb_direct_f64": [_I64, _P, _I64, _P, _D, _D, _P, _P],
+    "jb_probe_throughput": [_I, _I, _I, _P, _P],
 }
 
 EXPORTED = tuple(_SIGNATURES)

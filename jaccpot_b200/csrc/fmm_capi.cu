@@ -83,6 +83,74 @@ static int dispatch(int p, A... args) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Verification: FP64 direct sum on sampled targets (the error report every
+// result carries; runtime/reference.py:292 semantics, self pair excluded).
+// Block per target, threads stride over all sources, FP64 tree reduction.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_direct_f64(int64_t n, const float4* __restrict__ pos4, int64_t nt,
+                                                    const int* __restrict__ tsorted, double G, double eps2,
+                                                    double* __restrict__ out) {
+  __shared__ double red[4][256];
+  const int64_t q = blockIdx.x;
+  if (q >= nt) return;
+  const int i = tsorted[q];
+  const float4 ti = pos4[i];
+  const double xi = ti.x, yi = ti.y, zi = ti.z;
+  double ax = 0, ay = 0, az = 0, ph = 0;
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+    if (j == i) continue;
+    const float4 s = pos4[j];
+    const double dx = xi - s.x, dy = yi - s.y, dz = zi - s.z;
+    const double d2 = dx * dx + dy * dy + dz * dz + eps2;
+    const double ir = 1.0 / sqrt(d2);
+    const double w = (double)s.w * ir * ir * ir;
+    ax += w * dx;
+    ay += w * dy;
+    az += w * dz;
+    ph += (double)s.w * ir;
+  }
+  red[0][threadIdx.x] = ax;
+  red[1][threadIdx.x] = ay;
+  red[2][threadIdx.x] = az;
+  red[3][threadIdx.x] = ph;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[4 * q + 0] = -G * red[0][0];
+    out[4 * q + 1] = -G * red[1][0];
+    out[4 * q + 2] = -G * red[2][0];
+    out[4 * q + 3] = -G * red[3][0];
+  }
+}
+
+// Throughput probe: FP32 FMA chains (8 independent per thread) or MUFU rsqrt.
+__global__ void k_probe(int iters, int use_mufu, float* out) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = 1.0f + 1e-3f * (threadIdx.x + k);
+  const float b = 0.999f, c = 1e-4f;
+  if (use_mufu) {
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = rsqrtf(a[k] + c);
+    }
+  } else {
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], b, c);
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the chains live
+}
+
 static inline unsigned blocks_1d(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
 }  // namespace jb
@@ -131,6 +199,21 @@ JB_API int jb_validate_lists(int num_nodes, int num_internal, const int* left, c
   return launch_status();
 }
 
+JB_API int jb_direct_f64(int64_t n, const float* pos4, int64_t num_targets, const int* targets_sorted, double G,
+                         double eps2, double* out4, void* stream) {
+  if (n < 1 || num_targets < 0 || (num_targets > 0 && (!pos4 || !targets_sorted || !out4))) return JB_ERR_ARG;
+  if (num_targets == 0) return JB_OK;
+  k_direct_f64<<<(unsigned)num_targets, 256, 0, ST(stream)>>>(n, reinterpret_cast<const float4*>(pos4), num_targets,
+                                                              targets_sorted, G, eps2, out4);
+  return launch_status();
+}
+
+JB_API int jb_probe_throughput(int blocks, int iters, int use_mufu, float* sink, void* stream) {
+  if (blocks < 1 || iters < 1 || !sink) return JB_ERR_ARG;
+  k_probe<<<blocks, 256, 0, ST(stream)>>>(iters, use_mufu, sink);
+  return launch_status();
+}
+
 JB_API int jb_p2m(int p, const float* pos4, int num_nodes, int num_internal, const int* node_ranges, float* centers,
                   float* mult, void* stream) {
   if (!pos4 || !node_ranges || !centers || !mult || num_nodes < 1 || num_internal < 0) return JB_ERR_ARG;
@@ -156,14 +239,15 @@ JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* 
   return dispatch<RunL2L>(p, first, last, left, right, centers, locals, ST(stream));
 }
 
-JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_leaves,
+JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int leaf_first, int leaf_last,
                         const int* node_ranges, const float* centers, const float* locals, const int64_t* near_off,
                         const int* near_src, float G, float eps2, float* out_acc4, void* stream) {
-  if (!pos4 || !node_ranges || !centers || !locals || !near_off || !out_acc4 || num_leaves < 0 || num_internal < 0)
+  if (!pos4 || !node_ranges || !centers || !locals || !near_off || !out_acc4 || leaf_first < 0 ||
+      leaf_last < leaf_first || num_internal < 0)
     return JB_ERR_ARG;
   if (p2p_mode != JB_P2P_FP32 && p2p_mode != JB_P2P_KAHAN) return JB_ERR_ARG;
-  return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, num_leaves, node_ranges, centers, locals, near_off,
-                               near_src, G, eps2, out_acc4, ST(stream));
+  return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, leaf_first, leaf_last, node_ranges, centers, locals,
+                               near_off, near_src, G, eps2, out_acc4, ST(stream));
 }
 
 JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int* node_ranges, const float* centers,

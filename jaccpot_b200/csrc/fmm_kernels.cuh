@@ -277,7 +277,8 @@ __device__ __forceinline__ void p2p_block(const float4* __restrict__ spos, int n
 
 template <int P, bool KAHAN>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_eval(const float4* __restrict__ pos4, int num_internal,
-                                                                   int num_leaves, const int2* __restrict__ ranges,
+                                                                   int leaf_first, int leaf_last,
+                                                                   const int2* __restrict__ ranges,
                                                                    const float4* __restrict__ centers,
                                                                    const float* __restrict__ locals,
                                                                    const int64_t* __restrict__ near_off,
@@ -287,8 +288,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_eval(const float4*
   __shared__ float sF[kWarpsPerBlock][CS];
   __shared__ float4 sP[kWarpsPerBlock][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int leaf = blockIdx.x * kWarpsPerBlock + warp;
-  if (leaf >= num_leaves) return;
+  const int leaf = leaf_first + blockIdx.x * kWarpsPerBlock + warp;
+  if (leaf >= leaf_last) return;
   const int node = num_internal + leaf;
   const int2 rg = ranges[node];
   const float4 c = centers[node];
@@ -437,18 +438,18 @@ struct RunL2L {
 
 template <int P>
 struct RunLeafEval {
-  static int run(int mode, const float* pos4, int num_internal, int num_leaves, const int* ranges, const float* centers,
-                 const float* locals, const int64_t* near_off, const int* near_src, float G, float eps2, float* out,
-                 cudaStream_t st) {
-    if (num_leaves <= 0) return JB_OK;
-    const unsigned nb = blocks_for(num_leaves, kWarpsPerBlock);
+  static int run(int mode, const float* pos4, int num_internal, int leaf_first, int leaf_last, const int* ranges,
+                 const float* centers, const float* locals, const int64_t* near_off, const int* near_src, float G,
+                 float eps2, float* out, cudaStream_t st) {
+    if (leaf_last <= leaf_first) return JB_OK;
+    const unsigned nb = blocks_for(leaf_last - leaf_first, kWarpsPerBlock);
     if (mode == JB_P2P_KAHAN) {
       k_leaf_eval<P, true><<<nb, 32 * kWarpsPerBlock, 0, st>>>(
-          reinterpret_cast<const float4*>(pos4), num_internal, num_leaves, reinterpret_cast<const int2*>(ranges),
+          reinterpret_cast<const float4*>(pos4), num_internal, leaf_first, leaf_last, reinterpret_cast<const int2*>(ranges),
           reinterpret_cast<const float4*>(centers), locals, near_off, near_src, G, eps2, reinterpret_cast<float4*>(out));
     } else {
       k_leaf_eval<P, false><<<nb, 32 * kWarpsPerBlock, 0, st>>>(
-          reinterpret_cast<const float4*>(pos4), num_internal, num_leaves, reinterpret_cast<const int2*>(ranges),
+          reinterpret_cast<const float4*>(pos4), num_internal, leaf_first, leaf_last, reinterpret_cast<const int2*>(ranges),
           reinterpret_cast<const float4*>(centers), locals, near_off, near_src, G, eps2, reinterpret_cast<float4*>(out));
     }
     return launch_status();

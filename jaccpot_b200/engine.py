@@ -95,7 +95,8 @@ class Pass:
     kernels on `stream` (default: torch's current stream) and returns."""
 
     def __init__(self, dt: DeviceTopology, p: int, *, G: float = 1.0, eps2: float = 0.0,
-                 m2l_mode: int = _lib.JB_M2L_FP32, p2p_mode: int = _lib.JB_P2P_FP32):
+                 m2l_mode: int = _lib.JB_M2L_FP32, p2p_mode: int = _lib.JB_P2P_FP32,
+                 leaf_range: tuple[int, int] | None = None):
         if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
             raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
         self.dt = dt
@@ -106,6 +107,19 @@ class Pass:
         self.p2p_mode = int(p2p_mode)
         self.ws = Workspace.allocate(dt, self.p)
         self.lib = _lib.lib()
+        t = dt.topo
+        self.leaf_range = (0, t.num_leaves) if leaf_range is None else (int(leaf_range[0]), int(leaf_range[1]))
+        if self.leaf_range == (0, t.num_leaves):
+            self.m2l_targets, self.num_m2l_targets = dt.m2l_targets, dt.num_m2l_targets
+        else:
+            # only nodes whose particle span meets this leaf range need locals
+            lo = int(t.node_ranges[t.num_internal + self.leaf_range[0], 0])
+            hi = int(t.node_ranges[t.num_internal + self.leaf_range[1] - 1, 1])
+            tg = t.m2l_targets
+            keep = (t.node_ranges[tg, 1] >= lo) & (t.node_ranges[tg, 0] <= hi)
+            sel = np.ascontiguousarray(tg[keep])
+            self.num_m2l_targets = int(sel.size)
+            self.m2l_targets = torch.from_numpy(sel if sel.size else np.zeros(1, np.int32)).to(dt.device)
 
     # -- stages -------------------------------------------------------------
     def load_particles(self, positions: torch.Tensor, masses: torch.Tensor, stream=None) -> None:
@@ -130,7 +144,7 @@ class Pass:
     def m2l(self, stream=None) -> None:
         dt, ws, s = self.dt, self.ws, _stream_handle(stream)
         ws.locals.zero_()
-        _lib.check(self.lib.jb_m2l(self.p, self.m2l_mode, dt.num_m2l_targets, _ptr(dt.m2l_targets),
+        _lib.check(self.lib.jb_m2l(self.p, self.m2l_mode, self.num_m2l_targets, _ptr(self.m2l_targets),
                                    _ptr(ws.mult), _ptr(ws.centers), _ptr(dt.far_off), _ptr(dt.far_src),
                                    _ptr(ws.locals), s), "jb_m2l")
 
@@ -143,7 +157,8 @@ class Pass:
 
     def evaluate(self, stream=None) -> torch.Tensor:
         t, dt, ws = self.dt.topo, self.dt, self.ws
-        _lib.check(self.lib.jb_leaf_eval(self.p, self.p2p_mode, _ptr(ws.pos4), t.num_internal, t.num_leaves,
+        _lib.check(self.lib.jb_leaf_eval(self.p, self.p2p_mode, _ptr(ws.pos4), t.num_internal,
+                                         self.leaf_range[0], self.leaf_range[1],
                                          _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.locals),
                                          _ptr(dt.near_off), _ptr(dt.near_src), self.G, self.eps2,
                                          _ptr(ws.acc4), _stream_handle(stream)), "jb_leaf_eval")

@@ -44,6 +44,11 @@ class FMMPreparedState:
     leaf_size: int
     num_particles: int
     input_dtype: Any
+    scratch: dict = None
+
+    def __post_init__(self):
+        if self.scratch is None:
+            self.scratch = {}
 
     @property
     def inverse_permutation(self) -> np.ndarray:
@@ -160,6 +165,41 @@ class FastMultipoleMethod:
             acc = acc.cpu().numpy()
             pot = pot.cpu().numpy() if pot is not None else None
         return (acc, pot) if return_potential else acc
+
+    def differentiable_accelerations(self, state: FMMPreparedState, positions, masses, *, target_indices=None,
+                                     jit_traversal: bool = False, grad_plan=None, grad_config=None, out=None):
+        """Re-evaluates the whole pass (P2M -> M2M -> M2L -> L2L -> L2P + P2P) on
+        live positions/masses with the topology of `state` held fixed
+        (runtime/fmm_evaluate.py:733, :542-731).  Host inputs are copied to the
+        device and the result copied back (into `out` when given, which may be
+        a pinned host tensor); device inputs give a device result."""
+        if target_indices is not None:
+            raise ValueError("target_indices is not provided on the fixed-topology path")
+        ps = state.pass_
+        dev = state.device_topology.device
+        host = not (isinstance(positions, torch.Tensor) and positions.is_cuda)
+        pos = _to_torch(positions, dev, torch.float32) if not isinstance(positions, torch.Tensor) else positions
+        mass = _to_torch(masses, dev, torch.float32) if not isinstance(masses, torch.Tensor) else masses
+        if host:
+            if state.scratch.get("pos") is None:
+                state.scratch["pos"] = torch.empty((state.num_particles, 3), device=dev, dtype=torch.float32)
+                state.scratch["mass"] = torch.empty((state.num_particles,), device=dev, dtype=torch.float32)
+                state.scratch["acc"] = torch.empty((state.num_particles, 3), device=dev, dtype=torch.float32)
+            state.scratch["pos"].copy_(pos, non_blocking=True)
+            state.scratch["mass"].copy_(mass, non_blocking=True)
+            pos, mass = state.scratch["pos"], state.scratch["mass"]
+            acc = state.scratch["acc"]
+        else:
+            acc = torch.empty((state.num_particles, 3), device=dev, dtype=torch.float32)
+        ps.load_particles(pos, mass)
+        ps.run()
+        ps.unsort(acc, None)
+        if not host:
+            return acc
+        if out is None:
+            return acc.cpu()
+        out.copy_(acc, non_blocking=True)
+        return out
 
     def compute_accelerations(self, positions, masses, *, target_indices=None, bounds=None, leaf_size: int = 16,
                               max_order: int = 4, return_potential: bool = False, theta: Optional[float] = None,
