@@ -52,10 +52,11 @@ enum {
   JB_M2L_SPLIT_BF16 = 1  /* constant factors on tcgen05, BF16 hi/lo 3-product */
 };
 
-/* Near-field accumulation modes (jb_leaf_eval). */
+/* Near-field accumulation flags (jb_leaf_eval), OR-able. */
 enum {
   JB_P2P_FP32 = 0,
-  JB_P2P_KAHAN = 1  /* compensated per-target sums */
+  JB_P2P_KAHAN = 1,     /* compensated per-target sums */
+  JB_P2P_POTENTIAL = 2  /* also accumulate the potential (else out.w holds only the far part) */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -136,12 +137,19 @@ JB_API int jb_p2m(int p, const float* pos4, int num_nodes, int num_internal, con
 JB_API int jb_m2m_level(int p, int first, int last, const int* left, const int* right,
                         float* centers, float* mult, void* stream);
 
-/* Far field: for each target in `targets` (node ids, any order), sums the
- * M2L of every source in its CSR list into locals[target] (overwrites).
- * Replaces _accumulate_m2l_fullbatch/_chunked_scan + m2l_rot_scale_real_batch
- * (runtime/kernels/_m2l.py:1483-1793, operators/m2l_real_rot_scale.py:392). */
-JB_API int jb_m2l(int p, int mode, int num_targets, const int* targets, const float* mult,
-                  const float* centers, const int64_t* far_off, const int* far_src, float* locals,
+/* Far field (M2L + accumulation) over work units.  units is int4[num_units]:
+ * (target node, first pair, end pair, slot) with pairs indexing far_src (the
+ * CSR source list of the target); a unit covers at most a bounded number of
+ * consecutive pairs.  slot < 0: the unit covers the target's whole list and
+ * writes locals[target]; slot >= 0: it writes row `slot` of `partials`
+ * (num_slots x jb_coeff_stride(p) floats, caller-provided scratch), and the
+ * split list int4[num_split] = (target, first slot, slot count, 0) is then
+ * summed into locals in slot order.  Rows of targets without pairs are not
+ * written (zero them first).  Replaces _accumulate_m2l_fullbatch/_chunked_scan
+ * + m2l_rot_scale_real_batch (runtime/kernels/_m2l.py:1483-1793,
+ * operators/m2l_real_rot_scale.py:392-486). */
+JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float* mult, const float* centers,
+                  const int* far_src, float* locals, float* partials, int num_split, const int* split,
                   void* stream);
 
 /* Downward sweep, one level: for each internal node in [first, last), adds
@@ -150,17 +158,24 @@ JB_API int jb_m2l(int p, int mode, int num_targets, const int* targets, const fl
 JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* right,
                         const float* centers, float* locals, void* stream);
 
-/* Leaf evaluation: per target leaf, L2P of its local at every particle
- * (runtime/kernels/_evaluate.py:2106-2484, evaluate_local_real_with_grad)
- * plus the near field over the self leaf and its CSR neighbour leaves
+/* Leaf evaluation over work units: L2P of each leaf's local at its particles
+ * (runtime/kernels/_evaluate.py:2106-2484, evaluate_local_real_with_grad) plus
+ * the near field over the self leaf and the leaf's neighbour list
  * (nearfield/near_field.py:916, nearfield/_kernels.py:40-338), assembled as
  * acc = near - G * grad (runtime/kernels/_evaluate.py:1157-1172).
- * Evaluates leaves [leaf_first, leaf_last) (leaf indices, node id minus
- * num_internal); out_acc4[i] = (ax, ay, az, potential) in sorted order. */
-JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int leaf_first, int leaf_last,
-                        const int* node_ranges, const float* centers, const float* locals,
-                        const int64_t* near_off, const int* near_src, float G, float eps2,
-                        float* out_acc4, void* stream);
+ *   units int4[num_units] = (leaf index, first run, end run, source count)
+ *   aux   int2[num_units] = (slot, flags); flags & 1: this unit also does the
+ *                           self block and the far field of the leaf
+ *   runs  int2[...]       = (first sorted particle, count): contiguous source
+ *                           ranges (runs of consecutive neighbour leaves)
+ * slot < 0: writes out_acc4 for the leaf's particles; slot >= 0: writes 32
+ * float4 at partials[32*slot] (scratch), then split int4[num_split] = (leaf,
+ * first slot, slot count, 0) is summed into out_acc4.  out_acc4[i] = (ax, ay,
+ * az, potential) in sorted order; p2p_mode is a JB_P2P_* flag set. */
+JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_units, const int* units,
+                        const int* aux, const int* runs, const int* node_ranges, const float* centers,
+                        const float* locals, float G, float eps2, float* out_acc4, float* partials, int num_split,
+                        const int* split, void* stream);
 
 /* Target subset (runtime/kernels/_evaluate.py:1941-2095): targets_sorted are
  * sorted-slot indices; out_acc4[q] in target order. */

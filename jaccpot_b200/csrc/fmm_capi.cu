@@ -226,11 +226,16 @@ JB_API int jb_m2m_level(int p, int first, int last, const int* left, const int* 
   return dispatch<RunM2M>(p, first, last, left, right, centers, mult, ST(stream));
 }
 
-JB_API int jb_m2l(int p, int mode, int num_targets, const int* targets, const float* mult, const float* centers,
-                  const int64_t* far_off, const int* far_src, float* locals, void* stream) {
-  if (num_targets < 0 || (num_targets > 0 && (!targets || !mult || !centers || !far_off || !locals))) return JB_ERR_ARG;
+JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float* mult, const float* centers,
+                  const int* far_src, float* locals, float* partials, int num_split, const int* split,
+                  void* stream) {
+  if (num_units < 0 || num_split < 0 ||
+      (num_units > 0 && (!units || !mult || !centers || !far_src || !locals)) ||
+      (num_split > 0 && (!split || !partials || !locals)))
+    return JB_ERR_ARG;
   if (mode != JB_M2L_FP32) return JB_ERR_UNSUPPORTED;
-  return dispatch<RunM2L>(p, num_targets, targets, mult, centers, far_off, far_src, locals, ST(stream));
+  return dispatch<RunM2L>(p, num_units, units, mult, centers, far_src, locals, partials, num_split, split,
+                          ST(stream));
 }
 
 JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* right, const float* centers,
@@ -239,15 +244,17 @@ JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* 
   return dispatch<RunL2L>(p, first, last, left, right, centers, locals, ST(stream));
 }
 
-JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int leaf_first, int leaf_last,
-                        const int* node_ranges, const float* centers, const float* locals, const int64_t* near_off,
-                        const int* near_src, float G, float eps2, float* out_acc4, void* stream) {
-  if (!pos4 || !node_ranges || !centers || !locals || !near_off || !out_acc4 || leaf_first < 0 ||
-      leaf_last < leaf_first || num_internal < 0)
+JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_units, const int* units,
+                        const int* aux, const int* runs, const int* node_ranges, const float* centers,
+                        const float* locals, float G, float eps2, float* out_acc4, float* partials, int num_split,
+                        const int* split, void* stream) {
+  if (num_units < 0 || num_split < 0 || num_internal < 0 ||
+      (num_units > 0 && (!pos4 || !units || !aux || !runs || !node_ranges || !centers || !locals || !out_acc4)) ||
+      (num_split > 0 && (!split || !partials || !out_acc4 || !node_ranges)))
     return JB_ERR_ARG;
-  if (p2p_mode != JB_P2P_FP32 && p2p_mode != JB_P2P_KAHAN) return JB_ERR_ARG;
-  return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, leaf_first, leaf_last, node_ranges, centers, locals,
-                               near_off, near_src, G, eps2, out_acc4, ST(stream));
+  if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL)) return JB_ERR_ARG;
+  return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, num_units, units, aux, runs, node_ranges, centers,
+                               locals, G, eps2, out_acc4, partials, num_split, split, ST(stream));
 }
 
 JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int* node_ranges, const float* centers,

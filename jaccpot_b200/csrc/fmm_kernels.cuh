@@ -165,46 +165,115 @@ __global__ void __launch_bounds__(128) k_m2m_level(int first, int last, const in
 }
 
 // ---------------------------------------------------------------------------
-// M2L: thread per target.
+// M2L over work units.  A unit is (target, first pair, end pair, slot): at
+// most a fixed number of consecutive pairs of one target's CSR list, so no
+// thread walks an arbitrarily long list.  slot < 0: the unit holds the
+// target's whole list and writes locals[target]; slot >= 0: it writes the
+// partial row partials[slot], and k_m2l_reduce sums a target's partial rows
+// in slot order.  Thread per unit, units sorted longest first.
+//
+// The next pair's multipole row is fetched into a per-thread shared-memory
+// row with cp.async while the current pair is rotated back, which hides the
+// L2 gather latency; the row stride is an odd number of 16-byte words so the
+// per-thread LDS.128 reads are bank-conflict free.  The local accumulates in
+// a shared-memory column per thread.
 // ---------------------------------------------------------------------------
 constexpr int kM2LThreads = 128;
 
+__host__ __device__ constexpr int row4(int p) { return (cstride(p) / 4) | 1; }  // float4 per smem row (odd)
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 template <int P>
-__global__ void __launch_bounds__(kM2LThreads) k_m2l_fp32(int num_targets, const int* __restrict__ targets,
-                                                          const float* __restrict__ mult, const float4* __restrict__ centers,
-                                                          const int64_t* __restrict__ far_off, const int* __restrict__ far_src,
-                                                          float* __restrict__ locals) {
-  constexpr int C = csize(P), CS = cstride(P);
-  extern __shared__ float sacc[];  // [C][kM2LThreads]
-  const int t = blockIdx.x * kM2LThreads + threadIdx.x;
-  if (t >= num_targets) return;
-  const int tgt = targets[t];
+__global__ void __launch_bounds__(kM2LThreads) k_m2l_units(int num_units, const int4* __restrict__ units,
+                                                           const float* __restrict__ mult,
+                                                           const float4* __restrict__ centers,
+                                                           const int* __restrict__ far_src, float* __restrict__ locals,
+                                                           float* __restrict__ partials) {
+  constexpr int C = csize(P), CS = cstride(P), R4 = row4(P);
+  extern __shared__ float4 m2l_smem[];
+  float4* row = m2l_smem + threadIdx.x * R4;
+  float* sacc = reinterpret_cast<float*>(m2l_smem + kM2LThreads * R4);  // [C][kM2LThreads]
+  const int u = blockIdx.x * kM2LThreads + threadIdx.x;
+  if (u >= num_units) return;
+  const int4 U = units[u];
+  const int tgt = U.x, e0 = U.y, e1 = U.z, slot = U.w;
 #pragma unroll
   for (int k = 0; k < C; ++k) sacc[k * kM2LThreads + threadIdx.x] = 0.f;
   const float4 ct = centers[tgt];
-  const int64_t e0 = far_off[tgt], e1 = far_off[tgt + 1];
-  for (int64_t e = e0; e < e1; ++e) {
-    const int s = far_src[e];
-    const float4 cs = centers[s];
-    float v[C], w[C];
+  int s = far_src[e0];
+  {
     const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s * CS);
 #pragma unroll
+    for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
+    cp_async_commit();
+  }
+  float4 cs = centers[s];
+  for (int e = e0; e < e1; ++e) {
+    float v[C], w[C];
+    cp_async_wait_all();
+#pragma unroll
     for (int k = 0; k < CS / 4; ++k) {
-      const float4 q = __ldg(src + k);
+      const float4 q = row[k];
       if (4 * k + 0 < C) v[4 * k + 0] = q.x;
       if (4 * k + 1 < C) v[4 * k + 1] = q.y;
       if (4 * k + 2 < C) v[4 * k + 2] = q.z;
       if (4 * k + 3 < C) v[4 * k + 3] = q.w;
     }
-    m2l_pair<P>(v, w, ct.x - cs.x, ct.y - cs.y, ct.z - cs.z);
+    const float dx = ct.x - cs.x, dy = ct.y - cs.y, dz = ct.z - cs.z;
+    // prefetch the next pair's source id and centre
+    const bool more = e + 1 < e1;
+    const int sn = more ? __ldg(far_src + e + 1) : s;
+    const float4 csn = centers[sn];
+    Trig<P> taz, tax;
+    float r;
+    align_trig<P>(dx, dy, dz, taz, tax, &r);
+    dz_apply<P, false>(v, taz);
+    bu_apply<P, false, false, false>(v);
+    dz_apply<P, true>(v, tax);
+    bu_apply<P, false, true, false>(v);
+    zm2l<P>(v, w, r);
+    // every value read from `row` has been consumed: refill it for the next pair
+    if (more) {
+      const float4* src = reinterpret_cast<const float4*>(mult + (size_t)sn * CS);
+#pragma unroll
+      for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
+      cp_async_commit();
+    }
+    bu_apply<P, true, false, true>(w);
+    dz_apply<P, false>(w, tax);
+    bu_apply<P, true, false, false>(w);
+    dz_apply<P, true>(w, taz);
 #pragma unroll
     for (int k = 0; k < C; ++k) sacc[k * kM2LThreads + threadIdx.x] += w[k];
+    s = sn;
+    cs = csn;
   }
-  float* dst = locals + (size_t)tgt * CS;
+  float* dst = (slot < 0) ? locals + (size_t)tgt * CS : partials + (size_t)slot * CS;
 #pragma unroll
   for (int k = 0; k < C; ++k) dst[k] = sacc[k * kM2LThreads + threadIdx.x];
 #pragma unroll
   for (int k = C; k < CS; ++k) dst[k] = 0.f;
+}
+
+// Sums the partial rows of targets whose list was split: split[i] =
+// (target, first slot, number of slots, unused).  Thread per (target, coefficient).
+template <int P>
+__global__ void __launch_bounds__(256) k_m2l_reduce(int num_split, const int4* __restrict__ split,
+                                                    const float* __restrict__ partials, float* __restrict__ locals) {
+  constexpr int CS = cstride(P);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(t / CS), k = (int)(t % CS);
+  if (i >= num_split) return;
+  const int4 sp = split[i];
+  float a = 0.f;
+  for (int q = 0; q < sp.z; ++q) a += partials[(size_t)(sp.y + q) * CS + k];
+  locals[(size_t)sp.x * CS + k] = a;
 }
 
 // ---------------------------------------------------------------------------
@@ -231,7 +300,22 @@ __global__ void __launch_bounds__(128) k_l2l_level(int first, int last, const in
 }
 
 // ---------------------------------------------------------------------------
-// Leaf evaluation: L2P + P2P, warp per target leaf.
+// Leaf evaluation over work units: L2P + P2P, warp per unit.
+//
+// A unit is one target leaf and a slice of its near list, stored as runs of
+// consecutive source leaves (= contiguous particle ranges, runs[r] = (first
+// particle, count)); units[u] = (leaf, first run, end run, source count),
+// aux[u] = (slot, flags).  flags & 1: the unit also does the leaf's self block
+// (diagonal excluded) and its far field (L2P).  slot < 0: the unit covers the
+// whole leaf and writes out_acc4; otherwise it writes partial[slot][lane] and
+// k_leaf_reduce sums a leaf's slots in order.
+//
+// Sources stream through the warp in packed chunks of 32 (the runs are
+// concatenated; each lane tracks its own run), staged in shared memory and
+// broadcast; the next chunk's loads are issued before the current chunk is
+// consumed.  Leaves with <= 16 (<= 8) particles give each target 2 (4)
+// lanes that split every chunk, so most lanes do useful work.  KAHAN adds
+// each chunk's partial sums into compensated per-target accumulators.
 // ---------------------------------------------------------------------------
 struct SmemF {
   const float* f;
@@ -239,96 +323,166 @@ struct SmemF {
 };
 
 template <bool KAHAN>
-struct Acc4 {
-  float x = 0.f, y = 0.f, z = 0.f, w = 0.f;
-  float cx = 0.f, cy = 0.f, cz = 0.f, cw = 0.f;
-  __device__ __forceinline__ static void add(float& s, float& c, float v) {
+struct NearAcc {
+  float s[4] = {0.f, 0.f, 0.f, 0.f};
+  float c[4] = {0.f, 0.f, 0.f, 0.f};
+  __device__ __forceinline__ void add(int i, float v) {
     if (KAHAN) {
-      const float y = v - c;
-      const float t = s + y;
-      c = (t - s) - y;
-      s = t;
+      const float y = v - c[i];
+      const float t = s[i] + y;
+      c[i] = (t - s[i]) - y;
+      s[i] = t;
     } else {
-      s += v;
+      s[i] += v;
     }
   }
-  __device__ __forceinline__ void add(float ax, float ay, float az, float aw) {
-    add(x, cx, ax);
-    add(y, cy, ay);
-    add(z, cz, az);
-    add(w, cw, aw);
-  }
+  __device__ __forceinline__ float value(int i) const { return KAHAN ? s[i] - c[i] : s[i]; }
 };
 
-template <bool KAHAN>
-__device__ __forceinline__ void p2p_block(const float4* __restrict__ spos, int ns, int self_j, float4 ti, float eps2,
-                                          Acc4<KAHAN>& a) {
-  for (int j = 0; j < ns; ++j) {
-    const float4 s = spos[j];
+#define JB_PAD4 make_float4(1e18f, 1e18f, 1e18f, 0.f)
+
+template <int G, bool KAHAN, bool POT, bool SELF>
+__device__ __forceinline__ void near_chunk(const float4* __restrict__ sp, float4 ti, int h, int self_j, float eps2,
+                                           NearAcc<KAHAN>& a) {
+  float ax = 0.f, ay = 0.f, az = 0.f, aw = 0.f;
+#pragma unroll
+  for (int q = 0; q < 32 / G; ++q) {
+    const int j = q * G + h;
+    const float4 s = sp[j];
     const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
     const float ir = rsqrtf(d2);
-    const bool self = (j == self_j);
-    const float mir = self ? 0.f : s.w * ir;
-    const float w = self ? 0.f : mir * ir * ir;
-    a.add(w * dx, w * dy, w * dz, mir);
+    float mir = s.w * ir;
+    float w = mir * (ir * ir);
+    if (SELF) {
+      const bool me = (j == self_j);
+      mir = me ? 0.f : mir;
+      w = me ? 0.f : w;
+    }
+    ax = fmaf(w, dx, ax);
+    ay = fmaf(w, dy, ay);
+    az = fmaf(w, dz, az);
+    if (POT) aw += mir;
+  }
+  a.add(0, ax);
+  a.add(1, ay);
+  a.add(2, az);
+  if (POT) a.add(3, aw);
+}
+
+template <int P, int G, bool KAHAN, bool POT>
+__device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
+                                          const int2* __restrict__ runs, float4 c, const float* sF,
+                                          float4* sP, int lane, float G_, float eps2, float4* __restrict__ out,
+                                          float4* __restrict__ partial) {
+  constexpr int C = csize(P);
+  const int tl = lane / G, h = lane % G;
+  const int nt = rg.y - rg.x + 1;
+  const bool active = tl < nt;
+  const float4 ti = active ? pos4[rg.x + tl] : make_float4(0.f, 0.f, 0.f, 0.f);
+  NearAcc<KAHAN> a;
+  const bool first = (aux.y & 1) != 0;
+  if (first) {
+    sP[lane] = (lane < nt) ? pos4[rg.x + lane] : JB_PAD4;
+    __syncwarp();
+    near_chunk<G, KAHAN, POT, true>(sP, ti, h, tl, eps2, a);
+    __syncwarp();
+  }
+  const int nsrc = U.w;
+  if (nsrc > 0) {
+    int r = U.y, rbase = 0;
+    int2 run = runs[r];
+    auto fetch = [&](int f) -> float4 {
+      while (f >= rbase + run.y && r + 1 < U.z) {
+        rbase += run.y;
+        ++r;
+        run = runs[r];
+      }
+      return (f < nsrc) ? pos4[run.x + (f - rbase)] : JB_PAD4;
+    };
+    float4 qn = fetch(lane);
+    for (int base = 0; base < nsrc; base += 32) {
+      sP[lane] = qn;
+      __syncwarp();
+      if (base + 32 < nsrc) qn = fetch(base + 32 + lane);
+      near_chunk<G, KAHAN, POT, false>(sP, ti, h, -1, eps2, a);
+      __syncwarp();
+    }
+  }
+  float v[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    v[i] = (POT || i < 3) ? a.value(i) : 0.f;
+    if (G >= 2) v[i] += __shfl_xor_sync(0xffffffffu, v[i], 1);
+    if (G >= 4) v[i] += __shfl_xor_sync(0xffffffffu, v[i], 2);
+  }
+  float4 res = make_float4(-G_ * v[0], -G_ * v[1], -G_ * v[2], -G_ * v[3]);
+  if (first) {
+    float U_[C];
+    solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
+    float phi, g[3];
+    l2p_eval<P>(SmemF{sF}, U_, &phi, g);
+    res.x -= G_ * g[0];
+    res.y -= G_ * g[1];
+    res.z -= G_ * g[2];
+    res.w -= G_ * phi;
+  }
+  if (active && h == 0) {
+    if (aux.x < 0) out[rg.x + tl] = res;
+    else partial[(size_t)aux.x * 32 + tl] = res;
   }
 }
 
-template <int P, bool KAHAN>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_eval(const float4* __restrict__ pos4, int num_internal,
-                                                                   int leaf_first, int leaf_last,
-                                                                   const int2* __restrict__ ranges,
-                                                                   const float4* __restrict__ centers,
-                                                                   const float* __restrict__ locals,
-                                                                   const int64_t* __restrict__ near_off,
-                                                                   const int* __restrict__ near_src, float G, float eps2,
-                                                                   float4* __restrict__ out) {
-  constexpr int C = csize(P), CS = cstride(P);
+template <int P, bool KAHAN, bool POT>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_units(
+    const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
+    const int2* __restrict__ aux, const int2* __restrict__ runs, const int2* __restrict__ ranges,
+    const float4* __restrict__ centers, const float* __restrict__ locals, float G, float eps2,
+    float4* __restrict__ out, float4* __restrict__ partial) {
+  constexpr int CS = cstride(P);
   __shared__ float sF[kWarpsPerBlock][CS];
   __shared__ float4 sP[kWarpsPerBlock][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int leaf = leaf_first + blockIdx.x * kWarpsPerBlock + warp;
-  if (leaf >= leaf_last) return;
-  const int node = num_internal + leaf;
+  const int u = blockIdx.x * kWarpsPerBlock + warp;
+  if (u >= num_units) return;
+  const int4 U = units[u];
+  const int2 ax = aux[u];
+  const int node = num_internal + U.x;
   const int2 rg = ranges[node];
   const float4 c = centers[node];
-  for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
-  __syncwarp();
-  const int64_t e0 = near_off[leaf], e1 = near_off[leaf + 1];
-  for (int tb = rg.x; tb <= rg.y; tb += 32) {
-    const int ti_idx = tb + lane;
-    const bool active = ti_idx <= rg.y;
-    const float4 ti = active ? pos4[ti_idx] : make_float4(0.f, 0.f, 0.f, 0.f);
-    Acc4<KAHAN> a;
-    // self leaf (all chunks), excluding the diagonal
-    for (int sb = rg.x; sb <= rg.y; sb += 32) {
-      const int ns = min(32, rg.y - sb + 1);
-      __syncwarp();
-      if (lane < ns) sP[warp][lane] = pos4[sb + lane];
-      __syncwarp();
-      p2p_block<KAHAN>(sP[warp], ns, ti_idx - sb, ti, eps2, a);
-    }
-    for (int64_t e = e0; e < e1; ++e) {
-      const int2 sr = ranges[num_internal + near_src[e]];
-      for (int sb = sr.x; sb <= sr.y; sb += 32) {
-        const int ns = min(32, sr.y - sb + 1);
-        __syncwarp();
-        if (lane < ns) sP[warp][lane] = pos4[sb + lane];
-        __syncwarp();
-        p2p_block<KAHAN>(sP[warp], ns, -1, ti, eps2, a);
-      }
-    }
-    // far field
-    float U[C];
-    solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U);
-    float phi, g[3];
-    l2p_eval<P>(SmemF{sF[warp]}, U, &phi, g);
-    if (active) {
-      out[ti_idx] = make_float4(-G * a.x - G * g[0], -G * a.y - G * g[1], -G * a.z - G * g[2],
-                                -G * a.w - G * phi);
-    }
+  if (ax.y & 1) {
+    for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
+    __syncwarp();
   }
+  const int nt = rg.y - rg.x + 1;
+  if (nt <= 8)
+    leaf_unit<P, 4, KAHAN, POT>(pos4, rg, U, ax, runs, c, sF[warp], sP[warp], lane, G, eps2, out, partial);
+  else if (nt <= 16)
+    leaf_unit<P, 2, KAHAN, POT>(pos4, rg, U, ax, runs, c, sF[warp], sP[warp], lane, G, eps2, out, partial);
+  else
+    leaf_unit<P, 1, KAHAN, POT>(pos4, rg, U, ax, runs, c, sF[warp], sP[warp], lane, G, eps2, out, partial);
+}
+
+// Sums the partial results of leaves whose work was split: split[i] = (leaf,
+// first slot, number of slots, unused).  Thread per (leaf, particle slot).
+static __global__ void __launch_bounds__(256) k_leaf_reduce(int num_split, const int4* __restrict__ split, int num_internal,
+                                                     const int2* __restrict__ ranges, const float4* __restrict__ partial,
+                                                     float4* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(t >> 5), l = (int)(t & 31);
+  if (i >= num_split) return;
+  const int4 sp = split[i];
+  const int2 rg = ranges[num_internal + sp.x];
+  if (rg.x + l > rg.y) return;
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int q = 0; q < sp.z; ++q) {
+    const float4 v = partial[(size_t)(sp.y + q) * 32 + l];
+    a.x += v.x;
+    a.y += v.y;
+    a.z += v.z;
+    a.w += v.w;
+  }
+  out[rg.x + l] = a;
 }
 
 // ---------------------------------------------------------------------------
@@ -414,14 +568,23 @@ struct RunM2M {
 
 template <int P>
 struct RunM2L {
-  static int run(int num_targets, const int* targets, const float* mult, const float* centers, const int64_t* far_off,
-                 const int* far_src, float* locals, cudaStream_t st) {
-    if (num_targets <= 0) return JB_OK;
-    const size_t sm = sizeof(float) * csize(P) * kM2LThreads;
-    cudaFuncSetAttribute(k_m2l_fp32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_m2l_fp32<P><<<blocks_for(num_targets, kM2LThreads), kM2LThreads, sm, st>>>(
-        num_targets, targets, mult, reinterpret_cast<const float4*>(centers), far_off, far_src, locals);
-    return launch_status();
+  static int run(int num_units, const int* units, const float* mult, const float* centers, const int* far_src,
+                 float* locals, float* partials, int num_split, const int* split, cudaStream_t st) {
+    if (num_units > 0) {
+      const size_t sm = sizeof(float4) * kM2LThreads * row4(P) + sizeof(float) * csize(P) * kM2LThreads;
+      cudaFuncSetAttribute(k_m2l_units<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_m2l_units<P><<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
+          num_units, reinterpret_cast<const int4*>(units), mult, reinterpret_cast<const float4*>(centers), far_src,
+          locals, partials);
+      const int rc = launch_status();
+      if (rc) return rc;
+    }
+    if (num_split > 0) {
+      k_m2l_reduce<P><<<blocks_for((int64_t)num_split * cstride(P), 256), 256, 0, st>>>(
+          num_split, reinterpret_cast<const int4*>(split), partials, locals);
+      return launch_status();
+    }
+    return JB_OK;
   }
 };
 
@@ -438,21 +601,41 @@ struct RunL2L {
 
 template <int P>
 struct RunLeafEval {
-  static int run(int mode, const float* pos4, int num_internal, int leaf_first, int leaf_last, const int* ranges,
-                 const float* centers, const float* locals, const int64_t* near_off, const int* near_src, float G,
-                 float eps2, float* out, cudaStream_t st) {
-    if (leaf_last <= leaf_first) return JB_OK;
-    const unsigned nb = blocks_for(leaf_last - leaf_first, kWarpsPerBlock);
-    if (mode == JB_P2P_KAHAN) {
-      k_leaf_eval<P, true><<<nb, 32 * kWarpsPerBlock, 0, st>>>(
-          reinterpret_cast<const float4*>(pos4), num_internal, leaf_first, leaf_last, reinterpret_cast<const int2*>(ranges),
-          reinterpret_cast<const float4*>(centers), locals, near_off, near_src, G, eps2, reinterpret_cast<float4*>(out));
-    } else {
-      k_leaf_eval<P, false><<<nb, 32 * kWarpsPerBlock, 0, st>>>(
-          reinterpret_cast<const float4*>(pos4), num_internal, leaf_first, leaf_last, reinterpret_cast<const int2*>(ranges),
-          reinterpret_cast<const float4*>(centers), locals, near_off, near_src, G, eps2, reinterpret_cast<float4*>(out));
+  template <bool K, bool PT>
+  static void go(unsigned nb, cudaStream_t st, const float4* pos4, int num_internal, int num_units, const int4* units,
+                 const int2* aux, const int2* runs, const int2* ranges, const float4* centers, const float* locals,
+                 float G, float eps2, float4* out, float4* partial) {
+    k_leaf_units<P, K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs, ranges,
+                                                               centers, locals, G, eps2, out, partial);
+  }
+  static int run(int mode, const float* pos4, int num_internal, int num_units, const int* units, const int* aux,
+                 const int* runs, const int* ranges, const float* centers, const float* locals, float G, float eps2,
+                 float* out, float* partial, int num_split, const int* split, cudaStream_t st) {
+    if (num_units > 0) {
+      const unsigned nb = blocks_for(num_units, kWarpsPerBlock);
+      auto a0 = reinterpret_cast<const float4*>(pos4);
+      auto a1 = reinterpret_cast<const int4*>(units);
+      auto a2 = reinterpret_cast<const int2*>(aux);
+      auto a3 = reinterpret_cast<const int2*>(runs);
+      auto a4 = reinterpret_cast<const int2*>(ranges);
+      auto a5 = reinterpret_cast<const float4*>(centers);
+      auto o = reinterpret_cast<float4*>(out);
+      auto pt = reinterpret_cast<float4*>(partial);
+      const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
+      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
+      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
+      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
+      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
+      const int rc = launch_status();
+      if (rc) return rc;
     }
-    return launch_status();
+    if (num_split > 0) {
+      k_leaf_reduce<<<blocks_for((int64_t)num_split * 32, 256), 256, 0, st>>>(
+          num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(ranges),
+          reinterpret_cast<const float4*>(partial), reinterpret_cast<float4*>(out));
+      return launch_status();
+    }
+    return JB_OK;
   }
 };
 

@@ -16,6 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .schedule import leaf_schedule, m2l_schedule
 from .tree import Topology
 
 
@@ -96,7 +97,8 @@ class Pass:
 
     def __init__(self, dt: DeviceTopology, p: int, *, G: float = 1.0, eps2: float = 0.0,
                  m2l_mode: int = _lib.JB_M2L_FP32, p2p_mode: int = _lib.JB_P2P_FP32,
-                 leaf_range: tuple[int, int] | None = None):
+                 leaf_range: tuple[int, int] | None = None, m2l_unit_pairs: int = 64,
+                 leaf_unit_sources: int = 4096):
         if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
             raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
         self.dt = dt
@@ -109,17 +111,26 @@ class Pass:
         self.lib = _lib.lib()
         t = dt.topo
         self.leaf_range = (0, t.num_leaves) if leaf_range is None else (int(leaf_range[0]), int(leaf_range[1]))
-        if self.leaf_range == (0, t.num_leaves):
-            self.m2l_targets, self.num_m2l_targets = dt.m2l_targets, dt.num_m2l_targets
-        else:
+        targets = None
+        if self.leaf_range != (0, t.num_leaves):
             # only nodes whose particle span meets this leaf range need locals
             lo = int(t.node_ranges[t.num_internal + self.leaf_range[0], 0])
             hi = int(t.node_ranges[t.num_internal + self.leaf_range[1] - 1, 1])
             tg = t.m2l_targets
-            keep = (t.node_ranges[tg, 1] >= lo) & (t.node_ranges[tg, 0] <= hi)
-            sel = np.ascontiguousarray(tg[keep])
-            self.num_m2l_targets = int(sel.size)
-            self.m2l_targets = torch.from_numpy(sel if sel.size else np.zeros(1, np.int32)).to(dt.device)
+            targets = tg[(t.node_ranges[tg, 1] >= lo) & (t.node_ranges[tg, 0] <= hi)]
+        self.m2l_sched = m2l_schedule(t, max_pairs=m2l_unit_pairs, targets=targets)
+        self.leaf_sched = leaf_schedule(t, max_sources=leaf_unit_sources, leaf_range=self.leaf_range)
+        dev = dt.device
+        up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+        self.d_m2l_units = up(self.m2l_sched.units)
+        self.d_m2l_split = up(self.m2l_sched.split)
+        self.m2l_partials = torch.empty((max(self.m2l_sched.num_slots, 1), self.ws.stride), device=dev,
+                                        dtype=torch.float32)
+        self.d_leaf_units = up(self.leaf_sched.units)
+        self.d_leaf_aux = up(self.leaf_sched.aux)
+        self.d_leaf_runs = up(self.leaf_sched.runs)
+        self.d_leaf_split = up(self.leaf_sched.split)
+        self.leaf_partials = torch.empty((max(self.leaf_sched.num_slots, 1) * 32, 4), device=dev, dtype=torch.float32)
 
     # -- stages -------------------------------------------------------------
     def load_particles(self, positions: torch.Tensor, masses: torch.Tensor, stream=None) -> None:
@@ -142,11 +153,12 @@ class Pass:
                                              _ptr(ws.centers), _ptr(ws.mult), s), "jb_m2m_level")
 
     def m2l(self, stream=None) -> None:
-        dt, ws, s = self.dt, self.ws, _stream_handle(stream)
+        ws, s, sc = self.ws, _stream_handle(stream), self.m2l_sched
         ws.locals.zero_()
-        _lib.check(self.lib.jb_m2l(self.p, self.m2l_mode, self.num_m2l_targets, _ptr(self.m2l_targets),
-                                   _ptr(ws.mult), _ptr(ws.centers), _ptr(dt.far_off), _ptr(dt.far_src),
-                                   _ptr(ws.locals), s), "jb_m2l")
+        _lib.check(self.lib.jb_m2l(self.p, self.m2l_mode, int(sc.units.shape[0]), _ptr(self.d_m2l_units),
+                                   _ptr(ws.mult), _ptr(ws.centers), _ptr(self.dt.far_src), _ptr(ws.locals),
+                                   _ptr(self.m2l_partials), int(sc.split.shape[0]), _ptr(self.d_m2l_split), s),
+                   "jb_m2l")
 
     def l2l(self, stream=None) -> None:
         t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)
@@ -155,13 +167,15 @@ class Pass:
             _lib.check(self.lib.jb_l2l_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
                                              _ptr(ws.centers), _ptr(ws.locals), s), "jb_l2l_level")
 
-    def evaluate(self, stream=None) -> torch.Tensor:
-        t, dt, ws = self.dt.topo, self.dt, self.ws
-        _lib.check(self.lib.jb_leaf_eval(self.p, self.p2p_mode, _ptr(ws.pos4), t.num_internal,
-                                         self.leaf_range[0], self.leaf_range[1],
-                                         _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.locals),
-                                         _ptr(dt.near_off), _ptr(dt.near_src), self.G, self.eps2,
-                                         _ptr(ws.acc4), _stream_handle(stream)), "jb_leaf_eval")
+    def evaluate(self, stream=None, potential: bool = False) -> torch.Tensor:
+        t, dt, ws, sc = self.dt.topo, self.dt, self.ws, self.leaf_sched
+        mode = self.p2p_mode | (_lib.JB_P2P_POTENTIAL if potential else 0)
+        _lib.check(self.lib.jb_leaf_eval(self.p, mode, _ptr(ws.pos4), t.num_internal, int(sc.units.shape[0]),
+                                         _ptr(self.d_leaf_units), _ptr(self.d_leaf_aux), _ptr(self.d_leaf_runs),
+                                         _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.locals), self.G,
+                                         self.eps2, _ptr(ws.acc4), _ptr(self.leaf_partials),
+                                         int(sc.split.shape[0]), _ptr(self.d_leaf_split),
+                                         _stream_handle(stream)), "jb_leaf_eval")
         return ws.acc4
 
     def evaluate_targets(self, targets_sorted: torch.Tensor, out: torch.Tensor | None = None,
@@ -194,5 +208,6 @@ class Pass:
 
     def launches_per_run(self) -> int:
         t = self.dt.topo
-        # p2m + m2m levels + zero + m2l + l2l levels + leaf_eval
-        return 1 + t.num_levels + 1 + 1 + t.num_levels + 1
+        # p2m + m2m levels + m2l (+ reduce) + l2l levels + leaf eval (+ reduce)
+        return (1 + t.num_levels + 1 + int(self.m2l_sched.split.shape[0] > 0) + t.num_levels + 1
+                + int(self.leaf_sched.split.shape[0] > 0))

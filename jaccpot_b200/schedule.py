@@ -1,0 +1,133 @@
+"""Work-unit schedules for the far-field (M2L) and leaf-evaluation kernels.
+
+Built once per topology on the host (prepare time, like the reference's
+near-field schedules in nearfield/_schedules.py:271 and the M2L chunking of
+runtime/kernels/_m2l.py:1667).  Both bound the work of one GPU thread / warp
+so that no single long interaction list sets the kernel's duration:
+
+* M2L units: at most ``max_pairs`` consecutive pairs of one target's CSR list;
+* leaf units: one target leaf and a slice of its neighbour list holding at
+  most ``max_sources`` source particles, stored as runs of consecutive
+  neighbour leaves (contiguous particle ranges).
+
+Targets (leaves) split over several units get consecutive scratch slots and an
+entry in the split list; the reduce kernels sum those slots in order, so the
+result does not depend on scheduling.  Units are ordered by decreasing work.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .tree import Topology
+
+
+@dataclass
+class M2LSchedule:
+    units: np.ndarray  # int32[U, 4] (target, first pair, end pair, slot)
+    split: np.ndarray  # int32[S, 4] (target, first slot, slot count, 0)
+    num_slots: int
+
+
+@dataclass
+class LeafSchedule:
+    units: np.ndarray  # int32[U, 4] (leaf, first run, end run, source count)
+    aux: np.ndarray  # int32[U, 2] (slot, flags)
+    runs: np.ndarray  # int32[R, 2] (first particle, count)
+    split: np.ndarray  # int32[S, 4] (leaf, first slot, slot count, 0)
+    num_slots: int
+
+
+def _slots(n_per: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Slot of every unit (-1 for singletons) and each split owner's first slot."""
+    multi = np.repeat(n_per > 1, n_per)
+    slot = np.where(multi, np.cumsum(multi) - 1, -1).astype(np.int32)
+    first = np.cumsum(n_per) - n_per
+    return slot, slot[first]
+
+
+def m2l_schedule(topo: Topology, max_pairs: int = 64, targets: np.ndarray | None = None) -> M2LSchedule:
+    off = topo.far_offsets
+    counts = np.diff(off)
+    tg = topo.m2l_targets if targets is None else np.asarray(targets, dtype=np.int64)
+    tg = tg[counts[tg] > 0].astype(np.int64)
+    c = counts[tg]
+    nu = (c + max_pairs - 1) // max_pairs
+    if tg.size == 0:
+        return M2LSchedule(np.zeros((0, 4), np.int32), np.zeros((0, 4), np.int32), 0)
+    rep = np.repeat(tg, nu)
+    k = np.arange(int(nu.sum())) - np.repeat(np.cumsum(nu) - nu, nu)
+    start = off[rep] + k * max_pairs
+    end = np.minimum(start + max_pairs, off[rep + 1])
+    slot, first_slot = _slots(nu)
+    units = np.stack([rep, start, end, slot], axis=1).astype(np.int32)
+    order = np.argsort(-(end - start), kind="stable")
+    units = np.ascontiguousarray(units[order])
+    sp = nu > 1
+    split = np.stack([tg[sp], first_slot[sp], nu[sp], np.zeros(int(sp.sum()), np.int64)], axis=1).astype(np.int32)
+    return M2LSchedule(units, np.ascontiguousarray(split), int((slot >= 0).sum()))
+
+
+def leaf_schedule(topo: Topology, max_sources: int = 4096, leaf_range: tuple[int, int] | None = None) -> LeafSchedule:
+    lo, hi = (0, topo.num_leaves) if leaf_range is None else leaf_range
+    ni = topo.num_internal
+    cnt_leaf = (topo.node_ranges[ni:, 1] - topo.node_ranges[ni:, 0] + 1).astype(np.int64)
+    start_leaf = topo.node_ranges[ni:, 0].astype(np.int64)
+    noff = topo.near_offsets
+    e0, e1 = int(noff[lo]), int(noff[hi])
+    src = topo.near_leaves[e0:e1].astype(np.int64)
+    tgt = np.repeat(np.arange(lo, hi, dtype=np.int64), np.diff(noff[lo:hi + 1]))
+    w = cnt_leaf[src]
+    # exclusive cumulative source count within each target leaf
+    cs = np.cumsum(w)
+    leaf_base = np.concatenate([[0], cs])[noff[lo:hi + 1][:-1] - e0]
+    cum_excl = cs - w - np.repeat(leaf_base, np.diff(noff[lo:hi + 1]))
+    uil = cum_excl // max_sources  # unit index within its leaf
+    if src.size:
+        brk = np.ones(src.size, dtype=bool)
+        brk[1:] = (tgt[1:] != tgt[:-1]) | (uil[1:] != uil[:-1]) | (src[1:] != src[:-1] + 1)
+        rid = np.cumsum(brk) - 1
+        rfirst = np.nonzero(brk)[0]
+        run_start = start_leaf[src[rfirst]]
+        run_cnt = np.add.reduceat(w, rfirst)
+        runs = np.stack([run_start, run_cnt], axis=1).astype(np.int32)
+        run_tgt, run_uil = tgt[rfirst], uil[rfirst]
+        ubrk = np.ones(rfirst.size, dtype=bool)
+        ubrk[1:] = (run_tgt[1:] != run_tgt[:-1]) | (run_uil[1:] != run_uil[:-1])
+        ufirst = np.nonzero(ubrk)[0]
+        u_leaf = run_tgt[ufirst]
+        u_rb = ufirst
+        u_re = np.concatenate([ufirst[1:], [rfirst.size]])
+        u_ns = np.add.reduceat(run_cnt, ufirst)
+        u_first = run_uil[ufirst] == 0
+        del rid
+    else:
+        runs = np.zeros((0, 2), np.int32)
+        u_leaf = u_rb = u_re = u_ns = np.zeros(0, np.int64)
+        u_first = np.zeros(0, bool)
+    # leaves without neighbours still need their self block + far field
+    all_leaves = np.arange(lo, hi, dtype=np.int64)
+    has = np.zeros(hi - lo, dtype=bool)
+    has[u_leaf - lo] = True
+    lone = all_leaves[~has]
+    u_leaf = np.concatenate([u_leaf, lone])
+    u_rb = np.concatenate([u_rb, np.zeros(lone.size, np.int64)])
+    u_re = np.concatenate([u_re, np.zeros(lone.size, np.int64)])
+    u_ns = np.concatenate([u_ns, np.zeros(lone.size, np.int64)])
+    u_first = np.concatenate([u_first, np.ones(lone.size, bool)])
+    # group units of a leaf together (leaf order, first unit first) to assign slots
+    order = np.lexsort((~u_first, u_leaf))
+    u_leaf, u_rb, u_re, u_ns, u_first = u_leaf[order], u_rb[order], u_re[order], u_ns[order], u_first[order]
+    leaves_u, n_per = np.unique(u_leaf, return_counts=True)
+    slot, first_slot = _slots(n_per)
+    work = u_ns + np.where(u_first, cnt_leaf[u_leaf], 0)
+    units = np.stack([u_leaf, u_rb, u_re, u_ns], axis=1).astype(np.int32)
+    aux = np.stack([slot, u_first.astype(np.int64)], axis=1).astype(np.int32)
+    srt = np.argsort(-work, kind="stable")
+    sp = n_per > 1
+    split = np.stack([leaves_u[sp], first_slot[sp], n_per[sp], np.zeros(int(sp.sum()), np.int64)],
+                     axis=1).astype(np.int32)
+    return LeafSchedule(np.ascontiguousarray(units[srt]), np.ascontiguousarray(aux[srt]),
+                        np.ascontiguousarray(runs), np.ascontiguousarray(split), int((slot >= 0).sum()))

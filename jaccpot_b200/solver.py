@@ -148,7 +148,7 @@ class FastMultipoleMethod:
         dev = state.device_topology.device
         want_np = as_numpy if as_numpy is not None else not isinstance(target_indices, torch.Tensor)
         if target_indices is None:
-            ps.evaluate()
+            ps.evaluate(potential=return_potential)
             acc = torch.empty((state.num_particles, 3), device=dev, dtype=torch.float32)
             pot = torch.empty((state.num_particles,), device=dev, dtype=torch.float32) if return_potential else None
             ps.unsort(acc, pot)

@@ -142,7 +142,7 @@ def test_leaf_eval_parity(case):
     s = setup(case)
     s.ps.upward()
     s.ps.downward()
-    acc4 = s.ps.evaluate()
+    acc4 = s.ps.evaluate(potential=True)
     torch.cuda.synchronize()
     cen = s.ps.ws.centers.double().cpu().numpy()[:, :3]
     loc = s.coeffs(s.ps.ws.locals)
@@ -185,7 +185,7 @@ def test_near_field_pair_counts_are_exact(case):
     ps.load_particles(torch.from_numpy(s.pos).cuda(), torch.ones(n, device="cuda"))
     ps.ws.centers.zero_()
     ps.ws.locals.zero_()
-    acc4 = ps.evaluate()
+    acc4 = ps.evaluate(potential=True)
     torch.cuda.synchronize()
     c = float(2.0 ** -50)
     got = np.rint(-acc4[:, 3].double().cpu().numpy() / c).astype(np.int64)
@@ -240,6 +240,6 @@ def test_errors_are_reported_not_trapped():
     s = setup(CASES[0])
     lb = _lib.lib()
     assert lb.jb_p2m(11, 0, 1, 0, 0, 0, 0, 0) == _lib.JB_OK + 1  # null pointers -> JB_ERR_ARG
-    assert lb.jb_m2l(s.p, 7, 1, 1, 1, 1, 1, 1, 1, 0) == 8  # unknown mode
+    assert lb.jb_m2l(s.p, 7, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0) == 8  # unknown mode
     with pytest.raises(_lib.JBError):
         _lib.coeff_stride(0)
