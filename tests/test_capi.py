@@ -1,0 +1,54 @@
+"""The C-ABI library loads without a GPU and exports every entry point that
+include/*.h declares; argument validation answers without touching the
+device."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from jaccpot_b200 import _lib
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        names += re.findall(r"JB_API\s+[\w\s\*]+?\b(jb_\w+)\s*\(", h.read_text())
+    return sorted(set(names))
+
+
+def test_header_declares_the_pass():
+    names = declared_symbols()
+    for required in ("jb_tree_build", "jb_p2m", "jb_m2m_level", "jb_m2l", "jb_l2l_level", "jb_leaf_eval",
+                     "jb_eval_targets", "jb_gather_sorted", "jb_scatter_unsorted", "jb_validate_lists"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.lib()
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    assert set(declared_symbols()) <= set(_lib.EXPORTED)
+
+
+def test_argument_errors_without_a_device():
+    lib = _lib.lib()
+    assert lib.jb_coeff_stride(8) == 84
+    assert lib.jb_coeff_stride(0) == 0 and lib.jb_coeff_stride(11) == 0
+    assert lib.jb_p2m(8, None, 1, 0, None, None, None, None) == 1
+    assert lib.jb_m2l(8, 0, -1, None, None, None, None, None, None, 0, None, None) == 1
+    assert lib.jb_m2l(8, 9, 1, 1, 1, 1, 1, 1, 1, 0, None, None) == 8
+    assert lib.jb_leaf_eval(8, 64, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1.0, 0.0, 1, 1, 0, None, None) == 1
+    assert lib.jb_m2m_level(8, 5, 4, None, None, None, None, None) == 1
+    assert lib.jb_gather_sorted(-1, None, None, None, None, None) == 1
+    assert lib.jb_direct_f64(0, None, 0, None, 1.0, 0.0, None, None) == 1
+    info = _lib.TreeInfo()
+    assert lib.jb_tree_info(None, ctypes.byref(info)) == 1
