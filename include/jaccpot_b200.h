@@ -177,6 +177,26 @@ JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal
                         const float* locals, float G, float eps2, float* out_acc4, float* partials, int num_split,
                         const int* split, void* stream);
 
+/* jb_leaf_eval for callers that cannot allocate device memory: no reference
+ * counterpart (the reference's XLA runtime owns all buffers).  A jax.ffi /
+ * XLA custom-call handler only receives the buffers XLA planned for it and
+ * must not cudaMalloc in the middle of XLA's asynchronous schedule, and code
+ * running under CUDA stream capture may not cudaMalloc at all; both can still
+ * pass inputs and outputs.  Same arguments as jb_leaf_eval except that
+ * `partials` is replaced by num_slots (1 + the largest slot in aux / split,
+ * the schedule's slot count): the scratch is a static device array of
+ * JB_LEAF_EVAL_NOALLOC_MAX_SLOTS x 32 float4 (16 MiB) that every GPU loading
+ * the library holds until exit.  num_slots above the maximum returns
+ * JB_ERR_WORKSPACE.  Allocates nothing.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (different streams, no ordering between them) race. */
+#define JB_LEAF_EVAL_NOALLOC_MAX_SLOTS 32768
+JB_API int jb_leaf_eval_noalloc(int p, int p2p_mode, const float* pos4, int num_internal, int num_units,
+                                const int* units, const int* aux, const int* runs, const int* node_ranges,
+                                const float* centers, const float* locals, float G, float eps2, float* out_acc4,
+                                int num_slots, int num_split, const int* split, void* stream);
+
 /* Target subset (runtime/kernels/_evaluate.py:1941-2095): targets_sorted are
  * sorted-slot indices; out_acc4[q] in target order. */
 JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int* node_ranges,

@@ -27,6 +27,7 @@ ERRORS = {
 JB_MAX_ORDER = 10
 JB_M2L_FP32, JB_M2L_SPLIT_BF16 = 0, 1
 JB_P2P_FP32, JB_P2P_KAHAN, JB_P2P_POTENTIAL = 0, 1, 2
+JB_LEAF_EVAL_NOALLOC_MAX_SLOTS = 32768
 
 # jb_tree_copy field ids
 TREE_FIELDS = {
@@ -86,6 +87,7 @@ _SIGNATURES = {
     "jb_m2l": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_l2l_level": [_I, _I, _I, _P, _P, _P, _P, _P],
     "jb_leaf_eval": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _I, _P, _P],
+    "jb_leaf_eval_noalloc": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _I, _I, _P, _P],
     "jb_eval_targets": [_I, _P, _I, _P, _P, _P, _P, _P, _P, _I64, _P, _F, _F, _P, _P],
     "jb_scatter_unsorted": [_I64, _P, _P, _P, _P, _P],
     "jb_direct_f64": [_I64, _P, _I64, _P, _D, _D, _P, _P],
