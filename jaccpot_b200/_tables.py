@@ -113,5 +113,110 @@ def generate(out_path: Path, max_order: int = MAX_ORDER) -> Path:
     return out_path
 
 
+def zm2l_matrix(p: int) -> np.ndarray:
+    """z-axis M2L in scaled form (operators/real_translations.py:213-335):
+    F_n^m r^(n+1) = sum_{k=|m|}^{p-n} sgn(m) (n+k)! (M_k^m r^-k), with
+    sgn(m) = (-1)^m (2 if m != 0 else 1); packed indices n^2 + n + m."""
+    from math import factorial
+
+    C = (p + 1) ** 2
+    z = np.zeros((C, C))
+    for n in range(p + 1):
+        for m in range(-n, n + 1):
+            am = abs(m)
+            sg = (-1.0) ** am * (2.0 if m else 1.0)
+            for k in range(am, p - n + 1):
+                z[n * n + n + m, k * k + k + m] = sg * factorial(n + k)
+    return z
+
+
+def kfold_matrix(p: int) -> np.ndarray:
+    """K = B^T Z0 B over all degrees <= p (B block-diagonal per degree).
+
+    B and the degree scalings r^-k / r^-(n+1) commute (B maps each degree to
+    itself), so the middle of the rotate+scale chain
+    B^T (r^-(n+1) Z0 r^-k) B equals r^-(n+1) K r^-k with K constant."""
+    C = (p + 1) ** 2
+    b = np.zeros((C, C))
+    for ell in range(p + 1):
+        b[ell * ell:(ell + 1) ** 2, ell * ell:(ell + 1) ** 2] = bu_matrix(ell)
+    k = b.T @ zm2l_matrix(p) @ b
+    k[np.abs(k) < 1e-9 * max(1.0, np.abs(k).max())] = 0.0
+    return k
+
+
+def kfold_blocks(k: np.ndarray) -> list[list[int]]:
+    """Index sets of the diagonal blocks of K (rows == columns), plus the
+    indices that K maps to zero (returned as the last entry)."""
+    C = k.shape[0]
+    nz = k != 0
+    parent = list(range(C))
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    for i, j in zip(*np.nonzero(nz)):
+        parent[find(int(i))] = find(int(j))
+    groups: dict[int, list[int]] = {}
+    used = nz.any(axis=0) | nz.any(axis=1)
+    for i in range(C):
+        if used[i]:
+            groups.setdefault(find(i), []).append(i)
+    blocks = sorted(groups.values(), key=lambda g: (-len(g), g[0]))
+    for g in blocks:
+        sub = np.zeros(C, dtype=bool)
+        sub[g] = True
+        assert not (nz[sub][:, ~sub].any() or nz[~sub][:, sub].any()), "K blocks are not square"
+    unused = [i for i in range(C) if not used[i]]
+    return blocks + [unused]
+
+
+def _flit(x: float) -> str:
+    v = float(np.float32(x))
+    return f"{v!r}f" if v != 0 else "0.0f"
+
+
+def generate_kfold(out_path: Path, max_order: int = MAX_ORDER) -> Path:
+    """Unrolled in-place K application per order, K entries as literals."""
+    lines = [
+        "// Generated by jaccpot_b200/_tables.py -- do not edit.",
+        "// In-place v <- K v with K = B^T Z0 B (the constant middle of the real",
+        "// rotate+scale M2L), block by block; indices K maps to zero are cleared.",
+        "#pragma once",
+        "namespace jb {",
+        "template <int P> struct KFold;",
+    ]
+    for p in range(1, max_order + 1):
+        k = kfold_matrix(p)
+        *blocks, unused = kfold_blocks(k)
+        lines.append(f"template <> struct KFold<{p}> {{")
+        lines.append(f"  static constexpr int kNnz = {int((k != 0).sum())};")
+        lines.append("  static __device__ __forceinline__ void apply(float* v) {")
+        for g in blocks:
+            lines.append("    {")
+            lines.append("      " + " ".join(f"const float i{j} = v[{j}];" for j in g))
+            for i in g:
+                terms = [(j, k[i, j]) for j in g if k[i, j] != 0]
+                expr = f"{_flit(terms[0][1])} * i{terms[0][0]}"
+                for j, val in terms[1:]:
+                    expr = f"fmaf({_flit(val)}, i{j}, {expr})"
+                lines.append(f"      v[{i}] = {expr};")
+            lines.append("    }")
+        if unused:
+            lines.append("    " + " ".join(f"v[{i}] = 0.f;" for i in unused))
+        lines.append("  }")
+        lines.append("};")
+    lines.append("}  // namespace jb")
+    text = "\n".join(lines) + "\n"
+    out_path.parent.mkdir(parents=True, exist_ok=True)
+    if not out_path.exists() or out_path.read_text() != text:
+        out_path.write_text(text)
+    return out_path
+
+
 if __name__ == "__main__":
     generate(Path(__file__).resolve().parent / "csrc" / "generated" / "bu_tables.h")
+    generate_kfold(Path(__file__).resolve().parent / "csrc" / "generated" / "kfold_tables.h")

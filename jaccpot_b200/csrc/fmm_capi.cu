@@ -1,5 +1,5 @@
 // C-ABI entry points (include/jaccpot_b200.h) and the order-independent kernels.
-#include "fmm_kernels.cuh"
+#include "fmm_adjoint.cuh"
 
 #define JB_ORDERS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 JB_ORDERS(JB_DECLARE_ORDER)
@@ -83,6 +83,21 @@ static int dispatch(int p, A... args) {
   }
 }
 
+#define JB_ADJ_ORDERS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9)
+
+template <typename Fn>
+static int dispatch_adj(int p, Fn&& fn) {
+  switch (p) {
+#define JB_ACASE(PP) \
+  case PP:           \
+    return fn(RunAdj<PP>{});
+    JB_ADJ_ORDERS(JB_ACASE)
+#undef JB_ACASE
+    default:
+      return JB_ERR_ORDER;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Verification: FP64 direct sum on sampled targets (the error report every
 // result carries; runtime/reference.py:292 semantics, self pair excluded).
@@ -149,6 +164,110 @@ __global__ void k_probe(int iters, int use_mufu, float* out) {
 #pragma unroll
   for (int k = 0; k < 8; ++k) s += a[k];
   if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+// ---------------------------------------------------------------------------
+// Near field: warp per leaf unit, lane = target particle.  For the pair
+// (k, l), d = x_k - x_l, q = (|d|^2 + eps^2)^-1/2:
+//   dL/dx_k += G [ -m_l q^3 w_k + m_k q^3 w_l + 3 q^5 (m_l (w_k.d) - m_k (w_l.d)) d ]
+//   dL/dm_k += G q^3 (w_l . d)
+// which needs l in near(k) <=> k in near(l) (the lists are symmetric).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void adj_near_pair(float4 tk, float4 wk, float4 s, float4 ws, float eps2, bool skip,
+                                              float* a) {
+  const float dx = tk.x - s.x, dy = tk.y - s.y, dz = tk.z - s.z;
+  const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+  const float q = skip ? 0.f : rsqrtf(d2);
+  const float q3 = q * q * q;
+  const float q5 = q3 * q * q;
+  const float wkd = wk.x * dx + wk.y * dy + wk.z * dz;
+  const float wld = ws.x * dx + ws.y * dy + ws.z * dz;
+  const float c = 3.f * q5 * (s.w * wkd - tk.w * wld);
+  const float aml = -s.w * q3, amk = tk.w * q3;
+  a[0] += aml * wk.x + amk * ws.x + c * dx;
+  a[1] += aml * wk.y + amk * ws.y + c * dy;
+  a[2] += aml * wk.z + amk * ws.z + c * dz;
+  a[3] += q3 * wld;
+}
+
+static __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_adj_near(
+    const float4* __restrict__ pos4, const float4* __restrict__ w4, int num_internal, int num_units,
+    const int4* __restrict__ units, const int2* __restrict__ aux, const int2* __restrict__ runs,
+    const int2* __restrict__ ranges, float G, float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
+  __shared__ float4 sP[kWarpsPerBlock][32];
+  __shared__ float4 sW[kWarpsPerBlock][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarpsPerBlock + warp;
+  if (u >= num_units) return;
+  const int4 U = units[u];
+  const int2 ax = aux[u];
+  const int2 rg = ranges[num_internal + U.x];
+  const int nt = rg.y - rg.x + 1;
+  float a[4] = {0.f, 0.f, 0.f, 0.f};
+  // targets beyond 32 particles take further passes
+  for (int t0 = 0; t0 < nt; t0 += 32) {
+    const int tl = t0 + lane;
+    const bool active = tl < nt;
+    const float4 tk = active ? pos4[rg.x + tl] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 wk = active ? w4[rg.x + tl] : make_float4(0.f, 0.f, 0.f, 0.f);
+    a[0] = a[1] = a[2] = a[3] = 0.f;
+    if (ax.y & 1) {
+      for (int s0 = 0; s0 < nt; s0 += 32) {
+        const int j = s0 + lane;
+        sP[warp][lane] = (j < nt) ? pos4[rg.x + j] : JB_PAD4;
+        sW[warp][lane] = (j < nt) ? w4[rg.x + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q)
+          adj_near_pair(tk, wk, sP[warp][q], sW[warp][q], eps2, (s0 + q == tl) || (s0 + q >= nt), a);
+        __syncwarp();
+      }
+    }
+    const int nsrc = U.w;
+    int r = U.y, rbase = 0;
+    int2 run = (U.z > U.y) ? runs[r] : make_int2(0, 0);
+    for (int base = 0; base < nsrc; base += 32) {
+      const int f = base + lane;
+      while (f >= rbase + run.y && r + 1 < U.z) {
+        rbase += run.y;
+        ++r;
+        run = runs[r];
+      }
+      const bool ok = f < nsrc;
+      sP[warp][lane] = ok ? pos4[run.x + (f - rbase)] : JB_PAD4;
+      sW[warp][lane] = ok ? w4[run.x + (f - rbase)] : make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncwarp();
+#pragma unroll 8
+      for (int q = 0; q < 32; ++q) adj_near_pair(tk, wk, sP[warp][q], sW[warp][q], eps2, base + q >= nsrc, a);
+      __syncwarp();
+    }
+    if (active) {
+      const float4 res = make_float4(G * a[0], G * a[1], G * a[2], G * a[3]);
+      if (ax.x < 0) out[rg.x + tl] = res;
+      else partial[(size_t)ax.x * 32 + tl] = res;
+    }
+  }
+}
+
+// M2L centre-gradient gather, thread per node u: for every pair e = (u <- v)
+// of u's list, g_e belongs to u as target and the reverse pair (v <- u)
+// (index rev[e]) contributes -g_rev(e) to u as source.
+__global__ void k_adj_m2l_gather(int num_nodes, const int64_t* __restrict__ far_off, const int* __restrict__ rev,
+                                 const float4* __restrict__ g4, float4* __restrict__ cbar4) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= num_nodes) return;
+  float x = 0.f, y = 0.f, z = 0.f;
+  for (int64_t e = far_off[u]; e < far_off[u + 1]; ++e) {
+    const float4 a = g4[e], b = g4[rev[e]];
+    x += a.x - b.x;
+    y += a.y - b.y;
+    z += a.z - b.z;
+  }
+  float4 c = cbar4[u];
+  c.x += x;
+  c.y += y;
+  c.z += z;
+  cbar4[u] = c;
 }
 
 static inline unsigned blocks_1d(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
@@ -266,6 +385,101 @@ JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int
     return JB_ERR_ARG;
   return dispatch<RunTargets>(p, pos4, num_internal, node_ranges, centers, locals, near_off, near_src, leaf_of,
                               num_targets, targets_sorted, G, eps2, out_acc4, ST(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint (VJP) of the pass at fixed topology.
+// ---------------------------------------------------------------------------
+JB_API int jb_adj_near(const float* pos4, const float* w4, int num_internal, int num_units, const int* units,
+                       const int* aux, const int* runs, const int* node_ranges, float G, float eps2, float* out_xm4,
+                       float* partials, int num_split, const int* split, void* stream) {
+  if (num_units < 0 || num_split < 0 || num_internal < 0 ||
+      (num_units > 0 && (!pos4 || !w4 || !units || !aux || !runs || !node_ranges || !out_xm4)) ||
+      (num_split > 0 && (!split || !partials || !out_xm4 || !node_ranges)))
+    return JB_ERR_ARG;
+  if (num_units > 0) {
+    k_adj_near<<<blocks_1d(num_units, kWarpsPerBlock), 32 * kWarpsPerBlock, 0, ST(stream)>>>(
+        reinterpret_cast<const float4*>(pos4), reinterpret_cast<const float4*>(w4), num_internal, num_units,
+        reinterpret_cast<const int4*>(units), reinterpret_cast<const int2*>(aux), reinterpret_cast<const int2*>(runs),
+        reinterpret_cast<const int2*>(node_ranges), G, eps2, reinterpret_cast<float4*>(out_xm4),
+        reinterpret_cast<float4*>(partials));
+    const int rc = launch_status();
+    if (rc) return rc;
+  }
+  if (num_split > 0) {
+    k_leaf_reduce<<<blocks_1d((int64_t)num_split * 32, 256), 256, 0, ST(stream)>>>(
+        num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(node_ranges),
+        reinterpret_cast<const float4*>(partials), reinterpret_cast<float4*>(out_xm4));
+    return launch_status();
+  }
+  return JB_OK;
+}
+
+JB_API int jb_adj_leaf_far(int p, const float* pos4, const float* w4, int num_nodes, int num_internal,
+                           const int* node_ranges, const float* centers, const float* locals, float G, float* xm4,
+                           float* lbar, float* cbar4, void* stream) {
+  if (!pos4 || !w4 || !node_ranges || !centers || !locals || !xm4 || !lbar || !cbar4 || num_nodes < 1 ||
+      num_internal < 0 || num_internal >= num_nodes)
+    return JB_ERR_ARG;
+  return dispatch_adj(p, [&](auto R) {
+    return decltype(R)::leaf_far(pos4, w4, num_nodes, num_internal, node_ranges, centers, locals, G, xm4, lbar,
+                                 cbar4, ST(stream));
+  });
+}
+
+JB_API int jb_adj_l2l_level(int p, int first, int last, const int* left, const int* right, const float* centers,
+                            const float* locals, float* lbar, float* cbar4, void* stream) {
+  if (first < 0 || last < first || (last > first && (!left || !right || !centers || !locals || !lbar || !cbar4)))
+    return JB_ERR_ARG;
+  return dispatch_adj(p, [&](auto R) {
+    return decltype(R)::l2l_level(first, last, left, right, centers, locals, lbar, cbar4, ST(stream));
+  });
+}
+
+JB_API int jb_adj_m2l(int p, int num_units, const int* units, const float* lbar, const float* centers,
+                      const int* far_src, float* mbar, float* partials, int num_split, const int* split,
+                      void* stream) {
+  if (num_units < 0 || num_split < 0 || (num_units > 0 && (!units || !lbar || !centers || !far_src || !mbar)) ||
+      (num_split > 0 && (!split || !partials || !mbar)))
+    return JB_ERR_ARG;
+  if (p < 1 || p > JB_ADJ_MAX_ORDER) return JB_ERR_ORDER;
+  return dispatch<RunM2L>(p, num_units, units, lbar, centers, far_src, mbar, partials, num_split, split, ST(stream),
+                          true);
+}
+
+JB_API int jb_adj_m2l_centers(int p, int num_nodes, int64_t num_pairs, const int* pair_tgt, const int* far_src,
+                              const int64_t* far_off, const int* rev, const float* mult, const float* lbar,
+                              const float* centers, float* g4, float* cbar4, void* stream) {
+  if (num_nodes < 1 || num_pairs < 0 || !far_off || !cbar4 ||
+      (num_pairs > 0 && (!pair_tgt || !far_src || !rev || !mult || !lbar || !centers || !g4)))
+    return JB_ERR_ARG;
+  if (num_pairs == 0) return (p >= 1 && p <= JB_ADJ_MAX_ORDER) ? JB_OK : JB_ERR_ORDER;
+  const int rc = dispatch_adj(p, [&](auto R) {
+    return decltype(R)::m2l_pairs(num_pairs, pair_tgt, far_src, mult, lbar, centers, g4, ST(stream));
+  });
+  if (rc) return rc;
+  k_adj_m2l_gather<<<blocks_1d(num_nodes, 128), 128, 0, ST(stream)>>>(
+      num_nodes, far_off, rev, reinterpret_cast<const float4*>(g4), reinterpret_cast<float4*>(cbar4));
+  return launch_status();
+}
+
+JB_API int jb_adj_m2m_level(int p, int first, int last, const int* left, const int* right, const float* centers,
+                            const float* mult, float* mbar, float* cbar4, void* stream) {
+  if (first < 0 || last < first || (last > first && (!left || !right || !centers || !mult || !mbar || !cbar4)))
+    return JB_ERR_ARG;
+  return dispatch_adj(p, [&](auto R) {
+    return decltype(R)::m2m_level(first, last, left, right, centers, mult, mbar, cbar4, ST(stream));
+  });
+}
+
+JB_API int jb_adj_p2m(int p, const float* pos4, int num_nodes, int num_internal, const int* node_ranges,
+                      const float* centers, const float* mbar, const float* cbar4, float* xm4, void* stream) {
+  if (!pos4 || !node_ranges || !centers || !mbar || !cbar4 || !xm4 || num_nodes < 1 || num_internal < 0 ||
+      num_internal >= num_nodes)
+    return JB_ERR_ARG;
+  return dispatch_adj(p, [&](auto R) {
+    return decltype(R)::p2m(pos4, num_nodes, num_internal, node_ranges, centers, mbar, cbar4, xm4, ST(stream));
+  });
 }
 
 }  // extern "C"

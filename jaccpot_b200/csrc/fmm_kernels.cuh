@@ -189,12 +189,17 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int P>
-__global__ void __launch_bounds__(kM2LThreads) k_m2l_units(int num_units, const int4* __restrict__ units,
-                                                           const float* __restrict__ mult,
-                                                           const float4* __restrict__ centers,
-                                                           const int* __restrict__ far_src, float* __restrict__ locals,
-                                                           float* __restrict__ partials) {
+// NEG = true evaluates M2L(c_source - c_target) instead (the displacement of
+// the reverse pair), which is what the adjoint's transposed M2L needs: the
+// real M2L matrix is symmetric, so sum_v M2L(c_v - c_u)^T Lbar_v is this
+// kernel run over u's own list with Lbar in place of the multipoles.
+template <int P, bool NEG>
+__global__ void __launch_bounds__(kM2LThreads, 3) k_m2l_units(int num_units, const int4* __restrict__ units,
+                                                              const float* __restrict__ mult,
+                                                              const float4* __restrict__ centers,
+                                                              const int* __restrict__ far_src,
+                                                              float* __restrict__ locals,
+                                                              float* __restrict__ partials) {
   constexpr int C = csize(P), CS = cstride(P), R4 = row4(P);
   extern __shared__ float4 m2l_smem[];
   float4* row = m2l_smem + threadIdx.x * R4;
@@ -215,7 +220,7 @@ __global__ void __launch_bounds__(kM2LThreads) k_m2l_units(int num_units, const 
   }
   float4 cs = centers[s];
   for (int e = e0; e < e1; ++e) {
-    float v[C], w[C];
+    float v[C];
     cp_async_wait_all();
 #pragma unroll
     for (int k = 0; k < CS / 4; ++k) {
@@ -225,32 +230,20 @@ __global__ void __launch_bounds__(kM2LThreads) k_m2l_units(int num_units, const 
       if (4 * k + 2 < C) v[4 * k + 2] = q.z;
       if (4 * k + 3 < C) v[4 * k + 3] = q.w;
     }
-    const float dx = ct.x - cs.x, dy = ct.y - cs.y, dz = ct.z - cs.z;
-    // prefetch the next pair's source id and centre
+    // every value read from `row` is in registers: refill it for the next pair
     const bool more = e + 1 < e1;
     const int sn = more ? __ldg(far_src + e + 1) : s;
-    const float4 csn = centers[sn];
-    Trig<P> taz, tax;
-    float r;
-    align_trig<P>(dx, dy, dz, taz, tax, &r);
-    dz_apply<P, false>(v, taz);
-    bu_apply<P, false, false, false>(v);
-    dz_apply<P, true>(v, tax);
-    bu_apply<P, false, true, false>(v);
-    zm2l<P>(v, w, r);
-    // every value read from `row` has been consumed: refill it for the next pair
     if (more) {
       const float4* src = reinterpret_cast<const float4*>(mult + (size_t)sn * CS);
 #pragma unroll
       for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
       cp_async_commit();
     }
-    bu_apply<P, true, false, true>(w);
-    dz_apply<P, false>(w, tax);
-    bu_apply<P, true, false, false>(w);
-    dz_apply<P, true>(w, taz);
+    const float4 csn = centers[sn];
+    if (NEG) m2l_kfold<P>(v, cs.x - ct.x, cs.y - ct.y, cs.z - ct.z);
+    else m2l_kfold<P>(v, ct.x - cs.x, ct.y - cs.y, ct.z - cs.z);
 #pragma unroll
-    for (int k = 0; k < C; ++k) sacc[k * kM2LThreads + threadIdx.x] += w[k];
+    for (int k = 0; k < C; ++k) sacc[k * kM2LThreads + threadIdx.x] += v[k];
     s = sn;
     cs = csn;
   }
@@ -569,11 +562,12 @@ struct RunM2M {
 template <int P>
 struct RunM2L {
   static int run(int num_units, const int* units, const float* mult, const float* centers, const int* far_src,
-                 float* locals, float* partials, int num_split, const int* split, cudaStream_t st) {
+                 float* locals, float* partials, int num_split, const int* split, cudaStream_t st, bool neg = false) {
     if (num_units > 0) {
       const size_t sm = sizeof(float4) * kM2LThreads * row4(P) + sizeof(float) * csize(P) * kM2LThreads;
-      cudaFuncSetAttribute(k_m2l_units<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_m2l_units<P><<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
+      auto kern = neg ? k_m2l_units<P, true> : k_m2l_units<P, false>;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      kern<<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
           num_units, reinterpret_cast<const int4*>(units), mult, reinterpret_cast<const float4*>(centers), far_src,
           locals, partials);
       const int rc = launch_status();
@@ -662,4 +656,18 @@ struct RunTargets {
   extern template struct jb::RunM2L<PP>;      \
   extern template struct jb::RunL2L<PP>;      \
   extern template struct jb::RunLeafEval<PP>; \
-  extern template struct jb::RunTargets<PP>;
+  extern template struct jb::RunTargets<PP>;  \
+  JB_DECLARE_ADJ_##PP
+
+// The adjoint needs the order p+1 M2L, so it is built for p <= 9.
+#define JB_DECLARE_ADJ_1 extern template struct jb::RunAdj<1>;
+#define JB_DECLARE_ADJ_2 extern template struct jb::RunAdj<2>;
+#define JB_DECLARE_ADJ_3 extern template struct jb::RunAdj<3>;
+#define JB_DECLARE_ADJ_4 extern template struct jb::RunAdj<4>;
+#define JB_DECLARE_ADJ_5 extern template struct jb::RunAdj<5>;
+#define JB_DECLARE_ADJ_6 extern template struct jb::RunAdj<6>;
+#define JB_DECLARE_ADJ_7 extern template struct jb::RunAdj<7>;
+#define JB_DECLARE_ADJ_8 extern template struct jb::RunAdj<8>;
+#define JB_DECLARE_ADJ_9 extern template struct jb::RunAdj<9>;
+#define JB_DECLARE_ADJ_10
+#define JB_ADJ_MAX_ORDER 9

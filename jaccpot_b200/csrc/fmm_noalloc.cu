@@ -14,7 +14,7 @@
 // differs.
 #include <mutex>
 
-#include "fmm_kernels.cuh"
+#include "fmm_adjoint.cuh"
 
 #define JB_ORDERS_NA(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 JB_ORDERS_NA(JB_DECLARE_ORDER)

@@ -31,6 +31,7 @@
 #include <stdint.h>
 
 #include "generated/bu_tables.h"
+#include "generated/kfold_tables.h"
 
 namespace jb {
 
@@ -143,6 +144,78 @@ __device__ __forceinline__ void rot_mult_to_z(float* v, const Trig<P>& taz, cons
   bu_apply<P, false, false, false>(v);
   dz_apply<P, true>(v, tax);
   bu_apply<P, false, false, false>(v);
+}
+
+// v <- Dz(+a) v (NEG = false) or Dz(-a) v (NEG = true) on every degree, with
+// (cos a, sin a) = (c1, s1); cos/sin(m a) by angle addition, m outermost so
+// that only four trig values are live.
+template <int P, bool NEG>
+__device__ __forceinline__ void dz_rot(float* v, float c1, float s1) {
+  const float sa = NEG ? -s1 : s1;
+  float c = c1, s = sa;
+#pragma unroll
+  for (int m = 1; m <= P; ++m) {
+    if (m > 1) {
+      const float cn = c * c1 - s * sa;
+      s = fmaf(s, c1, c * sa);
+      c = cn;
+    }
+#pragma unroll
+    for (int l = m; l <= P; ++l) {
+      const int ip = shi(l, m), im = shi(l, -m);
+      const float vp = v[ip], vm = v[im];
+      v[ip] = c * vp - s * vm;
+      v[im] = fmaf(s, vp, c * vm);
+    }
+  }
+}
+
+// v[degree n] *= s^(n + OFF) for n = 0..P.
+template <int P, int OFF>
+__device__ __forceinline__ void scale_degrees(float* v, float s) {
+  float f = 1.f;
+#pragma unroll
+  for (int k = 0; k < OFF; ++k) f *= s;
+#pragma unroll
+  for (int n = 0; n <= P; ++n) {
+#pragma unroll
+    for (int m = -n; m <= n; ++m) v[shi(n, m)] *= f;
+    f *= s;
+  }
+}
+
+// One M2L in place, delta = target - source, as the chain
+//   Dz(az) -> B -> Dz(-ax) -> r^-k -> K -> r^-(n+1) -> Dz(ax) -> B^T -> Dz(-az)
+// which is the reference's rotate-to-z / z-M2L / rotate-back cascade
+// (operators/m2l_real_rot_scale.py:288-386) with its middle B^T Z B folded
+// into the constant K (B commutes with the per-degree radius scalings).
+template <int P>
+__device__ __forceinline__ void m2l_kfold(float* v, float dx, float dy, float dz) {
+  const float rho2 = dx * dx + dy * dy;
+  const float r2 = rho2 + dz * dz;
+  float caz = 1.f, saz = 0.f, cax = 1.f, sax = 0.f;
+  const float rho = sqrtf(rho2);
+  const float r = sqrtf(r2);
+  if (rho2 > 0.f) {
+    const float ir = 1.f / rho;
+    caz = dy * ir;
+    saz = dx * ir;
+  }
+  if (r2 > 0.f) {
+    const float ir = 1.f / r;
+    cax = dz * ir;
+    sax = rho * ir;
+  }
+  const float s = 1.f / fmaxf(r, 1.0e-30f);
+  dz_rot<P, false>(v, caz, saz);
+  bu_apply<P, false, false, false>(v);
+  dz_rot<P, true>(v, cax, sax);
+  scale_degrees<P, 0>(v, s);
+  KFold<P>::apply(v);
+  scale_degrees<P, 1>(v, s);
+  dz_rot<P, false>(v, cax, sax);
+  bu_apply<P, true, false, false>(v);
+  dz_rot<P, true>(v, caz, saz);
 }
 
 // z-M2L in scaled form; Mz is the rotated multipole, Lz the z-frame local.
@@ -333,6 +406,63 @@ __device__ __forceinline__ void l2p_eval(const FP& F, const float* U, float* phi
   }
 #undef JB_UL
   *phi = p0;
+  g[0] = gx;
+  g[1] = gy;
+  g[2] = gz;
+}
+
+// Calls f(axis, row, col, value) for every entry of the derivative ladders
+// D_a (a = x, y, z = 0, 1, 2): d/ddelta_a sum_col F[col] U_col(delta) =
+// sum_row (D_a F)[row] U_row(delta), (D_a F)[row] = sum value * F[col].  These
+// are the relations l2p_eval uses for the gradient; the adjoint kernels use
+// them for Hessian-vector products, for the derivative of a translated
+// expansion with respect to its displacement, and (transposed) for the
+// derivative of U itself: dU_col/ddelta_a = sum_row D_a[row][col] U_row.
+template <int P, typename Fn>
+__device__ __forceinline__ void for_ladder(Fn&& f) {
+#pragma unroll
+  for (int n = 1; n <= P; ++n) {
+    const int q = n - 1;
+    f(2, shi(q, 0), shi(n, 0), 1.f);
+    if (q >= 1) {
+      f(0, shi(q, 1), shi(n, 0), -1.f);
+      f(1, shi(q, -1), shi(n, 0), -1.f);
+    }
+#pragma unroll
+    for (int m = 1; m <= n; ++m) {
+      const int fc = shi(n, m), fs = shi(n, -m);
+      if (m <= q) {
+        f(2, shi(q, m), fc, 1.f);
+        f(2, shi(q, -m), fs, 1.f);
+      }
+      if (m - 1 <= q) {
+        f(0, shi(q, m - 1), fc, 0.5f);
+        f(1, shi(q, m - 1), fs, 0.5f);
+        if (m - 1 >= 1) {
+          f(1, shi(q, -(m - 1)), fc, -0.5f);
+          f(0, shi(q, -(m - 1)), fs, 0.5f);
+        }
+      }
+      if (m + 1 <= q) {
+        f(0, shi(q, m + 1), fc, -0.5f);
+        f(1, shi(q, -(m + 1)), fc, -0.5f);
+        f(0, shi(q, -(m + 1)), fs, -0.5f);
+        f(1, shi(q, m + 1), fs, 0.5f);
+      }
+    }
+  }
+}
+
+// g[a] = sum_row X[row] (D_a F)[row] for a = x, y, z.
+template <int P, typename FX, typename FF>
+__device__ __forceinline__ void ladder_dot3(const FX& X, const FF& F, float* g) {
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  for_ladder<P>([&](int a, int row, int col, float val) {
+    const float t = val * X(row) * F(col);
+    if (a == 0) gx += t;
+    else if (a == 1) gy += t;
+    else gz += t;
+  });
   g[0] = gx;
   g[1] = gy;
   g[2] = gz;

@@ -1,5 +1,5 @@
 // One expansion order of the pass kernels (built once per order with -DJB_ORDER=P).
-#include "fmm_kernels.cuh"
+#include "fmm_adjoint.cuh"
 
 #ifndef JB_ORDER
 #error "JB_ORDER must be defined"
@@ -11,3 +11,6 @@ template struct jb::RunM2L<JB_ORDER>;
 template struct jb::RunL2L<JB_ORDER>;
 template struct jb::RunLeafEval<JB_ORDER>;
 template struct jb::RunTargets<JB_ORDER>;
+#if JB_ORDER <= 9
+template struct jb::RunAdj<JB_ORDER>;
+#endif
