@@ -211,6 +211,54 @@ JB_API int jb_scatter_unsorted(int64_t n, const float* acc4, const int64_t* perm
                                float* out_pot, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Adjoint (vector-Jacobian product) at fixed topology.                     */
+/*                                                                          */
+/* Gradient of L = sum_i w_i . acc_i w.r.t. positions and masses, with the   */
+/* COM centres differentiated: the VJP that jax.grad takes through the       */
+/* reference's differentiable_accelerations (runtime/fmm_evaluate.py:542-731,*/
+/* :1175-1250), with its analytic near-field rule (nearfield/grad.py:726-869)*/
+/* and L2P rule (operators/real_p2m_l2p.py:402-491).  Run after a forward   */
+/* pass (centres, multipoles, final locals in place), in this order:        */
+/*   jb_adj_near, jb_adj_leaf_far, jb_adj_l2l_level (deepest level first),  */
+/*   jb_adj_m2l, jb_adj_m2l_centers, jb_adj_m2m_level (root first),         */
+/*   jb_adj_p2m.  cbar4 (num_nodes float4) and mbar (num_nodes x stride)    */
+/*   start at zero; w4 is the sorted float4 cotangent (w, 0);               */
+/*   xm4[i] = (dL/dx, dL/dy, dL/dz, dL/dm) sorted.  Needs symmetric near and */
+/*   far lists (jb_tree_build emits both directions).  Orders 1..9.         */
+/* ------------------------------------------------------------------------ */
+#define JB_ADJ_MAX_ORDER_API 9
+/* P2P VJP over the leaf-evaluation units (writes xm4; split leaves use
+ * partials + split exactly as jb_leaf_eval). */
+JB_API int jb_adj_near(const float* pos4, const float* w4, int num_internal, int num_units, const int* units,
+                       const int* aux, const int* runs, const int* node_ranges, float G, float eps2, float* out_xm4,
+                       float* partials, int num_split, const int* split, void* stream);
+/* L2P VJP: lbar[leaf] = dL/dlocal, adds the particle and leaf-centre terms. */
+JB_API int jb_adj_leaf_far(int p, const float* pos4, const float* w4, int num_nodes, int num_internal,
+                           const int* node_ranges, const float* centers, const float* locals, float G, float* xm4,
+                           float* lbar, float* cbar4, void* stream);
+/* L2L VJP for parents in [first, last) (transpose of runtime/kernels/_l2l.py:210-404). */
+JB_API int jb_adj_l2l_level(int p, int first, int last, const int* left, const int* right, const float* centers,
+                            const float* locals, float* lbar, float* cbar4, void* stream);
+/* M2L VJP w.r.t. the multipoles: mbar[u] = sum_v M2L(c_v - c_u) lbar[v] over u's
+ * list, same units / partials / split as jb_m2l (transpose of _m2l.py:1483-1793). */
+JB_API int jb_adj_m2l(int p, int num_units, const int* units, const float* lbar, const float* centers,
+                      const int* far_src, float* mbar, float* partials, int num_split, const int* split,
+                      void* stream);
+/* M2L VJP w.r.t. the centres: per pair (pair_tgt[e] <- far_src[e]) the
+ * displacement derivative into g4 (num_pairs float4 scratch), then gathered
+ * into cbar4 with rev[e] = index of the reverse pair. */
+JB_API int jb_adj_m2l_centers(int p, int num_nodes, int64_t num_pairs, const int* pair_tgt, const int* far_src,
+                              const int64_t* far_off, const int* rev, const float* mult, const float* lbar,
+                              const float* centers, float* g4, float* cbar4, void* stream);
+/* M2M + COM VJP for parents in [first, last) (transpose of
+ * upward/real_tree_expansions.py:216-364 and the COM of :439). */
+JB_API int jb_adj_m2m_level(int p, int first, int last, const int* left, const int* right, const float* centers,
+                            const float* mult, float* mbar, float* cbar4, void* stream);
+/* P2M + leaf COM VJP (transpose of real_tree_expansions.py:89-213); adds into xm4. */
+JB_API int jb_adj_p2m(int p, const float* pos4, int num_nodes, int num_internal, const int* node_ranges,
+                      const float* centers, const float* mbar, const float* cbar4, float* xm4, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Verification and measurement helpers (no reference counterpart in the    */
 /* hot path; they back the error report and the roofline denominators).    */
 /* ------------------------------------------------------------------------ */

@@ -89,6 +89,13 @@ _SIGNATURES = {
     "jb_leaf_eval": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _I, _P, _P],
     "jb_leaf_eval_noalloc": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _I, _I, _P, _P],
     "jb_eval_targets": [_I, _P, _I, _P, _P, _P, _P, _P, _P, _I64, _P, _F, _F, _P, _P],
+    "jb_adj_near": [_P, _P, _I, _I, _P, _P, _P, _P, _F, _F, _P, _P, _I, _P, _P],
+    "jb_adj_leaf_far": [_I, _P, _P, _I, _I, _P, _P, _P, _F, _P, _P, _P, _P],
+    "jb_adj_l2l_level": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P],
+    "jb_adj_m2l": [_I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P],
+    "jb_adj_m2l_centers": [_I, _I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "jb_adj_m2m_level": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P],
+    "jb_adj_p2m": [_I, _P, _I, _I, _P, _P, _P, _P, _P, _P],
     "jb_scatter_unsorted": [_I64, _P, _P, _P, _P, _P],
     "jb_direct_f64": [_I64, _P, _I64, _P, _D, _D, _P, _P],
     "jb_probe_throughput": [_I, _I, _I, _P, _P],

@@ -101,6 +101,8 @@ class Pass:
                  leaf_unit_sources: int = 4096):
         if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
             raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
+        if dt.topo.max_leaf_occupancy > 32:
+            raise ValueError("the leaf kernels take at most 32 particles per leaf (use leaf_size <= 32)")
         self.dt = dt
         self.p = int(p)
         self.G = float(G)
@@ -205,6 +207,93 @@ class Pass:
         self.upward(stream)
         self.downward(stream)
         return self.evaluate(stream)
+
+    # -- adjoint --------------------------------------------------------------
+    def _adj_buffers(self):
+        if getattr(self, "_adj", None) is None:
+            t, dev, cs = self.dt.topo, self.dt.device, self.ws.stride
+            f32 = dict(device=dev, dtype=torch.float32)
+            self._adj = {
+                "w4": torch.empty((t.num_particles, 4), **f32),
+                "zeros": torch.zeros((t.num_particles,), **f32),
+                "xm4": torch.empty((t.num_particles, 4), **f32),
+                "lbar": torch.empty((t.num_nodes, cs), **f32),
+                "mbar": torch.empty((t.num_nodes, cs), **f32),
+                "cbar4": torch.empty((t.num_nodes, 4), **f32),
+                "g4": torch.empty((max(t.num_far_pairs, 1), 4), **f32),
+                "pair_tgt": torch.from_numpy(t.far_pair_targets() if t.num_far_pairs else np.zeros(1, np.int32)).to(dev),
+                "rev": torch.from_numpy(t.far_reverse_index() if t.num_far_pairs else np.zeros(1, np.int32)).to(dev),
+            }
+            if not t.near_lists_symmetric():
+                raise ValueError("the near-field adjoint needs symmetric neighbour lists")
+            # full near list of every leaf (the forward schedule may be a leaf range)
+            self._adj_sched = leaf_schedule(t, max_sources=4096)
+            up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+            self._adj["units"] = up(self._adj_sched.units)
+            self._adj["aux"] = up(self._adj_sched.aux)
+            self._adj["runs"] = up(self._adj_sched.runs)
+            self._adj["split"] = up(self._adj_sched.split)
+            self._adj["partials"] = torch.empty((max(self._adj_sched.num_slots, 1) * 32, 4), **f32)
+        return self._adj
+
+    def vjp(self, w: torch.Tensor, grad_pos: torch.Tensor, grad_mass: torch.Tensor, stream=None,
+            recompute: bool = True) -> None:
+        """Gradient of sum(w * acc) w.r.t. the input-order positions and masses
+        currently loaded (acc = the pass's accelerations, input order), written
+        into grad_pos (N,3) and grad_mass (N,).  recompute=True reruns the
+        upward and downward sweeps first (multipoles / locals are not kept from
+        the forward call); False reuses the coefficients already in the
+        workspace."""
+        if self.p > 9:
+            raise ValueError("the adjoint is built for expansion orders <= 9")
+        if self.leaf_range != (0, self.dt.topo.num_leaves):
+            raise ValueError("the adjoint runs on the whole leaf range")
+        t, dt, ws, lb, s = self.dt.topo, self.dt, self.ws, self.lib, _stream_handle(stream)
+        A = self._adj_buffers()
+        sc = self._adj_sched
+        if recompute:
+            self.upward(stream)
+            self.downward(stream)
+        w = w.to(device=dt.device, dtype=torch.float32).contiguous()
+        _lib.check(lb.jb_gather_sorted(t.num_particles, _ptr(w), _ptr(A["zeros"]), _ptr(dt.perm), _ptr(A["w4"]), s),
+                   "jb_gather_sorted(w)")
+        A["cbar4"].zero_()
+        A["mbar"].zero_()
+        _lib.check(lb.jb_adj_near(_ptr(ws.pos4), _ptr(A["w4"]), t.num_internal, int(sc.units.shape[0]),
+                                  _ptr(A["units"]), _ptr(A["aux"]), _ptr(A["runs"]), _ptr(dt.node_ranges), self.G,
+                                  self.eps2, _ptr(A["xm4"]), _ptr(A["partials"]), int(sc.split.shape[0]),
+                                  _ptr(A["split"]), s), "jb_adj_near")
+        _lib.check(lb.jb_adj_leaf_far(self.p, _ptr(ws.pos4), _ptr(A["w4"]), t.num_nodes, t.num_internal,
+                                      _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.locals), self.G,
+                                      _ptr(A["xm4"]), _ptr(A["lbar"]), _ptr(A["cbar4"]), s), "jb_adj_leaf_far")
+        lo = dt.level_offsets
+        for lev in range(t.num_levels - 1, -1, -1):
+            _lib.check(lb.jb_adj_l2l_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
+                                           _ptr(ws.centers), _ptr(ws.locals), _ptr(A["lbar"]), _ptr(A["cbar4"]), s),
+                       "jb_adj_l2l_level")
+        msc = m2l_schedule(t, max_pairs=64) if not hasattr(self, "_adj_m2l") else self._adj_m2l
+        if not hasattr(self, "_adj_m2l"):
+            self._adj_m2l = msc
+            up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dt.device)
+            A["m2l_units"], A["m2l_split"] = up(msc.units), up(msc.split)
+            A["m2l_partials"] = torch.empty((max(msc.num_slots, 1), ws.stride), device=dt.device,
+                                            dtype=torch.float32)
+        _lib.check(lb.jb_adj_m2l(self.p, int(msc.units.shape[0]), _ptr(A["m2l_units"]), _ptr(A["lbar"]),
+                                 _ptr(ws.centers), _ptr(dt.far_src), _ptr(A["mbar"]), _ptr(A["m2l_partials"]),
+                                 int(msc.split.shape[0]), _ptr(A["m2l_split"]), s), "jb_adj_m2l")
+        _lib.check(lb.jb_adj_m2l_centers(self.p, t.num_nodes, t.num_far_pairs, _ptr(A["pair_tgt"]),
+                                         _ptr(dt.far_src), _ptr(dt.far_off), _ptr(A["rev"]), _ptr(ws.mult),
+                                         _ptr(A["lbar"]), _ptr(ws.centers), _ptr(A["g4"]), _ptr(A["cbar4"]), s),
+                   "jb_adj_m2l_centers")
+        for lev in range(t.num_levels):
+            _lib.check(lb.jb_adj_m2m_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
+                                           _ptr(ws.centers), _ptr(ws.mult), _ptr(A["mbar"]), _ptr(A["cbar4"]), s),
+                       "jb_adj_m2m_level")
+        _lib.check(lb.jb_adj_p2m(self.p, _ptr(ws.pos4), t.num_nodes, t.num_internal, _ptr(dt.node_ranges),
+                                 _ptr(ws.centers), _ptr(A["mbar"]), _ptr(A["cbar4"]), _ptr(A["xm4"]), s),
+                   "jb_adj_p2m")
+        _lib.check(lb.jb_scatter_unsorted(t.num_particles, _ptr(A["xm4"]), _ptr(dt.perm), _ptr(grad_pos),
+                                          _ptr(grad_mass), s), "jb_scatter_unsorted(grad)")
 
     def launches_per_run(self) -> int:
         t = self.dt.topo

@@ -170,13 +170,22 @@ class FastMultipoleMethod:
                                      jit_traversal: bool = False, grad_plan=None, grad_config=None, out=None):
         """Re-evaluates the whole pass (P2M -> M2M -> M2L -> L2L -> L2P + P2P) on
         live positions/masses with the topology of `state` held fixed
-        (runtime/fmm_evaluate.py:733, :542-731).  Host inputs are copied to the
+        (runtime/fmm_evaluate.py:733, :542-731).  When either input is a torch
+        tensor that requires grad, the result is differentiable: its backward
+        runs the hand-written adjoint kernels (jaccpot_b200.autodiff).  Host inputs are copied to the
         device and the result copied back (into `out` when given, which may be
         a pinned host tensor); device inputs give a device result."""
         if target_indices is not None:
             raise ValueError("target_indices is not provided on the fixed-topology path")
         ps = state.pass_
         dev = state.device_topology.device
+        if (isinstance(positions, torch.Tensor) and positions.requires_grad) or (
+                isinstance(masses, torch.Tensor) and masses.requires_grad):
+            from .autodiff import fmm_accelerations
+
+            pos = positions if isinstance(positions, torch.Tensor) else _to_torch(positions, dev, torch.float32)
+            mass = masses if isinstance(masses, torch.Tensor) else _to_torch(masses, dev, torch.float32)
+            return fmm_accelerations(pos.to(dev), mass.to(dev), ps)
         host = not (isinstance(positions, torch.Tensor) and positions.is_cuda)
         pos = _to_torch(positions, dev, torch.float32) if not isinstance(positions, torch.Tensor) else positions
         mass = _to_torch(masses, dev, torch.float32) if not isinstance(masses, torch.Tensor) else masses

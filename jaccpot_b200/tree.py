@@ -52,6 +52,35 @@ class Topology:
     def num_near_pairs(self) -> int:
         return int(self.near_leaves.shape[0])
 
+    def far_pair_targets(self) -> np.ndarray:
+        """int32[num_far]: the target node of every far pair (CSR row of each entry)."""
+        return np.repeat(np.arange(self.num_nodes, dtype=np.int32), np.diff(self.far_offsets)).astype(np.int32)
+
+    def far_reverse_index(self) -> np.ndarray:
+        """int32[num_far]: index of the pair (s <- t) for every pair (t <- s).
+
+        The dual traversal emits every accepted pair in both directions, so the
+        reverse always exists; raises if it does not (the adjoint relies on it)."""
+        tgt = self.far_pair_targets().astype(np.int64)
+        src = self.far_sources.astype(np.int64)
+        key = tgt * self.num_nodes + src
+        order = np.argsort(key, kind="stable")
+        rkey = src * self.num_nodes + tgt
+        pos = np.searchsorted(key[order], rkey)
+        pos = np.minimum(pos, max(key.size - 1, 0))
+        rev = order[pos] if key.size else np.zeros(0, np.int64)
+        if key.size and not np.array_equal(key[rev], rkey):
+            raise ValueError("far lists are not symmetric")
+        return rev.astype(np.int32)
+
+    def near_lists_symmetric(self) -> bool:
+        """True when leaf B is in A's neighbour list exactly when A is in B's."""
+        tgt = np.repeat(np.arange(self.num_leaves, dtype=np.int64), np.diff(self.near_offsets))
+        src = self.near_leaves.astype(np.int64)
+        a = np.sort(tgt * self.num_leaves + src)
+        b = np.sort(src * self.num_leaves + tgt)
+        return bool(np.array_equal(a, b))
+
     def near_pair_interactions(self) -> int:
         """Particle-particle interactions of the near field (self blocks included)."""
         cnt = (self.node_ranges[:, 1] - self.node_ranges[:, 0] + 1).astype(np.int64)
