@@ -152,6 +152,19 @@ JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float*
                   const int* far_src, float* locals, float* partials, int num_split, const int* split,
                   void* stream);
 
+/* Far field with a per-pair expansion order (gear): the reference's
+ * adaptive-order downward sweep, which buckets far pairs by gear and runs
+ * each bucket's M2L at that gear's order (runtime/fmm_prepare.py:2400-2480,
+ * _bucket_far_pairs_by_level_split).  Units (as jb_m2l) are grouped by gear:
+ * units[gear_unit_offsets[g] .. gear_unit_offsets[g+1]) run at order
+ * gear_orders[g] <= p_max (HOST arrays, num_gears entries / num_gears+1);
+ * far_src is the source list regrouped so no unit mixes gears.  Rows of
+ * mult / locals / partials have stride jb_coeff_stride(p_max); a gear reads
+ * the degrees <= its order and writes zeros above them. */
+JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orders, const int64_t* gear_unit_offsets,
+                        const int* units, const float* mult, const float* centers, const int* far_src,
+                        float* locals, float* partials, int num_split, const int* split, void* stream);
+
 /* Downward sweep, one level: for each internal node in [first, last), adds
  * l2l(parent) to both children (l2l_real, operators/real_translations.py:604;
  * _propagate_solidfmm_locals_by_level, runtime/kernels/_l2l.py:210-404). */
@@ -257,6 +270,45 @@ JB_API int jb_adj_m2m_level(int p, int first, int last, const int* left, const i
 /* P2M + leaf COM VJP (transpose of real_tree_expansions.py:89-213); adds into xm4. */
 JB_API int jb_adj_p2m(int p, const float* pos4, int num_nodes, int num_internal, const int* node_ranges,
                       const float* centers, const float* mbar, const float* cbar4, float* xm4, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Learned gear selector (replaces the analytic per-pair order policy of     */
+/* runtime/_adaptive_policy.py:249-372 that feeds the gear buckets of         */
+/* runtime/fmm_prepare.py:2400-2480).  MLP 12 -> 64 -> 64 -> 4, GELU, BF16    */
+/* weights (FP32 values rounded to BF16), FP32 accumulation; gears are the    */
+/* orders (2, 4, 6, 8).  Parameter vector layout: W1[64][12] b1[64]           */
+/* W2[64][64] b2[64] W3[4][64] b3[4].                                         */
+/* ------------------------------------------------------------------------ */
+JB_API int jb_gear_param_count(void);
+/* Per node: 8 log per-degree multipole powers (node_feat, num_nodes x 8) and
+ * the smallest particle force magnitude under the node (scale) from a
+ * previous pass's sorted acc4; level_offsets_host is a HOST array. */
+JB_API int jb_gear_node_features(int p, int num_nodes, int num_internal, const int* left, const int* right,
+                                 const int* level_offsets_host, int num_levels, const int* node_ranges,
+                                 const float* mult, const float* centers, const float* radii, const float* acc4,
+                                 float* node_feat, float* scale, void* stream);
+/* 12 features per far pair (pair_ids NULL = all pairs, else n selected ids). */
+JB_API int jb_gear_pair_features(int64_t n, const int64_t* pair_ids, const int* pair_tgt, const int* far_src,
+                                 const float* centers, const float* radii, const float* node_feat,
+                                 const float* scale, float G, float* out, void* stream);
+/* Training labels: log10(force error / target force scale) of each gear's M2L
+ * against the order-10 M2L (mult10: order-10 multipoles), n x 4. */
+JB_API int jb_gear_errors(int64_t n, const int64_t* pair_ids, const int* pair_tgt, const int* far_src,
+                          const float* mult10, const float* centers, const float* radii, const float* scale, float G,
+                          float* out, void* stream);
+/* One batch's parameter gradients (softmax cross-entropy on the gear label):
+ * block b writes gpart[b][param_count] and lpart[b] (ceil(n/128) blocks). */
+JB_API int jb_gear_train_grad(int n, const float* X, const int* labels, const float* Wq, float* gpart, float* lpart,
+                              void* stream);
+/* Adam step on FP32 master weights; Wq = BF16-rounded copy. */
+JB_API int jb_gear_adam(int nblocks, const float* gpart, float inv_batch, float lr, float beta1, float beta2,
+                        float eps, int step, float* master, float* m1, float* m2, float* Wq, void* stream);
+/* Fused inference per far pair: features, normalisation ((x - norm[k]) *
+ * norm[12 + k]), MLP, gear = lowest g with P(label <= g) >= conf, or the
+ * highest gear when the top probability is below min_top. */
+JB_API int jb_gear_select(int64_t n, const int* pair_tgt, const int* far_src, const float* centers,
+                          const float* radii, const float* node_feat, const float* scale, float G, const float* Wq,
+                          const float* norm, float conf, float min_top, int* gear_out, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Verification and measurement helpers (no reference counterpart in the    */

@@ -85,6 +85,7 @@ _SIGNATURES = {
     "jb_p2m": [_I, _P, _I, _I, _P, _P, _P, _P],
     "jb_m2m_level": [_I, _I, _I, _P, _P, _P, _P, _P],
     "jb_m2l": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P],
+    "jb_m2l_gears": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_l2l_level": [_I, _I, _I, _P, _P, _P, _P, _P],
     "jb_leaf_eval": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _I, _P, _P],
     "jb_leaf_eval_noalloc": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _I, _I, _P, _P],
@@ -96,6 +97,13 @@ _SIGNATURES = {
     "jb_adj_m2l_centers": [_I, _I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "jb_adj_m2m_level": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P],
     "jb_adj_p2m": [_I, _P, _I, _I, _P, _P, _P, _P, _P, _P],
+    "jb_gear_param_count": [],
+    "jb_gear_node_features": [_I, _I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P],
+    "jb_gear_pair_features": [_I64, _P, _P, _P, _P, _P, _P, _P, _F, _P, _P],
+    "jb_gear_errors": [_I64, _P, _P, _P, _P, _P, _P, _P, _F, _P, _P],
+    "jb_gear_train_grad": [_I, _P, _P, _P, _P, _P, _P],
+    "jb_gear_adam": [_I, _P, _F, _F, _F, _F, _F, _I, _P, _P, _P, _P, _P],
+    "jb_gear_select": [_I64, _P, _P, _P, _P, _P, _P, _F, _P, _P, _F, _F, _P, _P],
     "jb_scatter_unsorted": [_I64, _P, _P, _P, _P, _P],
     "jb_direct_f64": [_I64, _P, _I64, _P, _D, _D, _P, _P],
     "jb_probe_throughput": [_I, _I, _I, _P, _P],

@@ -74,7 +74,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         src = CSRC / "fmm_order.cu"
         if _stale(obj, _deps(src)):
             jobs_todo.append([nvcc, *NVCC_FLAGS, f"-DJB_ORDER={p}", "-c", str(src), "-o", str(obj)])
-    for name in ("fmm_capi", "fmm_noalloc", "m2l_tc"):
+    for name in ("fmm_capi", "fmm_noalloc", "fmm_gears", "m2l_tc"):
         src = CSRC / f"{name}.cu"
         if not src.exists():
             continue

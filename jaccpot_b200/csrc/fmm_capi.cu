@@ -357,6 +357,32 @@ JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float*
                           ST(stream));
 }
 
+JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orders, const int64_t* gear_unit_offsets,
+                        const int* units, const float* mult, const float* centers, const int* far_src,
+                        float* locals, float* partials, int num_split, const int* split, void* stream) {
+  if (p_max < 1 || p_max > JB_MAX_ORDER) return JB_ERR_ORDER;
+  if (num_gears < 1 || !gear_orders || !gear_unit_offsets || num_split < 0 || (num_split > 0 && (!split || !partials)))
+    return JB_ERR_ARG;
+  if (mode != JB_M2L_FP32) return JB_ERR_UNSUPPORTED;
+  const int rs = cstride(p_max);
+  for (int g = 0; g < num_gears; ++g) {
+    const int pg = gear_orders[g];
+    const int64_t u0 = gear_unit_offsets[g], u1 = gear_unit_offsets[g + 1];
+    if (pg < 1 || pg > p_max || u0 < 0 || u1 < u0) return JB_ERR_ARG;
+    if (u1 == u0) continue;
+    if (!units || !mult || !centers || !far_src || !locals) return JB_ERR_ARG;
+    const int rc = dispatch<RunM2L>(pg, (int)(u1 - u0), units + 4 * u0, mult, centers, far_src, locals, partials, 0,
+                                    (const int*)nullptr, ST(stream), false, rs);
+    if (rc) return rc;
+  }
+  if (num_split > 0) {
+    k_m2l_reduce<<<blocks_1d((int64_t)num_split * rs, 256), 256, 0, ST(stream)>>>(
+        num_split, reinterpret_cast<const int4*>(split), partials, locals, rs);
+    return launch_status();
+  }
+  return JB_OK;
+}
+
 JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* right, const float* centers,
                         float* locals, void* stream) {
   if (first < 0 || last < first || (last > first && (!left || !right || !centers || !locals))) return JB_ERR_ARG;

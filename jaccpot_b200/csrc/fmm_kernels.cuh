@@ -199,7 +199,9 @@ __global__ void __launch_bounds__(kM2LThreads, 3) k_m2l_units(int num_units, con
                                                               const float4* __restrict__ centers,
                                                               const int* __restrict__ far_src,
                                                               float* __restrict__ locals,
-                                                              float* __restrict__ partials) {
+                                                              float* __restrict__ partials, int rs) {
+  // rs: row stride (floats) of mult / locals / partials, >= cstride(P); a
+  // lower-order pass (gear) reads the prefix of each row (degrees <= P).
   constexpr int C = csize(P), CS = cstride(P), R4 = row4(P);
   extern __shared__ float4 m2l_smem[];
   float4* row = m2l_smem + threadIdx.x * R4;
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(kM2LThreads, 3) k_m2l_units(int num_units, con
   const float4 ct = centers[tgt];
   int s = far_src[e0];
   {
-    const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s * CS);
+    const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s * rs);
 #pragma unroll
     for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
     cp_async_commit();
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(kM2LThreads, 3) k_m2l_units(int num_units, con
     const bool more = e + 1 < e1;
     const int sn = more ? __ldg(far_src + e + 1) : s;
     if (more) {
-      const float4* src = reinterpret_cast<const float4*>(mult + (size_t)sn * CS);
+      const float4* src = reinterpret_cast<const float4*>(mult + (size_t)sn * rs);
 #pragma unroll
       for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
       cp_async_commit();
@@ -247,19 +249,17 @@ __global__ void __launch_bounds__(kM2LThreads, 3) k_m2l_units(int num_units, con
     s = sn;
     cs = csn;
   }
-  float* dst = (slot < 0) ? locals + (size_t)tgt * CS : partials + (size_t)slot * CS;
+  float* dst = (slot < 0) ? locals + (size_t)tgt * rs : partials + (size_t)slot * rs;
 #pragma unroll
   for (int k = 0; k < C; ++k) dst[k] = sacc[k * kM2LThreads + threadIdx.x];
-#pragma unroll
-  for (int k = C; k < CS; ++k) dst[k] = 0.f;
+  for (int k = C; k < rs; ++k) dst[k] = 0.f;
 }
 
 // Sums the partial rows of targets whose list was split: split[i] =
 // (target, first slot, number of slots, unused).  Thread per (target, coefficient).
-template <int P>
-__global__ void __launch_bounds__(256) k_m2l_reduce(int num_split, const int4* __restrict__ split,
-                                                    const float* __restrict__ partials, float* __restrict__ locals) {
-  constexpr int CS = cstride(P);
+static __global__ void __launch_bounds__(256) k_m2l_reduce(int num_split, const int4* __restrict__ split,
+                                                           const float* __restrict__ partials,
+                                                           float* __restrict__ locals, int CS) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (int)(t / CS), k = (int)(t % CS);
   if (i >= num_split) return;
@@ -562,20 +562,22 @@ struct RunM2M {
 template <int P>
 struct RunM2L {
   static int run(int num_units, const int* units, const float* mult, const float* centers, const int* far_src,
-                 float* locals, float* partials, int num_split, const int* split, cudaStream_t st, bool neg = false) {
+                 float* locals, float* partials, int num_split, const int* split, cudaStream_t st, bool neg = false,
+                 int rs = 0) {
+    if (rs <= 0) rs = cstride(P);
     if (num_units > 0) {
       const size_t sm = sizeof(float4) * kM2LThreads * row4(P) + sizeof(float) * csize(P) * kM2LThreads;
       auto kern = neg ? k_m2l_units<P, true> : k_m2l_units<P, false>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
           num_units, reinterpret_cast<const int4*>(units), mult, reinterpret_cast<const float4*>(centers), far_src,
-          locals, partials);
+          locals, partials, rs);
       const int rc = launch_status();
       if (rc) return rc;
     }
     if (num_split > 0) {
-      k_m2l_reduce<P><<<blocks_for((int64_t)num_split * cstride(P), 256), 256, 0, st>>>(
-          num_split, reinterpret_cast<const int4*>(split), partials, locals);
+      k_m2l_reduce<<<blocks_for((int64_t)num_split * rs, 256), 256, 0, st>>>(
+          num_split, reinterpret_cast<const int4*>(split), partials, locals, rs);
       return launch_status();
     }
     return JB_OK;

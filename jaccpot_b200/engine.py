@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .schedule import leaf_schedule, m2l_schedule
+from .schedule import gear_m2l_schedule, leaf_schedule, m2l_schedule
 from .tree import Topology
 
 
@@ -154,9 +154,37 @@ class Pass:
             _lib.check(self.lib.jb_m2m_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
                                              _ptr(ws.centers), _ptr(ws.mult), s), "jb_m2m_level")
 
+    def set_gears(self, gears, orders) -> None:
+        """Per-far-pair expansion orders: gears[e] indexes `orders` for pair e
+        of the CSR far list (None restores the single maximum order)."""
+        if gears is None:
+            self.gear_sched = None
+            return
+        orders = tuple(int(o) for o in orders)
+        if max(orders) > self.p or min(orders) < 1:
+            raise ValueError(f"gear orders must lie in [1, {self.p}]")
+        gs = gear_m2l_schedule(self.dt.topo, np.asarray(gears), orders)
+        dev = self.dt.device
+        up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+        self.gear_sched = gs
+        self.d_gear_units = up(gs.units)
+        self.d_gear_split = up(gs.split)
+        self.d_gear_src = up(gs.far_src)
+        self.h_gear_orders = np.ascontiguousarray(np.array(orders, dtype=np.int32))
+        self.h_gear_offsets = np.ascontiguousarray(gs.gear_offsets.astype(np.int64))
+        self.gear_partials = torch.empty((max(gs.num_slots, 1), self.ws.stride), device=dev, dtype=torch.float32)
+
     def m2l(self, stream=None) -> None:
         ws, s, sc = self.ws, _stream_handle(stream), self.m2l_sched
         ws.locals.zero_()
+        gs = getattr(self, "gear_sched", None)
+        if gs is not None:
+            _lib.check(self.lib.jb_m2l_gears(
+                self.p, self.m2l_mode, len(gs.orders), self.h_gear_orders.ctypes.data,
+                self.h_gear_offsets.ctypes.data, _ptr(self.d_gear_units), _ptr(ws.mult), _ptr(ws.centers),
+                _ptr(self.d_gear_src), _ptr(ws.locals), _ptr(self.gear_partials), int(gs.split.shape[0]),
+                _ptr(self.d_gear_split), s), "jb_m2l_gears")
+            return
         _lib.check(self.lib.jb_m2l(self.p, self.m2l_mode, int(sc.units.shape[0]), _ptr(self.d_m2l_units),
                                    _ptr(ws.mult), _ptr(ws.centers), _ptr(self.dt.far_src), _ptr(ws.locals),
                                    _ptr(self.m2l_partials), int(sc.split.shape[0]), _ptr(self.d_m2l_split), s),

@@ -1,0 +1,353 @@
+"""Learned gear selector: per-far-pair expansion order chosen by a small MLP.
+
+The reference's adaptive-order mode (``FastMultipoleMethod(adaptive_order=
+True, p_gears=...)``) tags every far pair with a gear from an analytic error
+proxy (runtime/_adaptive_policy.py:249-372) and runs the downward sweep
+bucketed by gear (runtime/fmm_prepare.py:2400-2480).  Here the tags come from
+a 12 -> 64 -> 64 -> 4 GELU network (BF16 weights, FP32 accumulation) whose
+training data are errors the FMM itself makes:
+
+* samples: far pairs of clustered systems (16 seeds at N = 262,144 by
+  default); features per pair (``jb_gear_pair_features``): opening ratio,
+  target share of it, 8 per-degree log multipole powers of the source, log
+  target/source mass, log target force scale in units of the source's
+  monopole field;
+* labels: the lowest gear whose M2L force error against the order-10 M2L of
+  the same multipole, on the near and far side of the target's bounding
+  sphere, is within ``budget`` times the smallest particle force in the target
+  node (``jb_gear_errors``);
+* training: softmax cross-entropy, Adam, hand-written kernels
+  (``jb_gear_train_grad`` / ``jb_gear_adam``);
+* inference (``jb_gear_select``, fused features + MLP per pair): the lowest
+  gear g with P(label <= g) >= conf; the highest gear (plain maximum order)
+  when the network's top probability is below ``min_top``.
+
+The force scale comes from a previous evaluation (the plain pass run by
+``prepare_state``), as the reference's policy takes it from
+``compute_node_force_scale_from_sorted_acc`` (_adaptive_policy.py:402).
+"""
+
+from __future__ import annotations
+
+import json
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib, engine, tree, workloads
+
+ORDERS = (2, 4, 6, 8)
+N_IN, N_OUT = 12, 4
+N_PARAMS = 5252
+DATA = Path(__file__).resolve().parent / "data"
+DEFAULT_MODEL = DATA / "gear_mlp_p8.npz"
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+@dataclass
+class GearModel:
+    params: np.ndarray  # float32[5252], BF16-rounded values
+    norm: np.ndarray  # float32[24]: feature means, then 1/std
+    budget: float = 1e-5
+    conf: float = 0.95
+    min_top: float = 0.5
+    orders: tuple = ORDERS
+    info: dict = field(default_factory=dict)
+
+    def save(self, path: Path) -> None:
+        path = Path(path)
+        path.parent.mkdir(parents=True, exist_ok=True)
+        np.savez(path, params=self.params, norm=self.norm, budget=self.budget, conf=self.conf,
+                 min_top=self.min_top, orders=np.array(self.orders), info=json.dumps(self.info))
+
+    @staticmethod
+    def load(path: Path = DEFAULT_MODEL) -> "GearModel":
+        d = np.load(Path(path))
+        return GearModel(params=d["params"].astype(np.float32), norm=d["norm"].astype(np.float32),
+                         budget=float(d["budget"]), conf=float(d["conf"]), min_top=float(d["min_top"]),
+                         orders=tuple(int(o) for o in d["orders"]), info=json.loads(str(d["info"])))
+
+
+class GearContext:
+    """Device-side per-topology data the selector needs (radii, pair targets)."""
+
+    def __init__(self, ps: engine.Pass):
+        t = ps.dt.topo
+        dev = ps.dt.device
+        self.ps = ps
+        self.radii = torch.from_numpy(t.radii_f64.astype(np.float32)).to(dev)
+        self.pair_tgt = torch.from_numpy(t.far_pair_targets() if t.num_far_pairs else np.zeros(1, np.int32)).to(dev)
+        self.node_feat = torch.empty((t.num_nodes, 8), device=dev, dtype=torch.float32)
+        self.scale = torch.empty((t.num_nodes,), device=dev, dtype=torch.float32)
+        self.h_levels = np.ascontiguousarray(t.level_offsets.astype(np.int32))
+
+    def node_features(self) -> None:
+        """From the multipoles / centres / sorted acc4 currently in the workspace."""
+        ps, t, ws = self.ps, self.ps.dt.topo, self.ps.ws
+        _lib.check(_lib.lib().jb_gear_node_features(
+            ps.p, t.num_nodes, t.num_internal, _ptr(ps.dt.left), _ptr(ps.dt.right), self.h_levels.ctypes.data,
+            t.num_levels, _ptr(ps.dt.node_ranges), _ptr(ws.mult), _ptr(ws.centers), _ptr(self.radii),
+            _ptr(ws.acc4), _ptr(self.node_feat), _ptr(self.scale), _stream()), "jb_gear_node_features")
+
+    def pair_features(self, pair_ids: torch.Tensor | None = None) -> torch.Tensor:
+        t = self.ps.dt.topo
+        n = t.num_far_pairs if pair_ids is None else int(pair_ids.shape[0])
+        out = torch.empty((max(n, 1), N_IN), device=self.ps.dt.device, dtype=torch.float32)
+        _lib.check(_lib.lib().jb_gear_pair_features(
+            n, _ptr(pair_ids), _ptr(self.pair_tgt), _ptr(self.ps.dt.far_src), _ptr(self.ps.ws.centers),
+            _ptr(self.radii), _ptr(self.node_feat), _ptr(self.scale), self.ps.G, _ptr(out), _stream()),
+            "jb_gear_pair_features")
+        return out[:n]
+
+    def select(self, model: GearModel) -> torch.Tensor:
+        t = self.ps.dt.topo
+        dev = self.ps.dt.device
+        n = t.num_far_pairs
+        gear = torch.empty((max(n, 1),), device=dev, dtype=torch.int32)
+        W = torch.from_numpy(model.params).to(dev)
+        nrm = torch.from_numpy(model.norm).to(dev)
+        _lib.check(_lib.lib().jb_gear_select(
+            n, _ptr(self.pair_tgt), _ptr(self.ps.dt.far_src), _ptr(self.ps.ws.centers), _ptr(self.radii),
+            _ptr(self.node_feat), _ptr(self.scale), self.ps.G, _ptr(W), _ptr(nrm), float(model.conf),
+            float(model.min_top), _ptr(gear), _stream()), "jb_gear_select")
+        return gear[:n]
+
+
+def apply_gears(ps: engine.Pass, model: GearModel) -> np.ndarray:
+    """Runs the plain pass on the loaded particles (force scale), selects the
+    gears with the network and installs them on ``ps``; returns them."""
+    if ps.p != max(model.orders):
+        raise ValueError(f"the selector's top gear is {max(model.orders)}, the pass order is {ps.p}")
+    ps.set_gears(None, None)
+    ps.run()
+    ctx = GearContext(ps)
+    ctx.node_features()
+    gears = ctx.select(model).cpu().numpy()
+    ps.set_gears(gears, model.orders)
+    return gears
+
+
+# ---------------------------------------------------------------------------
+# Training data
+# ---------------------------------------------------------------------------
+def make_samples(seed: int, n: int = 262144, per_seed: int = 131072, leaf_size: int = 32, theta: float = 0.6,
+                 G: float = 1.0, generator: str = "clustered", device="cuda"):
+    """Features (m, 12) and per-gear log10 relative errors (m, 4) for `per_seed`
+    far pairs of one seeded system."""
+    pos, mass = workloads.GENERATORS[generator](n, seed)
+    topo = tree.build_topology(pos, mass, leaf_size=leaf_size, theta=theta)
+    dt = engine.DeviceTopology(topo, device)
+    d_pos, d_mass = torch.from_numpy(pos).to(device), torch.from_numpy(mass).to(device)
+    ps = engine.Pass(dt, 8, G=G, eps2=0.0)
+    ps.load_particles(d_pos, d_mass)
+    ps.run()
+    ctx = GearContext(ps)
+    ctx.node_features()
+    p10 = engine.Pass(dt, 10, G=G, eps2=0.0)
+    p10.load_particles(d_pos, d_mass)
+    p10.upward()
+    rng = np.random.default_rng(1000 + seed)
+    m = min(per_seed, topo.num_far_pairs)
+    ids = torch.from_numpy(np.sort(rng.choice(topo.num_far_pairs, m, replace=False)).astype(np.int64)).to(device)
+    X = ctx.pair_features(ids)
+    Y = torch.empty((m, N_OUT), device=device, dtype=torch.float32)
+    _lib.check(_lib.lib().jb_gear_errors(m, _ptr(ids), _ptr(ctx.pair_tgt), _ptr(dt.far_src), _ptr(p10.ws.mult),
+                                         _ptr(ps.ws.centers), _ptr(ctx.radii), _ptr(ctx.scale), G, _ptr(Y),
+                                         _stream()), "jb_gear_errors")
+    torch.cuda.synchronize()
+    return X.cpu().numpy(), Y.cpu().numpy()
+
+
+def labels_for(Y: np.ndarray, budget: float) -> np.ndarray:
+    """Lowest gear whose log10 relative error is within budget (else the top gear)."""
+    ok = Y <= np.log10(budget)
+    lab = np.argmax(ok, axis=1)
+    lab[~ok.any(axis=1)] = Y.shape[1] - 1
+    return lab.astype(np.int32)
+
+
+# ---------------------------------------------------------------------------
+# Training (hand-written kernels)
+# ---------------------------------------------------------------------------
+def init_params(rng: np.random.Generator) -> np.ndarray:
+    w = np.zeros(N_PARAMS, np.float32)
+    o = 0
+    for fan_in, fan_out in ((N_IN, 64), (64, 64), (64, N_OUT)):
+        w[o:o + fan_in * fan_out] = rng.normal(0.0, np.sqrt(2.0 / fan_in), fan_in * fan_out)
+        o += fan_in * fan_out + fan_out
+    return w
+
+
+def bf16_round(a: np.ndarray) -> np.ndarray:
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def train(X: np.ndarray, labels: np.ndarray, epochs: int = 8, batch: int = 4096, lr: float = 2e-3, seed: int = 0,
+          device="cuda", log=None) -> tuple[np.ndarray, np.ndarray, list]:
+    """Trains on the GPU; returns (BF16-rounded params, normalisation, loss history)."""
+    rng = np.random.default_rng(seed)
+    mean = X.mean(axis=0)
+    std = X.std(axis=0)
+    std[std < 1e-6] = 1.0
+    norm = np.concatenate([mean, 1.0 / std]).astype(np.float32)
+    Xn = ((X - mean) / std).astype(np.float32)
+    dev = torch.device(device)
+    dX = torch.from_numpy(Xn).to(dev)
+    dL = torch.from_numpy(labels.astype(np.int32)).to(dev)
+    master = torch.from_numpy(init_params(rng)).to(dev)
+    Wq = torch.from_numpy(bf16_round(master.cpu().numpy())).to(dev)
+    m1 = torch.zeros_like(master)
+    m2 = torch.zeros_like(master)
+    nb = (batch + 127) // 128
+    gpart = torch.empty((nb, N_PARAMS), device=dev, dtype=torch.float32)
+    lpart = torch.empty((nb,), device=dev, dtype=torch.float32)
+    lb = _lib.lib()
+    n = Xn.shape[0]
+    step = 0
+    hist = []
+    for ep in range(epochs):
+        perm = torch.from_numpy(rng.permutation(n)).to(dev)
+        Xs, Ls = dX[perm].contiguous(), dL[perm].contiguous()
+        tot = 0.0
+        for a in range(0, n - batch + 1, batch):
+            step += 1
+            xb, lbl = Xs[a:a + batch], Ls[a:a + batch]
+            _lib.check(lb.jb_gear_train_grad(batch, _ptr(xb), _ptr(lbl), _ptr(Wq), _ptr(gpart), _ptr(lpart),
+                                             _stream()), "jb_gear_train_grad")
+            lr_t = lr * (0.5 * (1 + np.cos(np.pi * ep / epochs)))
+            _lib.check(lb.jb_gear_adam(nb, _ptr(gpart), 1.0 / batch, float(lr_t), 0.9, 0.999, 1e-8, step,
+                                       _ptr(master), _ptr(m1), _ptr(m2), _ptr(Wq), _stream()), "jb_gear_adam")
+            tot += float(lpart.sum())
+        hist.append(tot / max(1, (n // batch) * batch))
+        if log:
+            log(f"epoch {ep}: loss {hist[-1]:.4f}")
+    return Wq.cpu().numpy(), norm, hist
+
+
+def predict(model: GearModel, X: np.ndarray) -> np.ndarray:
+    """Host-side gear choice from features (same rule as jb_gear_select), for analysis."""
+    W = model.params.astype(np.float64)
+    x = (X - model.norm[:N_IN]) * model.norm[N_IN:]
+    from scipy.special import erf
+
+    gelu = lambda v: 0.5 * v * (1 + erf(v / np.sqrt(2.0)))
+    o = 0
+    W1 = W[o:o + 768].reshape(64, 12); o += 768
+    b1 = W[o:o + 64]; o += 64
+    W2 = W[o:o + 4096].reshape(64, 64); o += 4096
+    b2 = W[o:o + 64]; o += 64
+    W3 = W[o:o + 256].reshape(4, 64); o += 256
+    b3 = W[o:o + 4]
+    h1 = gelu(x @ W1.T + b1)
+    h2 = gelu(h1 @ W2.T + b2)
+    z = h2 @ W3.T + b3
+    pr = np.exp(z - z.max(1, keepdims=True))
+    pr /= pr.sum(1, keepdims=True)
+    cum = np.cumsum(pr, axis=1)
+    g = np.argmax(cum >= model.conf, axis=1)
+    g[pr.max(1) < model.min_top] = N_OUT - 1
+    return g
+
+
+# ---------------------------------------------------------------------------
+# Validation and the training driver
+# ---------------------------------------------------------------------------
+def evaluate_system(model: GearModel | None, seed: int, n: int = 262144, leaf_size: int = 32, theta: float = 0.6,
+                    targets: int = 4096, generator: str = "clustered", device="cuda", repeats: int = 5) -> dict:
+    """p99 relative force error vs FP64 direct sum and the M2L time of the
+    plain maximum-order pass and (if `model`) of the gear pass on one system."""
+    pos, mass = workloads.GENERATORS[generator](n, seed)
+    topo = tree.build_topology(pos, mass, leaf_size=leaf_size, theta=theta)
+    dt = engine.DeviceTopology(topo, device)
+    ps = engine.Pass(dt, 8, G=1.0, eps2=0.0)
+    ps.load_particles(torch.from_numpy(pos).to(device), torch.from_numpy(mass).to(device))
+    rng = np.random.default_rng(99)
+    tg = rng.choice(n, size=min(targets, n), replace=False)
+    ts = torch.from_numpy(topo.inverse_permutation[tg].astype(np.int32)).to(device)
+    ref = torch.empty((tg.size, 4), device=device, dtype=torch.float64)
+    _lib.check(_lib.lib().jb_direct_f64(n, _ptr(ps.ws.pos4), tg.size, _ptr(ts), 1.0, 0.0, _ptr(ref), _stream()),
+               "jb_direct_f64")
+    ref_np = ref[:, :3].cpu().numpy()
+
+    def run_and_err():
+        ps.run()
+        got = ps.ws.acc4[ts.long(), :3].double().cpu().numpy()
+        e = workloads.relative_errors(got, ref_np)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        times = []
+        for _ in range(repeats):
+            ev[0].record()
+            ps.m2l()
+            ev[1].record()
+            torch.cuda.synchronize()
+            times.append(ev[0].elapsed_time(ev[1]))
+        return float(np.percentile(e, 99)), float(np.median(times))
+
+    out = {"far_pairs": topo.num_far_pairs}
+    out["plain_p99"], out["plain_m2l_ms"] = run_and_err()
+    if model is not None:
+        gears = apply_gears(ps, model)
+        out["gear_fraction"] = (np.bincount(gears, minlength=len(model.orders)) / max(1, gears.size)).tolist()
+        out["gear_p99"], out["gear_m2l_ms"] = run_and_err()
+        ps.set_gears(None, None)
+    return out
+
+
+def main(argv=None):
+    import argparse
+
+    ap = argparse.ArgumentParser(description="train the gear selector on the GPU")
+    ap.add_argument("--seeds", type=int, default=16)
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--per-seed", type=int, default=131072)
+    ap.add_argument("--budgets", default="3e-5,1e-5,5e-6,2e-6,1e-6")
+    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--val-seed", type=int, default=100)
+    ap.add_argument("--target-p99", type=float, default=0.97e-4)
+    ap.add_argument("--out", default=str(DEFAULT_MODEL))
+    args = ap.parse_args(argv)
+    Xs, Ys = [], []
+    for s in range(args.seeds):
+        X, Y = make_samples(s, n=args.n, per_seed=args.per_seed)
+        Xs.append(X)
+        Ys.append(Y)
+        print(f"seed {s}: {X.shape[0]} samples", flush=True)
+    X, Y = np.concatenate(Xs), np.concatenate(Ys)
+    best = None
+    for b in sorted((float(v) for v in args.budgets.split(",")), reverse=True):
+        lab = labels_for(Y, b)
+        Wq, norm, hist = train(X, lab, epochs=args.epochs, log=None)
+        model = GearModel(params=Wq, norm=norm, budget=b)
+        pred = predict(model, X[:200000])
+        acc = float((pred == lab[:200000]).mean())
+        under = float((pred < lab[:200000]).mean())
+        val = evaluate_system(model, args.val_seed, n=args.n)
+        print(f"budget {b:.1e}: label fractions {np.bincount(lab, minlength=4) / lab.size}, loss {hist[-1]:.4f}, "
+              f"train acc {acc:.3f}, under-predicted {under:.4f}, val {val}", flush=True)
+        model.info = {"samples": int(X.shape[0]), "seeds": args.seeds, "n": args.n, "epochs": args.epochs,
+                      "final_loss": hist[-1], "train_accuracy": acc, "under_predicted": under, "validation": val,
+                      "label_fractions": (np.bincount(lab, minlength=4) / lab.size).tolist()}
+        # the gears may not make the error worse than the plain pass's by more
+        # than 2%, nor push it over the target when the plain pass meets it
+        if val["gear_p99"] <= max(args.target_p99, 1.02 * val["plain_p99"]):
+            best = model
+            break
+    if best is None:
+        raise SystemExit("no budget met the validation error target")
+    best.save(Path(args.out))
+    print(f"saved {args.out} (budget {best.budget:.1e})", flush=True)
+
+
+if __name__ == "__main__":
+    main()

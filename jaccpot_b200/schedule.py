@@ -70,6 +70,72 @@ def m2l_schedule(topo: Topology, max_pairs: int = 64, targets: np.ndarray | None
     return M2LSchedule(units, np.ascontiguousarray(split), int((slot >= 0).sum()))
 
 
+@dataclass
+class GearM2LSchedule:
+    """M2L units when every far pair carries its own expansion order (gear).
+
+    ``far_src`` is the CSR source list with each target's pairs regrouped by
+    gear (stable); ``units`` (target, first, end, slot) index it and never mix
+    gears; ``gear_offsets[g]:gear_offsets[g+1]`` are the units of gear g (one
+    launch each, at that gear's order).  Targets covered by more than one unit
+    write scratch slots that ``split`` sums in slot order."""
+
+    units: np.ndarray  # int32[U, 4]
+    split: np.ndarray  # int32[S, 4]
+    num_slots: int
+    far_src: np.ndarray  # int32[num_far] regrouped sources
+    gear_offsets: np.ndarray  # int64[G + 1]
+    orders: tuple
+    pairs_per_gear: np.ndarray  # int64[G]
+
+
+def gear_m2l_schedule(topo: Topology, gears: np.ndarray, orders, max_pairs: int = 64) -> GearM2LSchedule:
+    gears = np.asarray(gears, dtype=np.int64).reshape(-1)
+    if gears.shape[0] != topo.num_far_pairs:
+        raise ValueError("one gear per far pair is required")
+    ng = len(orders)
+    if gears.size and (gears.min() < 0 or gears.max() >= ng):
+        raise ValueError("gear index out of range")
+    off = topo.far_offsets
+    tgt = np.repeat(np.arange(topo.num_nodes, dtype=np.int64), np.diff(off))
+    order = np.lexsort((gears, tgt))  # by target, then gear (stable inside)
+    far_src = topo.far_sources[order].astype(np.int32)
+    g_sorted = gears[order]
+    t_sorted = tgt[order]
+    if order.size == 0:
+        z4 = np.zeros((0, 4), np.int32)
+        return GearM2LSchedule(z4, z4, 0, far_src, np.zeros(ng + 1, np.int64), tuple(orders), np.zeros(ng, np.int64))
+    brk = np.ones(order.size, dtype=bool)
+    brk[1:] = (t_sorted[1:] != t_sorted[:-1]) | (g_sorted[1:] != g_sorted[:-1])
+    seg_start = np.nonzero(brk)[0]
+    seg_end = np.concatenate([seg_start[1:], [order.size]])
+    seg_t, seg_g = t_sorted[seg_start], g_sorted[seg_start]
+    cnt = seg_end - seg_start
+    nu = (cnt + max_pairs - 1) // max_pairs
+    rep = np.repeat(np.arange(seg_start.size), nu)
+    k = np.arange(int(nu.sum())) - np.repeat(np.cumsum(nu) - nu, nu)
+    u_start = seg_start[rep] + k * max_pairs
+    u_end = np.minimum(u_start + max_pairs, seg_end[rep])
+    u_t, u_g = seg_t[rep], seg_g[rep]
+    # units are target-major here: number of units per target -> slots
+    tb = np.ones(u_t.size, dtype=bool)
+    tb[1:] = u_t[1:] != u_t[:-1]
+    t_first = np.nonzero(tb)[0]
+    n_per = np.diff(np.concatenate([t_first, [u_t.size]]))
+    slot, first_slot = _slots(n_per)
+    units = np.stack([u_t, u_start, u_end, slot], axis=1).astype(np.int32)
+    srt = np.lexsort((-(u_end - u_start), u_g))
+    units = np.ascontiguousarray(units[srt])
+    ug = u_g[srt]
+    gear_offsets = np.searchsorted(ug, np.arange(ng + 1)).astype(np.int64)
+    sp = n_per > 1
+    split = np.stack([u_t[t_first][sp], first_slot[sp], n_per[sp], np.zeros(int(sp.sum()), np.int64)],
+                     axis=1).astype(np.int32)
+    ppg = np.bincount(gears, minlength=ng).astype(np.int64)
+    return GearM2LSchedule(units, np.ascontiguousarray(split), int((slot >= 0).sum()), far_src, gear_offsets,
+                           tuple(int(o) for o in orders), ppg)
+
+
 def leaf_schedule(topo: Topology, max_sources: int = 4096, leaf_range: tuple[int, int] | None = None) -> LeafSchedule:
     lo, hi = (0, topo.num_leaves) if leaf_range is None else leaf_range
     ni = topo.num_internal

@@ -1,0 +1,78 @@
+"""Per-pair expansion orders (gears) in the M2L: the gear kernels against the
+oracle's M2L at each pair's own order, and the single-gear case against the
+plain pass."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover - CPU container
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import oracle as O  # noqa: E402
+from jaccpot_b200 import engine, tree, workloads  # noqa: E402
+
+COEF_RTOL = 2e-5
+ORDERS = (2, 4, 6, 8)
+
+
+@pytest.fixture(scope="module")
+def setup():
+    pos, mass = workloads.clustered(32768, seed=5)
+    topo = tree.build_topology(pos, mass, leaf_size=32, theta=0.6)
+    dt = engine.DeviceTopology(topo, "cuda")
+    ps = engine.Pass(dt, 8, G=1.0, eps2=0.0)
+    ps.load_particles(torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda())
+    ps.upward()
+    return topo, ps
+
+
+def _row_rel(a, b):
+    return np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-300)
+
+
+def test_single_gear_equals_plain(setup):
+    topo, ps = setup
+    ps.set_gears(None, None)
+    ps.m2l()
+    ref = ps.ws.locals.clone()
+    ps.set_gears(np.full(topo.num_far_pairs, 3), ORDERS)
+    ps.m2l()
+    got = ps.ws.locals.clone()
+    ps.set_gears(None, None)
+    torch.cuda.synchronize()
+    r, g = ref.double().cpu().numpy(), got.double().cpu().numpy()
+    has = np.abs(r).max(axis=1) > 0
+    assert np.all(g[~has] == 0)
+    assert _row_rel(g[has], r[has]).max() <= 1e-6
+
+
+def test_mixed_gears_match_oracle(setup):
+    topo, ps = setup
+    rng = np.random.default_rng(2)
+    gears = rng.integers(0, 4, size=topo.num_far_pairs)
+    ps.set_gears(gears, ORDERS)
+    ps.m2l()
+    torch.cuda.synchronize()
+    got = ps.ws.locals.double().cpu().numpy()[:, :81]
+    ps.set_gears(None, None)
+    mult = ps.ws.mult.double().cpu().numpy()[:, :81]
+    cen = ps.ws.centers.double().cpu().numpy()[:, :3]
+    tgt = np.repeat(np.arange(topo.num_nodes), np.diff(topo.far_offsets))
+    src = topo.far_sources.astype(np.int64)
+    ref = np.zeros_like(got)
+    for g, p in enumerate(ORDERS):
+        sel = gears == g
+        C = (p + 1) ** 2
+        out = O.m2l(p, mult[src[sel], :C], cen[tgt[sel]] - cen[src[sel]])
+        np.add.at(ref[:, :C], tgt[sel], out)
+    has = np.diff(topo.far_offsets) > 0
+    err = _row_rel(got[has], ref[has])
+    assert np.percentile(err, 99) <= COEF_RTOL, np.percentile(err, [50, 99, 100])
+    assert err.max() <= 50 * COEF_RTOL
+    assert np.all(got[~has] == 0)
