@@ -294,12 +294,18 @@ def evaluate_system(model: GearModel | None, seed: int, n: int = 262144, leaf_si
             times.append(ev[0].elapsed_time(ev[1]))
         return float(np.percentile(e, 99)), float(np.median(times))
 
-    out = {"far_pairs": topo.num_far_pairs}
+    out = {"n": n, "far_pairs": topo.num_far_pairs}
     out["plain_p99"], out["plain_m2l_ms"] = run_and_err()
+    plain_acc = ps.ws.acc4[:, :3].clone()
     if model is not None:
         gears = apply_gears(ps, model)
         out["gear_fraction"] = (np.bincount(gears, minlength=len(model.orders)) / max(1, gears.size)).tolist()
         out["gear_p99"], out["gear_m2l_ms"] = run_and_err()
+        # error the gears add on top of the plain pass, over all particles
+        d = torch.linalg.vector_norm(ps.ws.acc4[:, :3] - plain_acc, dim=1)
+        rel = (d / torch.linalg.vector_norm(plain_acc, dim=1).clamp_min(1e-30)).double().cpu().numpy()
+        out["added_p99"] = float(np.percentile(rel, 99))
+        out["added_max"] = float(rel.max())
         ps.set_gears(None, None)
     return out
 
@@ -311,10 +317,11 @@ def main(argv=None):
     ap.add_argument("--seeds", type=int, default=16)
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--per-seed", type=int, default=131072)
-    ap.add_argument("--budgets", default="3e-5,1e-5,5e-6,2e-6,1e-6")
+    ap.add_argument("--budgets", default="1e-5,3e-6,1e-6,3e-7,1e-7")
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--val-seed", type=int, default=100)
-    ap.add_argument("--target-p99", type=float, default=0.97e-4)
+    ap.add_argument("--val-n", type=int, default=2097152)
+    ap.add_argument("--max-added-p99", type=float, default=2e-5)
     ap.add_argument("--out", default=str(DEFAULT_MODEL))
     args = ap.parse_args(argv)
     Xs, Ys = [], []
@@ -332,15 +339,16 @@ def main(argv=None):
         pred = predict(model, X[:200000])
         acc = float((pred == lab[:200000]).mean())
         under = float((pred < lab[:200000]).mean())
-        val = evaluate_system(model, args.val_seed, n=args.n)
+        val = evaluate_system(model, args.val_seed, n=args.val_n)
         print(f"budget {b:.1e}: label fractions {np.bincount(lab, minlength=4) / lab.size}, loss {hist[-1]:.4f}, "
               f"train acc {acc:.3f}, under-predicted {under:.4f}, val {val}", flush=True)
         model.info = {"samples": int(X.shape[0]), "seeds": args.seeds, "n": args.n, "epochs": args.epochs,
                       "final_loss": hist[-1], "train_accuracy": acc, "under_predicted": under, "validation": val,
                       "label_fractions": (np.bincount(lab, minlength=4) / lab.size).tolist()}
-        # the gears may not make the error worse than the plain pass's by more
-        # than 2%, nor push it over the target when the plain pass meets it
-        if val["gear_p99"] <= max(args.target_p99, 1.02 * val["plain_p99"]):
+        # the error the gears add to the plain pass (p99 over all particles of
+        # an unseen system at the evaluation size) must stay small next to the
+        # 1e-4 budget, which the plain maximum-order pass already uses most of
+        if val["added_p99"] <= args.max_added_p99:
             best = model
             break
     if best is None:

@@ -85,8 +85,10 @@ class FastMultipoleMethod:
         nearfield_compensated: bool = False,
         device: str | torch.device = "cuda",
         advanced: Any = None,
+        gear_model: Any = None,
         **legacy_kwargs: Any,
     ):
+        legacy_gear_model = gear_model
         preset = str(getattr(preset, "value", preset)).lower()
         if preset not in _PRESETS:
             raise ValueError(f"unknown preset {preset!r}")
@@ -112,6 +114,9 @@ class FastMultipoleMethod:
         self.p2p_mode = _lib.JB_P2P_KAHAN if nearfield_compensated else _lib.JB_P2P_FP32
         self.adaptive_order = bool(adaptive_order)
         self.p_gears = tuple(p_gears) if p_gears is not None else None
+        self.gear_model = legacy_gear_model
+        if self.adaptive_order and self.p_gears is not None and max(self.p_gears) < 1:
+            raise ValueError("p_gears must hold positive orders")
         self.device = torch.device(device)
         self._last_state: Optional[FMMPreparedState] = None
 
@@ -130,6 +135,14 @@ class FastMultipoleMethod:
                   p2p_mode=self.p2p_mode)
         ps.load_particles(_to_torch(positions, self.device, torch.float32),
                           _to_torch(masses, self.device, torch.float32))
+        if self.adaptive_order:
+            # learned per-pair gears, chosen from a plain pass's force scale
+            from . import gears as _gears
+
+            model = self.gear_model if self.gear_model is not None else _gears.GearModel.load()
+            if self.p_gears is not None and tuple(self.p_gears) != tuple(model.orders):
+                raise ValueError(f"the gear model is trained for p_gears={model.orders}")
+            _gears.apply_gears(ps, model)
         ps.upward()
         ps.downward()
         st = FMMPreparedState(topology=topo, device_topology=dt, pass_=ps, max_order=int(max_order), theta=th,
