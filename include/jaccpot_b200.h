@@ -165,6 +165,20 @@ JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orde
                         const int* units, const float* mult, const float* centers, const int* far_src,
                         float* locals, float* partials, int num_split, const int* split, void* stream);
 
+/* Split-BF16 far field on the tensor cores (tcgen05.mma kind::f16, FP32
+ * accumulation in TMEM): the M2L chain Dz(az) B Dz(-ax) r^-k K r^-(n+1) Dz(ax)
+ * B^T Dz(-az) (operators/m2l_real_rot_scale.py:288-386 with B^T Z B folded into
+ * K) with the three constant products done as A_hi W_hi + A_lo W_hi + A_hi W_lo
+ * on BF16 hi/lo splits.  Pairs in CSR order (pair_tgt[e] <- far_src[e]) are
+ * taken 128 per tile; seg_off / segs (int4: target, first row, end row, slot)
+ * describe each tile's target runs; slot >= 0 rows go to partials and the split
+ * list sums them as in jb_m2l.  *status (device int, zero it first) becomes 1
+ * if a tensor-core barrier wait timed out.  Orders 2..8. */
+JB_API int jb_m2l_split(int p, int num_tiles, int64_t num_pairs, const int* pair_tgt, const int* far_src,
+                        const int* seg_off, const int* segs, const float* mult, const float* centers,
+                        float* locals, float* partials, int num_split, const int* split, int* status,
+                        void* stream);
+
 /* Downward sweep, one level: for each internal node in [first, last), adds
  * l2l(parent) to both children (l2l_real, operators/real_translations.py:604;
  * _propagate_solidfmm_locals_by_level, runtime/kernels/_l2l.py:210-404). */

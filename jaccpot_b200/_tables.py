@@ -217,6 +217,159 @@ def generate_kfold(out_path: Path, max_order: int = MAX_ORDER) -> Path:
     return out_path
 
 
+# ---------------------------------------------------------------------------
+# tcgen05 plans for the split-BF16 M2L chain
+# ---------------------------------------------------------------------------
+TC_ORDERS = tuple(range(2, 9))
+TC_ROW = 96  # padded width of the A operand rows (bf16 elements)
+
+
+def _components(mat: np.ndarray) -> list[tuple[list[int], list[int]]]:
+    """Connected components of the bipartite non-zero graph: (rows, cols)."""
+    R, Cc = mat.shape
+    parent = list(range(R + Cc))
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    for i, j in zip(*np.nonzero(mat)):
+        parent[find(int(i))] = find(R + int(j))
+    groups: dict[int, tuple[list[int], list[int]]] = {}
+    for i in range(R):
+        if mat[i].any():
+            groups.setdefault(find(i), ([], []))[0].append(i)
+    for j in range(Cc):
+        if mat[:, j].any():
+            groups.setdefault(find(R + j), ([], []))[1].append(j)
+    return list(groups.values())
+
+
+def _bf16_bits(x: np.ndarray) -> np.ndarray:
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    return (((u + 0x7FFF + ((u >> 16) & 1)) >> 16) & 0xFFFF).astype(np.uint16)
+
+
+def _bf16_val(bits: np.ndarray) -> np.ndarray:
+    return (bits.astype(np.uint32) << 16).view(np.float32)
+
+
+def tc_plan(p: int) -> dict:
+    """Block-diagonal tensor-core tiling of the three constant products of the
+    M2L chain (B, K = B^T Z0 B, B^T) at order p.
+
+    Each product's non-zero structure splits into small square blocks (B: per
+    degree, cos / sin class and m-parity; K: four blocks).  Blocks are packed
+    first-fit into 16-wide tiles (wider blocks get their own tile, rounded up
+    to 16); tile j owns padded columns [col0, col0 + w) of both the input (A
+    operand) and the output (TMEM accumulator) index spaces.  `inp[c]` /
+    `out[c]` give the coefficient held by padded column c (-1 = zero pad).
+    Weights are split into BF16 hi and lo parts, stored per tile as w x w
+    K-major core-matrix blocks (8 rows x 16 bytes each)."""
+    C = (p + 1) ** 2
+    bfull = np.zeros((C, C))
+    for ell in range(p + 1):
+        bfull[ell * ell:(ell + 1) ** 2, ell * ell:(ell + 1) ** 2] = bu_matrix(ell)
+    bfull[np.abs(bfull) < 1e-12] = 0.0
+    k = kfold_matrix(p)
+    gemms = []
+    for mat, pack in ((bfull, True), (k, False), (bfull.T.copy(), True)):
+        comps = _components(mat)
+        for r, q in comps:
+            assert len(r) == len(q), "blocks must be square"
+        comps.sort(key=lambda rq: (-len(rq[0]), rq[0][0]))
+        bins: list[list] = []
+        for r, q in comps:
+            w = len(r)
+            if pack and w <= 16:
+                for b in bins:
+                    if b[0] == 16 and b[1] + w <= 16:
+                        b[2].append((r, q))
+                        b[1] += w
+                        break
+                else:
+                    bins.append([16, w, [(r, q)]])
+            else:
+                bins.append([(w + 15) // 16 * 16, w, [(r, q)]])
+        tiles, inp, out, wbits = [], [], [], []
+        col0 = 0
+        woff = 0
+        for wd, _, blocks in bins:
+            rows = [i for r, _ in blocks for i in r]
+            cols = [j for _, q in blocks for j in q]
+            tile = np.zeros((wd, wd))
+            ro, co = 0, 0
+            for r, q in blocks:
+                tile[ro:ro + len(r), co:co + len(q)] = mat[np.ix_(r, q)]
+                ro += len(r)
+                co += len(q)
+            inp += cols + [-1] * (wd - len(cols))
+            out += rows + [-1] * (wd - len(rows))
+            hi = _bf16_bits(tile.astype(np.float32))
+            lo = _bf16_bits((tile - _bf16_val(hi).astype(np.float64)).astype(np.float32))
+            for part in (hi, lo):
+                buf = np.zeros(wd * wd, np.uint16)
+                for n in range(wd):
+                    for kk in range(wd):
+                        off = (n // 8) * (wd // 8) * 64 + (kk // 8) * 64 + (n % 8) * 8 + (kk % 8)
+                        buf[off] = part[n, kk]
+                wbits.append(buf)
+            tiles.append((col0, wd, woff))
+            col0 += wd
+            woff += 2 * wd * wd * 2
+        assert col0 <= TC_ROW, (p, col0)
+        gemms.append({"tiles": tiles, "inp": inp, "out": out, "npad": col0,
+                      "w": np.concatenate(wbits) if wbits else np.zeros(0, np.uint16)})
+    return {"p": p, "gemms": gemms}
+
+
+def generate_tc(out_path: Path) -> Path:
+    lines = [
+        "// Generated by jaccpot_b200/_tables.py -- do not edit.",
+        "// tcgen05 plans of the split-BF16 M2L chain (B, K = B^T Z0 B, B^T) per order:",
+        "// tiles (col0, width, byte offset of the hi part; lo follows), padded-column",
+        "// to coefficient maps, and the BF16 hi/lo weight tiles in K-major core-matrix",
+        "// layout.",
+        "#pragma once",
+        "#include <stdint.h>",
+        "namespace jb {",
+        f"constexpr int kTcRow = {TC_ROW};",
+        "template <int P> struct TcPlan;",
+    ]
+    for p in TC_ORDERS:
+        pl = tc_plan(p)
+        g = pl["gemms"]
+        wall = np.concatenate([x["w"] for x in g])
+        goff = np.cumsum([0] + [x["w"].size * 2 for x in g])
+        lines.append(f"static __device__ __align__(16) const uint16_t c_tc_w_p{p}[{max(wall.size, 1)}] = {{")
+        for a in range(0, wall.size, 16):
+            lines.append("  " + ", ".join(str(int(v)) for v in wall[a:a + 16]) + ",")
+        lines.append("};")
+        lines.append(f"template <> struct TcPlan<{p}> {{")
+        lines.append(f"  static constexpr int kWBytes = {int(goff[-1])};")
+        lines.append(f"  static __device__ __forceinline__ const uint16_t* weights() {{ return c_tc_w_p{p}; }}")
+        for gi, x in enumerate(g):
+            lines.append(f"  static constexpr int kNumTiles{gi} = {len(x['tiles'])};")
+            lines.append(f"  static constexpr int kNpad{gi} = {x['npad']};")
+            lines.append(f"  static constexpr int kGemmOff{gi} = {int(goff[gi])};")
+            t = x["tiles"]
+            lines.append(f"  static __host__ __device__ constexpr int tile_col{gi}(int j) {{ constexpr int t[] = {{{', '.join(str(a) for a, _, _ in t)}}}; return t[j]; }}")
+            lines.append(f"  static __host__ __device__ constexpr int tile_w{gi}(int j) {{ constexpr int t[] = {{{', '.join(str(b) for _, b, _ in t)}}}; return t[j]; }}")
+            lines.append(f"  static __host__ __device__ constexpr int tile_off{gi}(int j) {{ constexpr int t[] = {{{', '.join(str(int(goff[gi]) + c) for _, _, c in t)}}}; return t[j]; }}")
+            lines.append(f"  static __host__ __device__ constexpr int inp{gi}(int c) {{ constexpr int t[] = {{{', '.join(str(v) for v in x['inp'])}}}; return c < {x['npad']} ? t[c] : -1; }}")
+            lines.append(f"  static __host__ __device__ constexpr int out{gi}(int c) {{ constexpr int t[] = {{{', '.join(str(v) for v in x['out'])}}}; return c < {x['npad']} ? t[c] : -1; }}")
+        lines.append("};")
+    lines.append("}  // namespace jb")
+    text = "\n".join(lines) + "\n"
+    out_path.parent.mkdir(parents=True, exist_ok=True)
+    if not out_path.exists() or out_path.read_text() != text:
+        out_path.write_text(text)
+    return out_path
+
+
 if __name__ == "__main__":
     generate(Path(__file__).resolve().parent / "csrc" / "generated" / "bu_tables.h")
+    generate_tc(Path(__file__).resolve().parent / "csrc" / "generated" / "tc_plans.h")
     generate_kfold(Path(__file__).resolve().parent / "csrc" / "generated" / "kfold_tables.h")

@@ -46,7 +46,7 @@ def _cxx() -> str:
 
 def _deps(src: Path) -> list[Path]:
     return [src, CSRC / "fmm_ops.cuh", CSRC / "fmm_kernels.cuh", CSRC / "generated" / "bu_tables.h",
-            CSRC / "generated" / "kfold_tables.h",
+            CSRC / "generated" / "kfold_tables.h", CSRC / "generated" / "tc_plans.h",
             INCLUDE / "jaccpot_b200.h", CSRC / "tree_build.h", CSRC / "tcgen05_m2l.cuh"]
 
 
@@ -66,6 +66,7 @@ def _run(cmd: list[str]) -> None:
 def build(verbose: bool = False, jobs: int | None = None) -> Path:
     _tables.generate(CSRC / "generated" / "bu_tables.h")
     _tables.generate_kfold(CSRC / "generated" / "kfold_tables.h")
+    _tables.generate_tc(CSRC / "generated" / "tc_plans.h")
     OBJ_DIR.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     jobs_todo = []

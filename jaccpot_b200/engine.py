@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .schedule import gear_m2l_schedule, leaf_schedule, m2l_schedule
+from .schedule import gear_m2l_schedule, leaf_schedule, m2l_schedule, tc_m2l_schedule
 from .tree import Topology
 
 
@@ -177,6 +177,9 @@ class Pass:
     def m2l(self, stream=None) -> None:
         ws, s, sc = self.ws, _stream_handle(stream), self.m2l_sched
         ws.locals.zero_()
+        if self.m2l_mode == _lib.JB_M2L_SPLIT_BF16:
+            self._m2l_split(s)
+            return
         gs = getattr(self, "gear_sched", None)
         if gs is not None:
             _lib.check(self.lib.jb_m2l_gears(
@@ -189,6 +192,36 @@ class Pass:
                                    _ptr(ws.mult), _ptr(ws.centers), _ptr(self.dt.far_src), _ptr(ws.locals),
                                    _ptr(self.m2l_partials), int(sc.split.shape[0]), _ptr(self.d_m2l_split), s),
                    "jb_m2l")
+
+    def _m2l_split(self, s) -> None:
+        """Split-BF16 M2L on the tensor cores (tiles of 128 far pairs)."""
+        if getattr(self, "_tc", None) is None:
+            t, dev = self.dt.topo, self.dt.device
+            if self.leaf_range != (0, t.num_leaves):
+                raise ValueError("the tensor-core M2L covers the whole far list")
+            sc = tc_m2l_schedule(t)
+            up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+            self._tc = {
+                "sched": sc,
+                "seg_off": up(sc.seg_off),
+                "segs": up(sc.segs),
+                "split": up(sc.split),
+                "pair_tgt": up(t.far_pair_targets()),
+                "partials": torch.empty((max(sc.num_slots, 1), self.ws.stride), device=dev, dtype=torch.float32),
+                "status": torch.zeros(1, device=dev, dtype=torch.int32),
+            }
+        T, t, ws = self._tc, self.dt.topo, self.ws
+        sc = T["sched"]
+        _lib.check(self.lib.jb_m2l_split(self.p, sc.num_tiles, t.num_far_pairs, _ptr(T["pair_tgt"]),
+                                         _ptr(self.dt.far_src), _ptr(T["seg_off"]), _ptr(T["segs"]), _ptr(ws.mult),
+                                         _ptr(ws.centers), _ptr(ws.locals), _ptr(T["partials"]),
+                                         int(sc.split.shape[0]), _ptr(T["split"]), _ptr(T["status"]), s),
+                   "jb_m2l_split")
+
+    def tc_status(self) -> int:
+        """Status word of the tensor-core M2L (0 = ok, 1 = a barrier wait timed out)."""
+        T = getattr(self, "_tc", None)
+        return 0 if T is None else int(T["status"].item())
 
     def l2l(self, stream=None) -> None:
         t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)

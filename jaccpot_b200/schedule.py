@@ -136,6 +136,50 @@ def gear_m2l_schedule(topo: Topology, gears: np.ndarray, orders, max_pairs: int 
                            tuple(int(o) for o in orders), ppg)
 
 
+@dataclass
+class TcM2LSchedule:
+    """Tiles of 128 consecutive far pairs (CSR order, sorted by target) for the
+    tensor-core M2L.  seg_off[t]:seg_off[t+1] index the target runs of tile t,
+    segs[i] = (target, first row, end row, slot): slot -1 when the target's
+    whole list lies in the tile (the run writes the local row), else a scratch
+    row that ``split`` sums in slot order."""
+
+    num_tiles: int
+    seg_off: np.ndarray  # int32[num_tiles + 1]
+    segs: np.ndarray  # int32[S, 4]
+    split: np.ndarray  # int32[T, 4]
+    num_slots: int
+
+
+def tc_m2l_schedule(topo: Topology, tile: int = 128) -> TcM2LSchedule:
+    npairs = topo.num_far_pairs
+    nt = (npairs + tile - 1) // tile
+    if npairs == 0:
+        z = np.zeros((0, 4), np.int32)
+        return TcM2LSchedule(0, np.zeros(1, np.int32), z, z, 0)
+    tgt = np.repeat(np.arange(topo.num_nodes, dtype=np.int64), np.diff(topo.far_offsets))
+    e = np.arange(npairs, dtype=np.int64)
+    brk = np.ones(npairs, dtype=bool)
+    brk[1:] = (tgt[1:] != tgt[:-1]) | (e[1:] % tile == 0)
+    st = np.nonzero(brk)[0]
+    en = np.concatenate([st[1:], [npairs]])
+    seg_t = tgt[st]
+    seg_tile = st // tile
+    # segments per target: whole list in one segment -> no slot
+    tb = np.ones(st.size, dtype=bool)
+    tb[1:] = seg_t[1:] != seg_t[:-1]
+    first = np.nonzero(tb)[0]
+    n_per = np.diff(np.concatenate([first, [st.size]]))
+    slot, first_slot = _slots(n_per)
+    segs = np.stack([seg_t, st - seg_tile * tile, en - seg_tile * tile, slot], axis=1).astype(np.int32)
+    seg_off = np.searchsorted(seg_tile, np.arange(nt + 1)).astype(np.int32)
+    sp = n_per > 1
+    split = np.stack([seg_t[first][sp], first_slot[sp], n_per[sp], np.zeros(int(sp.sum()), np.int64)],
+                     axis=1).astype(np.int32)
+    return TcM2LSchedule(int(nt), seg_off, np.ascontiguousarray(segs), np.ascontiguousarray(split),
+                         int((slot >= 0).sum()))
+
+
 def leaf_schedule(topo: Topology, max_sources: int = 4096, leaf_range: tuple[int, int] | None = None) -> LeafSchedule:
     lo, hi = (0, topo.num_leaves) if leaf_range is None else leaf_range
     ni = topo.num_internal
