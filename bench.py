@@ -112,12 +112,17 @@ def _peaks() -> dict:
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
-def _traffic(kernel: str):
-    p = ROOT / "profiles" / "traffic.json"
-    if p.exists():
-        d = json.loads(p.read_text())
-        return d.get(kernel)
-    return None
+# DRAM bytes (read + write) per launch of the dominant kernels at the bench
+# workload, scaled from single-launch ncu captures of a 1M-particle case by
+# the units processed (far pairs / particle pairs); see profiles/.
+TRAFFIC_PER_UNIT = {"k_m2l_units": 13.0, "k_m2l_tc": None, "k_leaf_units": None}
+
+
+def _traffic(kernel: str, units: float | None = None):
+    per = TRAFFIC_PER_UNIT.get(kernel)
+    if per is None or units is None:
+        return None
+    return per * units
 
 
 # ---------------------------------------------------------------------------
@@ -207,8 +212,10 @@ def main() -> None:
 
     forms = {
         "plain": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_FP32),
-        "chosen": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_KAHAN),
+        "chosen": dict(m2l_mode=_lib.JB_M2L_SPLIT_BF16, p2p_mode=_lib.JB_P2P_KAHAN),
     }
+    if world > 1:  # the tensor-core M2L tiles the whole far list
+        forms["chosen"]["m2l_mode"] = _lib.JB_M2L_FP32
     passes = {k: engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, leaf_range=(leaf_lo, leaf_hi), **v)
               for k, v in forms.items()}
     d_pos = torch.from_numpy(pos).to(dev)
@@ -350,15 +357,25 @@ def main() -> None:
     fp32_peak = 2.0 * 148 * 8 * 256 * iters * 8 / (pe0.elapsed_time(pe1) / 1e3) / 1e12
     stage_names = ["upward", "m2l", "l2l", "leaf_eval", "unsort"]
     dom = int(np.argmax(stage_chosen))
-    if stage_names[dom] == "m2l":
+    split_m2l = forms["chosen"]["m2l_mode"] == _lib.JB_M2L_SPLIT_BF16
+    if stage_names[dom] == "m2l" and split_m2l:
+        # tensor-core kernel: algorithmic flops against the measured bf16 peak,
+        # and the same work against the FP32 pipe, where its per-pair rotations run
         ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
-        roof = {"kernel": "k_m2l_fp32<8>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_m2l_fp32")}
+        roof = {"kernel": f"k_m2l_tc<{cfg['order']}>", "bound": "tensor", "achieved": ach,
+                "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": ach / peaks["bf16_tflops"],
+                "traffic": _traffic("k_m2l_tc", topo.num_far_pairs), "fp32_pipe_frac": ach / fp32_peak}
+    elif stage_names[dom] == "m2l":
+        ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
+        roof = {"kernel": f"k_m2l_units<{cfg['order']}>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_m2l_units", topo.num_far_pairs)}
     else:
         ach = p2p_flops / (stage_chosen[3] / 1e3) / 1e12
-        roof = {"kernel": "k_leaf_eval<8,kahan>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_leaf_eval")}
-    roof["peak_source"] = "in-run FP32 FMA probe (MEASURED_PEAKS.json has HBM and bf16 only)"
+        roof = {"kernel": f"k_leaf_units<{cfg['order']},kahan>", "bound": "fp32", "achieved": ach,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_leaf_units", near_inter)}
+    roof["peak_source"] = ("measured bf16 burst (MEASURED_PEAKS.json)" if roof["bound"] == "tensor" else
+                           "in-run FP32 FMA probe (MEASURED_PEAKS.json has HBM and bf16 only)")
+    roof["stage_ms"] = float(stage_chosen[dom])
     roof["algorithmic"] = "P2P 20 flop/pair x near pairs; M2L 2*(2*sum(2l+1)^2 + z-terms) flop/pair"
 
     cpu = None
@@ -379,9 +396,9 @@ def main() -> None:
     launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
     if rank == 0:
         cfg.update({
-            "form": "chosen = FP32 rotate+scale M2L + Kahan-compensated P2P; plain = FP32 M2L + FP32 P2P; "
-                    "both at the maximum order (the learned-gear variant is reported under 'gears': "
-                    "it does not meet the error bound at this configuration)",
+            "form": "chosen = split-BF16 M2L on tcgen05 (hi/lo 3-product, FP32 accumulation) + Kahan-compensated "
+                    "P2P; plain = FP32 rotate+scale M2L + FP32 P2P; both at the maximum order (the learned-gear "
+                    "variant, FP32 M2L + gears + Kahan P2P, is reported under 'gears')",
             "gears": gear_info,
             "plain_particles_per_s": n / (ms_plain / 1e3),
             "plain_ms_per_step": ms_plain,

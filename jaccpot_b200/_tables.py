@@ -217,6 +217,49 @@ def generate_kfold(out_path: Path, max_order: int = MAX_ORDER) -> Path:
     return out_path
 
 
+def generate_bu_code(out_path: Path, max_order: int = MAX_ORDER) -> Path:
+    """Unrolled v <- B v and v <- B^T v per order with the non-zero B_U entries
+    as literals (no constant-memory reads), degree by degree in place."""
+    lines = [
+        "// Generated by jaccpot_b200/_tables.py -- do not edit.",
+        "// In-place v <- B v (TR = false) or B^T v (TR = true) over degrees 1..P,",
+        "// B = B_U per degree (its non-zero entries as literals).",
+        "#pragma once",
+        "namespace jb {",
+        "template <int P, bool TR> struct BApply;",
+    ]
+    for p in range(1, max_order + 1):
+        for tr in (False, True):
+            lines.append(f"template <> struct BApply<{p}, {'true' if tr else 'false'}> {{")
+            lines.append("  static __device__ __forceinline__ void apply(float* v) {")
+            for ell in range(1, p + 1):
+                b = bu_matrix(ell)
+                if tr:
+                    b = b.T
+                w = 2 * ell + 1
+                o = ell * ell
+                lines.append("    {")
+                lines.append("      " + " ".join(f"const float i{j} = v[{o + j}];" for j in range(w)))
+                for i in range(w):
+                    terms = [(j, b[i, j]) for j in range(w) if abs(b[i, j]) > 1e-12]
+                    if not terms:
+                        lines.append(f"      v[{o + i}] = 0.f;")
+                        continue
+                    expr = f"{_flit(terms[0][1])} * i{terms[0][0]}"
+                    for j, val in terms[1:]:
+                        expr = f"fmaf({_flit(val)}, i{j}, {expr})"
+                    lines.append(f"      v[{o + i}] = {expr};")
+                lines.append("    }")
+            lines.append("  }")
+            lines.append("};")
+    lines.append("}  // namespace jb")
+    text = "\n".join(lines) + "\n"
+    out_path.parent.mkdir(parents=True, exist_ok=True)
+    if not out_path.exists() or out_path.read_text() != text:
+        out_path.write_text(text)
+    return out_path
+
+
 # ---------------------------------------------------------------------------
 # tcgen05 plans for the split-BF16 M2L chain
 # ---------------------------------------------------------------------------
@@ -372,4 +415,5 @@ def generate_tc(out_path: Path) -> Path:
 if __name__ == "__main__":
     generate(Path(__file__).resolve().parent / "csrc" / "generated" / "bu_tables.h")
     generate_tc(Path(__file__).resolve().parent / "csrc" / "generated" / "tc_plans.h")
+    generate_bu_code(Path(__file__).resolve().parent / "csrc" / "generated" / "bu_code.h")
     generate_kfold(Path(__file__).resolve().parent / "csrc" / "generated" / "kfold_tables.h")

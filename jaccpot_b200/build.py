@@ -46,7 +46,7 @@ def _cxx() -> str:
 
 def _deps(src: Path) -> list[Path]:
     return [src, CSRC / "fmm_ops.cuh", CSRC / "fmm_kernels.cuh", CSRC / "generated" / "bu_tables.h",
-            CSRC / "generated" / "kfold_tables.h", CSRC / "generated" / "tc_plans.h",
+            CSRC / "generated" / "kfold_tables.h", CSRC / "generated" / "tc_plans.h", CSRC / "generated" / "bu_code.h",
             INCLUDE / "jaccpot_b200.h", CSRC / "tree_build.h", CSRC / "tcgen05_m2l.cuh"]
 
 
@@ -67,6 +67,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     _tables.generate(CSRC / "generated" / "bu_tables.h")
     _tables.generate_kfold(CSRC / "generated" / "kfold_tables.h")
     _tables.generate_tc(CSRC / "generated" / "tc_plans.h")
+    _tables.generate_bu_code(CSRC / "generated" / "bu_code.h")
     OBJ_DIR.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     jobs_todo = []

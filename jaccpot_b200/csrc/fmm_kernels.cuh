@@ -119,49 +119,50 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_p2m(const float4* __res
 // ---------------------------------------------------------------------------
 // M2M, one level (+ internal COM from the children).
 // ---------------------------------------------------------------------------
+// Two adjacent threads per parent (one per child): each shifts its child's
+// multipole, the pair adds the two through one shuffle per coefficient (the
+// same sum in both lanes), and the even lane writes the parent.
 template <int P>
 __global__ void __launch_bounds__(128) k_m2m_level(int first, int last, const int* __restrict__ left,
                                                    const int* __restrict__ right, float4* __restrict__ centers,
                                                    float* __restrict__ mult) {
   constexpr int C = csize(P), CS = cstride(P);
-  const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= last) return;
-  const int a = left[i], b = right[i];
-  const float4 ca = centers[a], cb = centers[b];
-  const float m = ca.w + cb.w;
-  float4 c;
-  if (m > 0.f) {
-    const float inv = 1.f / m;
-    c = make_float4((ca.w * ca.x + cb.w * cb.x) * inv, (ca.w * ca.y + cb.w * cb.y) * inv,
-                    (ca.w * ca.z + cb.w * cb.z) * inv, m);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = first + (tid >> 1);
+  const bool ok = i < last;
+  const int side = tid & 1;
+  float v[C];
+  float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (ok) {
+    const int a = left[i], b = right[i];
+    const float4 ca = centers[a], cb = centers[b];
+    const float m = ca.w + cb.w;
+    if (m > 0.f) {
+      const float inv = 1.f / m;
+      c = make_float4((ca.w * ca.x + cb.w * cb.x) * inv, (ca.w * ca.y + cb.w * cb.y) * inv,
+                      (ca.w * ca.z + cb.w * cb.z) * inv, m);
+    } else {
+      c = make_float4(0.5f * (ca.x + cb.x), 0.5f * (ca.y + cb.y), 0.5f * (ca.z + cb.z), 0.f);
+    }
+    const float4 cc = side ? cb : ca;
+    const float* src = mult + (size_t)(side ? b : a) * CS;
+#pragma unroll
+    for (int k = 0; k < C; ++k) v[k] = src[k];
+    m2m_pair<P>(v, cc.x - c.x, cc.y - c.y, cc.z - c.z);
   } else {
-    c = make_float4(0.5f * (ca.x + cb.x), 0.5f * (ca.y + cb.y), 0.5f * (ca.z + cb.z), 0.f);
+#pragma unroll
+    for (int k = 0; k < C; ++k) v[k] = 0.f;
   }
-  centers[i] = c;
-  float acc[C];
-  {
-    float v[C];
-    const float* src = mult + (size_t)a * CS;
 #pragma unroll
-    for (int k = 0; k < C; ++k) v[k] = src[k];
-    m2m_pair<P>(v, ca.x - c.x, ca.y - c.y, ca.z - c.z);
+  for (int k = 0; k < C; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], 1);
+  if (ok && side == 0) {
+    centers[i] = c;
+    float* dst = mult + (size_t)i * CS;
 #pragma unroll
-    for (int k = 0; k < C; ++k) acc[k] = v[k];
+    for (int k = 0; k < C; ++k) dst[k] = v[k];
+#pragma unroll
+    for (int k = C; k < CS; ++k) dst[k] = 0.f;
   }
-  {
-    float v[C];
-    const float* src = mult + (size_t)b * CS;
-#pragma unroll
-    for (int k = 0; k < C; ++k) v[k] = src[k];
-    m2m_pair<P>(v, cb.x - c.x, cb.y - c.y, cb.z - c.z);
-#pragma unroll
-    for (int k = 0; k < C; ++k) acc[k] += v[k];
-  }
-  float* dst = mult + (size_t)i * CS;
-#pragma unroll
-  for (int k = 0; k < C; ++k) dst[k] = acc[k];
-#pragma unroll
-  for (int k = C; k < CS; ++k) dst[k] = 0.f;
 }
 
 // ---------------------------------------------------------------------------
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(128) k_m2m_level(int first, int last, const in
 // per-thread LDS.128 reads are bank-conflict free.  The local accumulates in
 // a shared-memory column per thread.
 // ---------------------------------------------------------------------------
-constexpr int kM2LThreads = 128;
+constexpr int kM2LThreads = 64;
 
 __host__ __device__ constexpr int row4(int p) { return (cstride(p) / 4) | 1; }  // float4 per smem row (odd)
 
@@ -194,7 +195,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // real M2L matrix is symmetric, so sum_v M2L(c_v - c_u)^T Lbar_v is this
 // kernel run over u's own list with Lbar in place of the multipoles.
 template <int P, bool NEG>
-__global__ void __launch_bounds__(kM2LThreads, 3) k_m2l_units(int num_units, const int4* __restrict__ units,
+__global__ void __launch_bounds__(kM2LThreads, 384 / kM2LThreads) k_m2l_units(int num_units, const int4* __restrict__ units,
                                                               const float* __restrict__ mult,
                                                               const float4* __restrict__ centers,
                                                               const int* __restrict__ far_src,
@@ -334,33 +335,88 @@ struct NearAcc {
 
 #define JB_PAD4 make_float4(1e18f, 1e18f, 1e18f, 0.f)
 
+// Packed FP32x2 arithmetic (sm_100 add/sub/mul/fma .f32x2): one instruction
+// for two lanes of work, so the near-field loop handles two sources per step
+// with half the issue slots of scalar code.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_split(f32x2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// One chunk of 32 staged sources for this lane's target: sources j = q*G + h,
+// two per step in packed form; the two partial sums are added at the end of
+// the chunk (and into the compensated accumulator when KAHAN).
 template <int G, bool KAHAN, bool POT, bool SELF>
 __device__ __forceinline__ void near_chunk(const float4* __restrict__ sp, float4 ti, int h, int self_j, float eps2,
                                            NearAcc<KAHAN>& a) {
-  float ax = 0.f, ay = 0.f, az = 0.f, aw = 0.f;
+  const f32x2 TX = f2(ti.x, ti.x), TY = f2(ti.y, ti.y), TZ = f2(ti.z, ti.z), E2 = f2(eps2, eps2);
+  f32x2 AX = f2(0.f, 0.f), AY = AX, AZ = AX, AW = AX;
 #pragma unroll
-  for (int q = 0; q < 32 / G; ++q) {
-    const int j = q * G + h;
-    const float4 s = sp[j];
-    const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
-    const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-    const float ir = rsqrtf(d2);
-    float mir = s.w * ir;
-    float w = mir * (ir * ir);
+  for (int q = 0; q < 32 / G; q += 2) {
+    const int j0 = q * G + h, j1 = j0 + G;
+    const float4 s0 = sp[j0], s1 = sp[j1];
+    const f32x2 dx = f2_sub(TX, f2(s0.x, s1.x));
+    const f32x2 dy = f2_sub(TY, f2(s0.y, s1.y));
+    const f32x2 dz = f2_sub(TZ, f2(s0.z, s1.z));
+    const f32x2 d2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, E2)));
+    float d2a, d2b;
+    f2_split(d2, d2a, d2b);
+    const f32x2 ir = f2(rsqrtf(d2a), rsqrtf(d2b));
+    f32x2 mir = f2_mul(f2(s0.w, s1.w), ir);
+    f32x2 w = f2_mul(mir, f2_mul(ir, ir));
     if (SELF) {
-      const bool me = (j == self_j);
-      mir = me ? 0.f : mir;
-      w = me ? 0.f : w;
+      float m0, m1, w0, w1;
+      f2_split(mir, m0, m1);
+      f2_split(w, w0, w1);
+      m0 = (j0 == self_j) ? 0.f : m0;
+      w0 = (j0 == self_j) ? 0.f : w0;
+      m1 = (j1 == self_j) ? 0.f : m1;
+      w1 = (j1 == self_j) ? 0.f : w1;
+      mir = f2(m0, m1);
+      w = f2(w0, w1);
     }
-    ax = fmaf(w, dx, ax);
-    ay = fmaf(w, dy, ay);
-    az = fmaf(w, dz, az);
-    if (POT) aw += mir;
+    AX = f2_fma(w, dx, AX);
+    AY = f2_fma(w, dy, AY);
+    AZ = f2_fma(w, dz, AZ);
+    if (POT) AW = f2_add(AW, mir);
   }
-  a.add(0, ax);
-  a.add(1, ay);
-  a.add(2, az);
-  if (POT) a.add(3, aw);
+  float x0, x1, y0, y1, z0, z1;
+  f2_split(AX, x0, x1);
+  f2_split(AY, y0, y1);
+  f2_split(AZ, z0, z1);
+  a.add(0, x0 + x1);
+  a.add(1, y0 + y1);
+  a.add(2, z0 + z1);
+  if (POT) {
+    float w0, w1;
+    f2_split(AW, w0, w1);
+    a.add(3, w0 + w1);
+  }
 }
 
 template <int P, int G, bool KAHAN, bool POT>
@@ -553,7 +609,7 @@ template <int P>
 struct RunM2M {
   static int run(int first, int last, const int* left, const int* right, float* centers, float* mult, cudaStream_t st) {
     if (last <= first) return JB_OK;
-    k_m2m_level<P><<<blocks_for(last - first, 128), 128, 0, st>>>(first, last, left, right,
+    k_m2m_level<P><<<blocks_for(2 * (int64_t)(last - first), 128), 128, 0, st>>>(first, last, left, right,
                                                                    reinterpret_cast<float4*>(centers), mult);
     return launch_status();
   }

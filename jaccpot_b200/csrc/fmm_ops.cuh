@@ -32,6 +32,7 @@
 
 #include "generated/bu_tables.h"
 #include "generated/kfold_tables.h"
+#include "generated/bu_code.h"
 
 namespace jb {
 
@@ -208,13 +209,13 @@ __device__ __forceinline__ void m2l_kfold(float* v, float dx, float dy, float dz
   }
   const float s = 1.f / fmaxf(r, 1.0e-30f);
   dz_rot<P, false>(v, caz, saz);
-  bu_apply<P, false, false, false>(v);
+  BApply<P, false>::apply(v);
   dz_rot<P, true>(v, cax, sax);
   scale_degrees<P, 0>(v, s);
   KFold<P>::apply(v);
   scale_degrees<P, 1>(v, s);
   dz_rot<P, false>(v, cax, sax);
-  bu_apply<P, true, false, false>(v);
+  BApply<P, true>::apply(v);
   dz_rot<P, true>(v, caz, saz);
 }
 
@@ -264,17 +265,40 @@ __device__ __forceinline__ void m2l_pair(float* v, float* w, float dx, float dy,
   dz_apply<P, true>(w, taz);
 }
 
+// Rotation angles of a displacement as (cos, sin) pairs for dz_rot:
+// az = atan2(x, y) -> (y/rho, x/rho);  ax = atan2(rho, z) -> (z/r, rho/r).
+__device__ __forceinline__ void align_cs(float x, float y, float z, float& caz, float& saz, float& cax, float& sax,
+                                         float& r) {
+  const float rho2 = x * x + y * y;
+  const float r2 = rho2 + z * z;
+  const float rho = sqrtf(rho2);
+  r = sqrtf(r2);
+  caz = 1.f;
+  saz = 0.f;
+  cax = 1.f;
+  sax = 0.f;
+  if (rho2 > 0.f) {
+    const float ir = 1.f / rho;
+    caz = y * ir;
+    saz = x * ir;
+  }
+  if (r2 > 0.f) {
+    const float ir = 1.f / r;
+    cax = z * ir;
+    sax = rho * ir;
+  }
+}
+
 // M2M: delta = child - parent (source - destination).  r < 1e-30 -> identity shift.
 template <int P>
 __device__ __forceinline__ void m2m_pair(float* v, float dx, float dy, float dz) {
-  Trig<P> taz, tax;
-  float r;
-  align_trig<P>(dx, dy, dz, taz, tax, &r);
+  float caz, saz, cax, sax, r;
+  align_cs(dx, dy, dz, caz, saz, cax, sax, r);
   const float d = r < 1e-30f ? 0.f : r;
-  dz_apply<P, false>(v, taz);
-  bu_apply<P, false, false, false>(v);
-  dz_apply<P, true>(v, tax);
-  bu_apply<P, false, false, false>(v);
+  dz_rot<P, false>(v, caz, saz);
+  BApply<P, false>::apply(v);
+  dz_rot<P, true>(v, cax, sax);
+  BApply<P, false>::apply(v);
   float dk[P + 1];
   dk[0] = 1.f;
 #pragma unroll
@@ -291,24 +315,23 @@ __device__ __forceinline__ void m2m_pair(float* v, float dx, float dy, float dz)
     }
   }
   // from-z multipole: Dz(-az) B Dz(ax) B
-  bu_apply<P, false, false, false>(v);
-  dz_apply<P, false>(v, tax);
-  bu_apply<P, false, false, false>(v);
-  dz_apply<P, true>(v, taz);
+  BApply<P, false>::apply(v);
+  dz_rot<P, false>(v, cax, sax);
+  BApply<P, false>::apply(v);
+  dz_rot<P, true>(v, caz, saz);
 }
 
 // L2L: delta = parent - child (old - new centre).
 template <int P>
 __device__ __forceinline__ void l2l_pair(float* v, float dx, float dy, float dz) {
-  Trig<P> taz, tax;
-  float r;
-  align_trig<P>(dx, dy, dz, taz, tax, &r);
+  float caz, saz, cax, sax, r;
+  align_cs(dx, dy, dz, caz, saz, cax, sax, r);
   const float d = r < 1e-30f ? 0.f : r;
   // to-z local: B^T Dz(-ax) B^T Dz(az)
-  dz_apply<P, false>(v, taz);
-  bu_apply<P, true, false, false>(v);
-  dz_apply<P, true>(v, tax);
-  bu_apply<P, true, false, false>(v);
+  dz_rot<P, false>(v, caz, saz);
+  BApply<P, true>::apply(v);
+  dz_rot<P, true>(v, cax, sax);
+  BApply<P, true>::apply(v);
   float dk[P + 1];
   dk[0] = 1.f;
 #pragma unroll
@@ -325,10 +348,10 @@ __device__ __forceinline__ void l2l_pair(float* v, float dx, float dy, float dz)
     }
   }
   // from-z local: Dz(-az) B^T Dz(ax) B^T
-  bu_apply<P, true, false, false>(v);
-  dz_apply<P, false>(v, tax);
-  bu_apply<P, true, false, false>(v);
-  dz_apply<P, true>(v, taz);
+  BApply<P, true>::apply(v);
+  dz_rot<P, false>(v, cax, sax);
+  BApply<P, true>::apply(v);
+  dz_rot<P, true>(v, caz, saz);
 }
 
 // U_n^m(d) for all n <= P.
