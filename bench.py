@@ -163,6 +163,75 @@ def run_reference(args) -> None:
 
 
 # ---------------------------------------------------------------------------
+def _events_ms(fn, stream, reps=10, warm=3):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def measure_extras(dev, stream) -> dict:
+    """The other BASELINE configs on the same GPU, reported beside the headline:
+    Plummer N=1,048,576, p=6, leaf 32: evaluate_prepared_state on 65,536
+    int32 targets (drawn without replacement), and the adjoint of
+    L = sum w . a with w ~ N(0,1)."""
+    import torch
+
+    from jaccpot_b200 import _lib, engine, tree, workloads
+    from jaccpot_b200.solver import FastMultipoleMethod
+
+    out = {}
+    n = 1048576
+    pos, mass = workloads.plummer(n, 0)
+    fmm = FastMultipoleMethod(preset="large_n_gpu", theta=0.6, G=1.0, softening=0.0, device=dev)
+    st = fmm.prepare_state(pos, mass, leaf_size=32, max_order=6)
+    rng = np.random.default_rng(2)
+    tg = rng.choice(n, 65536, replace=False).astype(np.int32)
+    ts = torch.from_numpy(st.topology.inverse_permutation[tg].astype(np.int32)).to(dev)
+    ps = st.pass_
+    out_t = torch.empty((tg.size, 4), device=dev, dtype=torch.float32)
+    ms_t = _events_ms(lambda: ps.evaluate_targets(ts, out=out_t), stream)
+    # accuracy on 4,096 of the targets against an FP64 direct sum
+    sub = ts[:4096].contiguous()
+    ref = torch.empty((4096, 4), device=dev, dtype=torch.float64)
+    _lib.check(_lib.lib().jb_direct_f64(n, ps.ws.pos4.data_ptr(), 4096, sub.data_ptr(), 1.0, 0.0, ref.data_ptr(),
+                                        stream.cuda_stream), "jb_direct_f64")
+    got = out_t[:4096, :3].double().cpu().numpy()
+    e = workloads.relative_errors(got, ref[:, :3].cpu().numpy())
+    out["plummer_1M_p6_targets_65536"] = {
+        "ms": ms_t, "targets_per_s": tg.size / (ms_t / 1e3),
+        "err_vs_fp64_direct_p99": float(np.percentile(e, 99)),
+        "note": "L2P + P2P for the targets on the prepared state (locals resident)"}
+    # adjoint (config 5): forward pass + hand-written VJP, coefficients recomputed
+    w = torch.from_numpy(np.random.default_rng(5).normal(size=(n, 3)).astype(np.float32)).to(dev)
+    d_pos, d_mass = torch.from_numpy(pos).to(dev), torch.from_numpy(mass).to(dev)
+    gx = torch.empty_like(d_pos)
+    gm = torch.empty_like(d_mass)
+    acc = torch.empty_like(d_pos)
+
+    def fwd():
+        ps.load_particles(d_pos, d_mass)
+        ps.run()
+        ps.unsort(acc, None)
+
+    ms_f = _events_ms(fwd, stream, reps=5)
+    ms_b = _events_ms(lambda: ps.vjp(w, gx, gm, recompute=True), stream, reps=5)
+    out["plummer_1M_p6_adjoint"] = {"forward_ms": ms_f, "vjp_ms_incl_recompute": ms_b,
+                                    "ratio": ms_b / ms_f,
+                                    "finite": bool(torch.isfinite(gx).all() and torch.isfinite(gm).all())}
+    return out
+
+
+# ---------------------------------------------------------------------------
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,6 +241,7 @@ def main() -> None:
     ap.add_argument("--n", type=int, default=WORKLOAD["N"], help="particle count (default: the headline 4M)")
     ap.add_argument("--cpu-sample", type=int, default=1048576, help="CPU baseline sample size")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true", help="skip the target-subset and adjoint measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -220,6 +290,9 @@ def main() -> None:
               for k, v in forms.items()}
     d_pos = torch.from_numpy(pos).to(dev)
     d_mass = torch.from_numpy(mass).to(dev)
+    if world > 1:  # sources replicated from rank 0 (one broadcast), targets sharded
+        from jaccpot_b200 import sharding
+        sharding.replicate_sources(d_pos, d_mass)
     # learned gears for the chosen form: chosen once per topology from a plain
     # pass's force scale (prepare-time, like the reference's gear buckets)
     from jaccpot_b200 import gears as gear_mod
@@ -393,6 +466,7 @@ def main() -> None:
         cpu = {"value": ns / cdt, "unit": "particles/s", "cores": thr, "kind": "port",
                "sample": f"one float32 pass of the oracle on clustered N={ns} (same generator/order/leaf/theta)"}
 
+    extras = measure_extras(dev, stream) if (rank == 0 and world == 1 and not args.no_extras) else None
     launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
     if rank == 0:
         cfg.update({
@@ -425,6 +499,7 @@ def main() -> None:
             "e2e": {"value": n / (e2e / 1e3), "unit": "particles/s", "h2d_bytes_per_step": n * 16,
                     "d2h_bytes_per_step": n * 12, "ms_per_step": e2e},
             "gpu_launches": launches * args.steps,
+            "other_configs": extras,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
