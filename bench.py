@@ -46,10 +46,12 @@ WORKLOAD = {
     "N": 4194304,
     "order": 8,
     "leaf_size": 32,
-    "theta": 0.6,
+    # the 'balanced' preset's theta = 0.6 puts this workload exactly on the error
+    # bound (p99 = 1.00e-4 over 32,768 targets); 0.55 meets it with margin
+    "theta": 0.55,
     "seed": 0,
 }
-ERR_TARGETS = 4096
+ERR_TARGETS = 32768
 ERR_BOUND = 1e-4
 
 
@@ -389,7 +391,8 @@ def main() -> None:
         torch.cuda.synchronize()
         got = acc_out[torch.from_numpy(tg).to(dev)].double().cpu().numpy()
         e = workloads.relative_errors(got, ref[:, :3].cpu().numpy())
-        errs[name] = {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+        errs[name] = {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
+                      "p99_first_4096": float(np.percentile(e[:4096], 99))}
     if gear_info is not None:
         gear_info["err_vs_fp64_direct"] = errs.pop("gears")
         gear_info["err_bound_met"] = bool(gear_info["err_vs_fp64_direct"]["p99"] <= ERR_BOUND)
