@@ -8,9 +8,9 @@
 //   P2M        warp per leaf: COM by warp reduction, U_n^m per lane, transpose
 //              reduction of the (p+1)^2 coefficients through shared memory;
 //   M2M / L2L  thread per (parent) / (parent, child), one launch per level;
-//   M2L        thread per target node walking its CSR source list, targets
-//              pre-sorted by list length so warps stay converged; the
-//              per-thread local accumulates in a shared-memory column;
+//   M2L        thread per work unit (<= 64 pairs of one target's CSR list),
+//              units sorted by length so warps stay converged; the local
+//              accumulates in registers;
 //   leaf eval  warp per target leaf: L2P (lane = particle, the leaf's local
 //              staged once in shared memory) fused with the P2P near field,
 //              source leaves staged 32 particles at a time in shared memory.
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(128) k_m2m_level(int first, int last, const in
 // row with cp.async while the current pair is rotated back, which hides the
 // L2 gather latency; the row stride is an odd number of 16-byte words so the
 // per-thread LDS.128 reads are bank-conflict free.  The local accumulates in
-// a shared-memory column per thread.
+// registers (255 per thread, 8 warps per SM).
 // ---------------------------------------------------------------------------
 constexpr int kM2LThreads = 64;
 
@@ -195,7 +195,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // real M2L matrix is symmetric, so sum_v M2L(c_v - c_u)^T Lbar_v is this
 // kernel run over u's own list with Lbar in place of the multipoles.
 template <int P, bool NEG>
-__global__ void __launch_bounds__(kM2LThreads, 384 / kM2LThreads) k_m2l_units(int num_units, const int4* __restrict__ units,
+__global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units(int num_units, const int4* __restrict__ units,
                                                               const float* __restrict__ mult,
                                                               const float4* __restrict__ centers,
                                                               const int* __restrict__ far_src,
@@ -206,13 +206,13 @@ __global__ void __launch_bounds__(kM2LThreads, 384 / kM2LThreads) k_m2l_units(in
   constexpr int C = csize(P), CS = cstride(P), R4 = row4(P);
   extern __shared__ float4 m2l_smem[];
   float4* row = m2l_smem + threadIdx.x * R4;
-  float* sacc = reinterpret_cast<float*>(m2l_smem + kM2LThreads * R4);  // [C][kM2LThreads]
   const int u = blockIdx.x * kM2LThreads + threadIdx.x;
   if (u >= num_units) return;
   const int4 U = units[u];
   const int tgt = U.x, e0 = U.y, e1 = U.z, slot = U.w;
+  float acc[C];
 #pragma unroll
-  for (int k = 0; k < C; ++k) sacc[k * kM2LThreads + threadIdx.x] = 0.f;
+  for (int k = 0; k < C; ++k) acc[k] = 0.f;
   const float4 ct = centers[tgt];
   int s = far_src[e0];
   {
@@ -246,13 +246,13 @@ __global__ void __launch_bounds__(kM2LThreads, 384 / kM2LThreads) k_m2l_units(in
     if (NEG) m2l_kfold<P>(v, cs.x - ct.x, cs.y - ct.y, cs.z - ct.z);
     else m2l_kfold<P>(v, ct.x - cs.x, ct.y - cs.y, ct.z - cs.z);
 #pragma unroll
-    for (int k = 0; k < C; ++k) sacc[k * kM2LThreads + threadIdx.x] += v[k];
+    for (int k = 0; k < C; ++k) acc[k] += v[k];
     s = sn;
     cs = csn;
   }
   float* dst = (slot < 0) ? locals + (size_t)tgt * rs : partials + (size_t)slot * rs;
 #pragma unroll
-  for (int k = 0; k < C; ++k) dst[k] = sacc[k * kM2LThreads + threadIdx.x];
+  for (int k = 0; k < C; ++k) dst[k] = acc[k];
   for (int k = C; k < rs; ++k) dst[k] = 0.f;
 }
 
@@ -622,7 +622,7 @@ struct RunM2L {
                  int rs = 0) {
     if (rs <= 0) rs = cstride(P);
     if (num_units > 0) {
-      const size_t sm = sizeof(float4) * kM2LThreads * row4(P) + sizeof(float) * csize(P) * kM2LThreads;
+      const size_t sm = sizeof(float4) * kM2LThreads * row4(P);
       auto kern = neg ? k_m2l_units<P, true> : k_m2l_units<P, false>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
