@@ -173,11 +173,14 @@ JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orde
  * taken 128 per tile; seg_off / segs (int4: target, first row, end row, slot)
  * describe each tile's target runs; slot >= 0 rows go to partials and the split
  * list sums them as in jb_m2l.  *status (device int, zero it first) becomes 1
- * if a tensor-core barrier wait timed out.  Orders 2..8. */
-JB_API int jb_m2l_split(int p, int num_tiles, int64_t num_pairs, const int* pair_tgt, const int* far_src,
-                        const int* seg_off, const int* segs, const float* mult, const float* centers,
-                        float* locals, float* partials, int num_split, const int* split, int* status,
-                        void* stream);
+ * if a tensor-core barrier wait timed out.  products = 3: B, K and B^T all run
+ * on the tensor cores (three MMA round trips per tile); products = 1: only K
+ * does, B and B^T run as literal-constant FMAs in registers (one round
+ * trip).  Orders 2..8. */
+JB_API int jb_m2l_split(int p, int products, int num_tiles, int64_t num_pairs, const int* pair_tgt,
+                        const int* far_src, const int* seg_off, const int* segs, const float* mult,
+                        const float* centers, float* locals, float* partials, int num_split, const int* split,
+                        int* status, void* stream);
 
 /* Downward sweep, one level: for each internal node in [first, last), adds
  * l2l(parent) to both children (l2l_real, operators/real_translations.py:604;

@@ -174,7 +174,10 @@ __device__ __forceinline__ void issue(uint32_t tmem, uint32_t a_hi, uint32_t a_l
   }
 }
 
-template <int P>
+// KONLY = true: only the K product runs on the tensor cores and B / B^T run
+// as literal-constant FMAs in registers (one MMA round trip per tile instead
+// of three); false: all three products on the tensor cores.
+template <int P, bool KONLY>
 __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_pairs, const int* __restrict__ pair_tgt,
                                                      const int* __restrict__ far_src, const int* __restrict__ seg_off,
                                                      const int4* __restrict__ segs, const float* __restrict__ mult,
@@ -192,11 +195,13 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5;
 
-  // constant weight tiles -> shared memory
+  // constant weight tiles -> shared memory (only K's when the others run in registers)
   {
-    const uint4* src = reinterpret_cast<const uint4*>(PL::weights());
+    constexpr int w0 = KONLY ? PL::kGemmOff1 : 0;
+    constexpr int w1 = KONLY ? PL::kGemmOff2 : PL::kWBytes;
+    const uint4* src = reinterpret_cast<const uint4*>(PL::weights()) + w0 / 16;
     uint4* dst = reinterpret_cast<uint4*>(w_s);
-    for (int k = tid; k < PL::kWBytes / 16; k += kThreads) dst[k] = src[k];
+    for (int k = tid; k < (w1 - w0) / 16; k += kThreads) dst[k] = src[k];
   }
   const uint32_t mbar = su32(&s_mbar);
   if (tid == 0) {
@@ -214,7 +219,10 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_
   fence_after();
   const uint32_t tmem = s_tmem;
   const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);
-  const uint32_t sa_hi = su32(a_hi), sa_lo = su32(a_lo), sw = su32(w_s);
+  const uint32_t sa_hi = su32(a_hi), sa_lo = su32(a_lo);
+  // tile offsets are relative to the whole weight array; with KONLY only K's
+  // part is resident, so its base is shifted back by K's offset
+  const uint32_t sw = su32(w_s) - (KONLY ? (uint32_t)PL::kGemmOff1 : 0u);
   uint32_t phase = 0;
   bool aborted = false;
   bool pending = false;  // a commit whose barrier phase has not been consumed
@@ -256,26 +264,30 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_
       for (int k = 0; k < C; ++k) v[k] = 0.f;
     }
 
-    // ---- product 1: B
-    write_a<P, 0>(v, a_hi, a_lo, tid);
-    fence_proxy_async();
-    fence_before();
-    __syncthreads();
-    if (tid == 0) {
+    if (KONLY) {
+      BApply<P, false>::apply(v);
+    } else {
+      // ---- product 1: B
+      write_a<P, 0>(v, a_hi, a_lo, tid);
+      fence_proxy_async();
+      fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after();
+        issue<P, 0>(tmem, sa_hi, sa_lo, sw);
+        mma_commit(mbar);
+      }
+      pending = true;
+      const bool ok1 = mbar_wait(mbar, phase);
+      if (__syncthreads_or(!ok1)) {
+        aborted = true;
+        break;
+      }
+      phase ^= 1u;
+      pending = false;
       fence_after();
-      issue<P, 0>(tmem, sa_hi, sa_lo, sw);
-      mma_commit(mbar);
+      read_d<P, 0>(tmem_row, v);
     }
-    pending = true;
-    bool ok = mbar_wait(mbar, phase);
-    if (__syncthreads_or(!ok)) {
-      aborted = true;
-      break;
-    }
-    phase ^= 1u;
-    pending = false;
-    fence_after();
-    read_d<P, 0>(tmem_row, v);
     dz_rot<P, true>(v, cax, sax);
     scale_degrees<P, 0>(v, s);
 
@@ -290,8 +302,8 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_
       mma_commit(mbar);
     }
     pending = true;
-    ok = mbar_wait(mbar, phase);
-    if (__syncthreads_or(!ok)) {
+    const bool ok2 = mbar_wait(mbar, phase);
+    if (__syncthreads_or(!ok2)) {
       aborted = true;
       break;
     }
@@ -302,26 +314,30 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_
     scale_degrees<P, 1>(v, s);
     dz_rot<P, false>(v, cax, sax);
 
-    // ---- product 3: B^T
-    write_a<P, 2>(v, a_hi, a_lo, tid);
-    fence_proxy_async();
-    fence_before();
-    __syncthreads();
-    if (tid == 0) {
+    if (KONLY) {
+      BApply<P, true>::apply(v);
+    } else {
+      // ---- product 3: B^T
+      write_a<P, 2>(v, a_hi, a_lo, tid);
+      fence_proxy_async();
+      fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after();
+        issue<P, 2>(tmem, sa_hi, sa_lo, sw);
+        mma_commit(mbar);
+      }
+      pending = true;
+      const bool ok3 = mbar_wait(mbar, phase);
+      if (__syncthreads_or(!ok3)) {
+        aborted = true;
+        break;
+      }
+      phase ^= 1u;
+      pending = false;
       fence_after();
-      issue<P, 2>(tmem, sa_hi, sa_lo, sw);
-      mma_commit(mbar);
+      read_d<P, 2>(tmem_row, v);
     }
-    pending = true;
-    ok = mbar_wait(mbar, phase);
-    if (__syncthreads_or(!ok)) {
-      aborted = true;
-      break;
-    }
-    phase ^= 1u;
-    pending = false;
-    fence_after();
-    read_d<P, 2>(tmem_row, v);
     dz_rot<P, true>(v, caz, saz);
 
     // ---- accumulate runs of equal target (rows of the tile are pairs in list order)
@@ -359,14 +375,19 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_
 template <int P>
 int run(int num_tiles, int64_t num_pairs, const int* pair_tgt, const int* far_src, const int* seg_off, const int* segs,
         const float* mult, const float* centers, float* locals, float* partials, int num_split, const int* split,
-        int* status, cudaStream_t st) {
-  const size_t sm = 128 + 2 * (size_t)kAPartBytes + (size_t)TcPlan<P>::kWBytes;
+        int* status, bool konly, cudaStream_t st) {
+  using PL = TcPlan<P>;
+  const size_t wbytes = konly ? (size_t)(PL::kGemmOff2 - PL::kGemmOff1) : (size_t)PL::kWBytes;
+  const size_t sm = 128 + 2 * (size_t)kAPartBytes + wbytes;
   static_assert(128 * (csize(P) | 1) * 4 <= 2 * kAPartBytes, "output rows must fit in the A region");
-  cudaError_t e = cudaFuncSetAttribute(k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  auto kern = konly ? k_m2l_tc<P, true> : k_m2l_tc<P, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return cuda_status(e);
   if (num_tiles > 0) {
-    const int grid = num_tiles < 148 * 3 ? num_tiles : 148 * 3;
-    k_m2l_tc<P><<<grid, kThreads, sm, st>>>(num_tiles, num_pairs, pair_tgt, far_src, seg_off,
+    // CTAs resident per SM: shared memory bound, and 128 TMEM columns each (<= 512)
+    const int per_sm = sm <= 56 * 1024 ? 4 : 3;
+    const int grid = num_tiles < 148 * per_sm ? num_tiles : 148 * per_sm;
+    kern<<<grid, kThreads, sm, st>>>(num_tiles, num_pairs, pair_tgt, far_src, seg_off,
                                              reinterpret_cast<const int4*>(segs), mult,
                                              reinterpret_cast<const float4*>(centers), locals, partials, status);
     const int rc = launch_status();
@@ -384,11 +405,11 @@ int run(int num_tiles, int64_t num_pairs, const int* pair_tgt, const int* far_sr
 }  // namespace tc
 }  // namespace jb
 
-extern "C" JB_API int jb_m2l_split(int p, int num_tiles, int64_t num_pairs, const int* pair_tgt, const int* far_src,
-                                   const int* seg_off, const int* segs, const float* mult, const float* centers,
-                                   float* locals, float* partials, int num_split, const int* split, int* status,
-                                   void* stream) {
-  if (num_tiles < 0 || num_pairs < 0 || num_split < 0 || !status ||
+extern "C" JB_API int jb_m2l_split(int p, int products, int num_tiles, int64_t num_pairs, const int* pair_tgt,
+                                   const int* far_src, const int* seg_off, const int* segs, const float* mult,
+                                   const float* centers, float* locals, float* partials, int num_split,
+                                   const int* split, int* status, void* stream) {
+  if ((products != 1 && products != 3) || num_tiles < 0 || num_pairs < 0 || num_split < 0 || !status ||
       (num_tiles > 0 && (!pair_tgt || !far_src || !seg_off || !segs || !mult || !centers || !locals)) ||
       (num_split > 0 && (!split || !partials)) || (int64_t)num_tiles * 128 < num_pairs)
     return JB_ERR_ARG;
@@ -397,7 +418,7 @@ extern "C" JB_API int jb_m2l_split(int p, int num_tiles, int64_t num_pairs, cons
 #define JB_TC_CASE(PP) \
   case PP:             \
     return jb::tc::run<PP>(num_tiles, num_pairs, pair_tgt, far_src, seg_off, segs, mult, centers, locals, partials, \
-                           num_split, split, status, st);
+                           num_split, split, status, products == 1, st);
     JB_TC_CASE(2) JB_TC_CASE(3) JB_TC_CASE(4) JB_TC_CASE(5) JB_TC_CASE(6) JB_TC_CASE(7) JB_TC_CASE(8)
 #undef JB_TC_CASE
     default:

@@ -108,6 +108,8 @@ class Pass:
         self.G = float(G)
         self.eps2 = float(eps2)
         self.m2l_mode = int(m2l_mode)
+        # split-BF16 M2L: 1 = only K on the tensor cores (faster), 3 = B, K and B^T
+        self.tc_products = 1
         self.p2p_mode = int(p2p_mode)
         self.ws = Workspace.allocate(dt, self.p)
         self.lib = _lib.lib()
@@ -212,7 +214,7 @@ class Pass:
             }
         T, t, ws = self._tc, self.dt.topo, self.ws
         sc = T["sched"]
-        _lib.check(self.lib.jb_m2l_split(self.p, sc.num_tiles, t.num_far_pairs, _ptr(T["pair_tgt"]),
+        _lib.check(self.lib.jb_m2l_split(self.p, self.tc_products, sc.num_tiles, t.num_far_pairs, _ptr(T["pair_tgt"]),
                                          _ptr(self.dt.far_src), _ptr(T["seg_off"]), _ptr(T["segs"]), _ptr(ws.mult),
                                          _ptr(ws.centers), _ptr(ws.locals), _ptr(T["partials"]),
                                          int(sc.split.shape[0]), _ptr(T["split"]), _ptr(T["status"]), s),
