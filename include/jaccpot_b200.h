@@ -182,6 +182,15 @@ JB_API int jb_m2l_split(int p, int products, int num_tiles, int64_t num_pairs, c
                         const float* centers, float* locals, float* partials, int num_split, const int* split,
                         int* status, void* stream);
 
+/* Split-BF16 far field, unit layout: the same work units / partials / split
+ * list as jb_m2l (thread = unit); step j takes the j-th pair of 128 units as
+ * one tensor-core tile for the K product (B and B^T in registers) and each
+ * thread accumulates its local in registers.  *status as jb_m2l_split.
+ * Orders 2..8. */
+JB_API int jb_m2l_split_units(int p, int num_units, const int* units, const float* mult, const float* centers,
+                              const int* far_src, float* locals, float* partials, int num_split, const int* split,
+                              int* status, void* stream);
+
 /* Downward sweep, one level: for each internal node in [first, last), adds
  * l2l(parent) to both children (l2l_real, operators/real_translations.py:604;
  * _propagate_solidfmm_locals_by_level, runtime/kernels/_l2l.py:210-404). */

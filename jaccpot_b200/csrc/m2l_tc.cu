@@ -402,6 +402,197 @@ int run(int num_tiles, int64_t num_pairs, const int* pair_tgt, const int* far_sr
   return JB_OK;
 }
 
+
+// Unit layout: thread t of a CTA owns work unit t of its group of 128 (at most
+// 64 consecutive pairs of one target, the same units as k_m2l_units, sorted
+// longest first so a group's units have similar lengths).  Step j of the
+// group handles the j-th pair of every unit: each thread runs the rotations,
+// B and B^T in registers, the K product of all 128 pairs is one set of
+// tensor-core tiles (MMA row = thread), and the local accumulates in
+// registers, so no cross-thread reduction is needed.  The next pair's source
+// row is fetched with cp.async into a per-thread shared row while the current
+// one is processed.
+template <int P>
+__global__ void __launch_bounds__(kThreads, 2) k_m2l_tc_units(int num_units, const int4* __restrict__ units,
+                                                              const float* __restrict__ mult,
+                                                              const float4* __restrict__ centers,
+                                                              const int* __restrict__ far_src,
+                                                              float* __restrict__ locals,
+                                                              float* __restrict__ partials, int* __restrict__ status) {
+  using PL = TcPlan<P>;
+  constexpr int C = csize(P), CS = cstride(P), R4 = row4(P);
+  constexpr int WB = PL::kGemmOff2 - PL::kGemmOff1;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  unsigned char* a_hi = sm;
+  unsigned char* a_lo = sm + kAPartBytes;
+  unsigned char* w_s = sm + 2 * kAPartBytes;
+  float4* rows = reinterpret_cast<float4*>(w_s + WB);
+  __shared__ uint64_t s_mbar;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_steps;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  float4* row = rows + tid * R4;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(PL::weights()) + PL::kGemmOff1 / 16;
+    uint4* dst = reinterpret_cast<uint4*>(w_s);
+    for (int k = tid; k < WB / 16; k += kThreads) dst[k] = src[k];
+  }
+  const uint32_t mbar = su32(&s_mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&s_tmem)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+  const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t sa_hi = su32(a_hi), sa_lo = su32(a_lo);
+  const uint32_t sw = su32(w_s) - (uint32_t)PL::kGemmOff1;
+  uint32_t phase = 0;
+  bool aborted = false, pending = false;
+  const int num_groups = (num_units + kThreads - 1) / kThreads;
+
+  for (int g = blockIdx.x; g < num_groups && !aborted; g += gridDim.x) {
+    const int u = g * kThreads + tid;
+    const bool has = u < num_units;
+    const int4 U = has ? units[u] : make_int4(0, 0, 0, -1);
+    const int len = U.z - U.y;
+    // steps = the group's longest unit (units come sorted longest first, but
+    // the maximum is taken anyway so any order is correct)
+    if (tid == 0) s_steps = 0;
+    __syncthreads();
+    if (len > 0) atomicMax(&s_steps, len);
+    __syncthreads();
+    const int steps = s_steps;
+    const float4 ct = has ? centers[U.x] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float acc[C];
+#pragma unroll
+    for (int k = 0; k < C; ++k) acc[k] = 0.f;
+    int sidx = (len > 0) ? far_src[U.y] : 0;
+    if (len > 0) {
+      const float4* src = reinterpret_cast<const float4*>(mult + (size_t)sidx * CS);
+#pragma unroll
+      for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
+      cp_async_commit();
+    }
+    float4 cs = (len > 0) ? centers[sidx] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = 0; j < steps; ++j) {
+      const bool act = j < len;
+      float v[C];
+      float caz = 1.f, saz = 0.f, cax = 1.f, sax = 0.f, s = 1.f;
+      if (act) {
+        cp_async_wait_all();
+#pragma unroll
+        for (int k = 0; k < CS / 4; ++k) {
+          const float4 q = row[k];
+          if (4 * k + 0 < C) v[4 * k + 0] = q.x;
+          if (4 * k + 1 < C) v[4 * k + 1] = q.y;
+          if (4 * k + 2 < C) v[4 * k + 2] = q.z;
+          if (4 * k + 3 < C) v[4 * k + 3] = q.w;
+        }
+        const float dx = ct.x - cs.x, dy = ct.y - cs.y, dz = ct.z - cs.z;
+        if (j + 1 < len) {
+          sidx = __ldg(far_src + U.y + j + 1);
+          const float4* src = reinterpret_cast<const float4*>(mult + (size_t)sidx * CS);
+#pragma unroll
+          for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
+          cp_async_commit();
+          cs = centers[sidx];
+        }
+        float r;
+        align_cs(dx, dy, dz, caz, saz, cax, sax, r);
+        s = 1.f / fmaxf(r, 1.0e-30f);
+        dz_rot<P, false>(v, caz, saz);
+        BApply<P, false>::apply(v);
+        dz_rot<P, true>(v, cax, sax);
+        scale_degrees<P, 0>(v, s);
+      } else {
+#pragma unroll
+        for (int k = 0; k < C; ++k) v[k] = 0.f;
+      }
+      write_a<P, 1>(v, a_hi, a_lo, tid);
+      fence_proxy_async();
+      fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after();
+        issue<P, 1>(tmem, sa_hi, sa_lo, sw);
+        mma_commit(mbar);
+      }
+      pending = true;
+      const bool ok = mbar_wait(mbar, phase);
+      if (__syncthreads_or(!ok)) {
+        aborted = true;
+        break;
+      }
+      phase ^= 1u;
+      pending = false;
+      fence_after();
+      read_d<P, 1>(tmem_row, v);
+      if (act) {
+        scale_degrees<P, 1>(v, s);
+        dz_rot<P, false>(v, cax, sax);
+        BApply<P, true>::apply(v);
+        dz_rot<P, true>(v, caz, saz);
+#pragma unroll
+        for (int k = 0; k < C; ++k) acc[k] += v[k];
+      }
+    }
+    if (aborted) break;
+    if (has && len > 0) {
+      float* dst = (U.w < 0) ? locals + (size_t)U.x * CS : partials + (size_t)U.w * CS;
+#pragma unroll
+      for (int k = 0; k < C; ++k) dst[k] = acc[k];
+#pragma unroll
+      for (int k = C; k < CS; ++k) dst[k] = 0.f;
+    }
+  }
+  if (aborted) {
+    if (tid == 0) atomicExch(status, 1);
+    if (pending) (void)mbar_wait(mbar, phase);
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+template <int P>
+int run_units(int num_units, const int* units, const float* mult, const float* centers, const int* far_src,
+              float* locals, float* partials, int num_split, const int* split, int* status, cudaStream_t st) {
+  using PL = TcPlan<P>;
+  const size_t sm = 128 + 2 * (size_t)kAPartBytes + (size_t)(PL::kGemmOff2 - PL::kGemmOff1) +
+                    (size_t)kThreads * row4(P) * 16;
+  cudaError_t e = cudaFuncSetAttribute(k_m2l_tc_units<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (num_units > 0) {
+    const int groups = (num_units + kThreads - 1) / kThreads;
+    const int grid = groups < 148 * 2 ? groups : 148 * 2;
+    k_m2l_tc_units<P><<<grid, kThreads, sm, st>>>(num_units, reinterpret_cast<const int4*>(units), mult,
+                                                   reinterpret_cast<const float4*>(centers), far_src, locals,
+                                                   partials, status);
+    const int rc = launch_status();
+    if (rc) return rc;
+  }
+  if (num_split > 0) {
+    const int cs = cstride(P);
+    k_m2l_reduce<<<(unsigned)(((int64_t)num_split * cs + 255) / 256), 256, 0, st>>>(
+        num_split, reinterpret_cast<const int4*>(split), partials, locals, cs);
+    return launch_status();
+  }
+  return JB_OK;
+}
+
 }  // namespace tc
 }  // namespace jb
 
@@ -421,6 +612,26 @@ extern "C" JB_API int jb_m2l_split(int p, int products, int num_tiles, int64_t n
                            num_split, split, status, products == 1, st);
     JB_TC_CASE(2) JB_TC_CASE(3) JB_TC_CASE(4) JB_TC_CASE(5) JB_TC_CASE(6) JB_TC_CASE(7) JB_TC_CASE(8)
 #undef JB_TC_CASE
+    default:
+      return JB_ERR_UNSUPPORTED;
+  }
+}
+
+extern "C" JB_API int jb_m2l_split_units(int p, int num_units, const int* units, const float* mult,
+                                         const float* centers, const int* far_src, float* locals, float* partials,
+                                         int num_split, const int* split, int* status, void* stream) {
+  if (num_units < 0 || num_split < 0 || !status ||
+      (num_units > 0 && (!units || !mult || !centers || !far_src || !locals)) ||
+      (num_split > 0 && (!split || !partials || !locals)))
+    return JB_ERR_ARG;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  switch (p) {
+#define JB_TCU_CASE(PP) \
+  case PP:              \
+    return jb::tc::run_units<PP>(num_units, units, mult, centers, far_src, locals, partials, num_split, split, \
+                                 status, st);
+    JB_TCU_CASE(2) JB_TCU_CASE(3) JB_TCU_CASE(4) JB_TCU_CASE(5) JB_TCU_CASE(6) JB_TCU_CASE(7) JB_TCU_CASE(8)
+#undef JB_TCU_CASE
     default:
       return JB_ERR_UNSUPPORTED;
   }

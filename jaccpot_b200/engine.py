@@ -108,7 +108,10 @@ class Pass:
         self.G = float(G)
         self.eps2 = float(eps2)
         self.m2l_mode = int(m2l_mode)
-        # split-BF16 M2L: 1 = only K on the tensor cores (faster), 3 = B, K and B^T
+        # split-BF16 M2L layout: "units" (thread per work unit, K on the tensor
+        # cores), or "tiles" (128 consecutive pairs per tile) with tc_products
+        # 1 (K on the tensor cores) or 3 (B, K and B^T)
+        self.tc_layout = "units"
         self.tc_products = 1
         self.p2p_mode = int(p2p_mode)
         self.ws = Workspace.allocate(dt, self.p)
@@ -196,7 +199,17 @@ class Pass:
                    "jb_m2l")
 
     def _m2l_split(self, s) -> None:
-        """Split-BF16 M2L on the tensor cores (tiles of 128 far pairs)."""
+        """Split-BF16 M2L on the tensor cores."""
+        if self.tc_layout == "units":
+            if getattr(self, "_tc_status", None) is None:
+                self._tc_status = torch.zeros(1, device=self.dt.device, dtype=torch.int32)
+            ws, sc = self.ws, self.m2l_sched
+            _lib.check(self.lib.jb_m2l_split_units(self.p, int(sc.units.shape[0]), _ptr(self.d_m2l_units),
+                                                   _ptr(ws.mult), _ptr(ws.centers), _ptr(self.dt.far_src),
+                                                   _ptr(ws.locals), _ptr(self.m2l_partials),
+                                                   int(sc.split.shape[0]), _ptr(self.d_m2l_split),
+                                                   _ptr(self._tc_status), s), "jb_m2l_split_units")
+            return
         if getattr(self, "_tc", None) is None:
             t, dev = self.dt.topo, self.dt.device
             if self.leaf_range != (0, t.num_leaves):
@@ -223,7 +236,9 @@ class Pass:
     def tc_status(self) -> int:
         """Status word of the tensor-core M2L (0 = ok, 1 = a barrier wait timed out)."""
         T = getattr(self, "_tc", None)
-        return 0 if T is None else int(T["status"].item())
+        st = 0 if T is None else int(T["status"].item())
+        U = getattr(self, "_tc_status", None)
+        return st | (0 if U is None else int(U.item()))
 
     def l2l(self, stream=None) -> None:
         t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)

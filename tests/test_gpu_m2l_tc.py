@@ -26,12 +26,14 @@ def _row_rel(a, b):
     return np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-300)
 
 
-@pytest.mark.parametrize("p,products", [(4, 1), (6, 1), (8, 1), (4, 3), (8, 3)])
-def test_split_m2l_matches_oracle(p, products):
+@pytest.mark.parametrize("p,layout,products", [(4, "units", 1), (6, "units", 1), (8, "units", 1),
+                                               (4, "tiles", 1), (8, "tiles", 1), (4, "tiles", 3), (8, "tiles", 3)])
+def test_split_m2l_matches_oracle(p, layout, products):
     pos, mass = workloads.clustered(32768, seed=5)
     topo = tree.build_topology(pos, mass, leaf_size=32, theta=0.6)
     dt = engine.DeviceTopology(topo, "cuda")
     ps = engine.Pass(dt, p, G=1.0, eps2=0.0, m2l_mode=_lib.JB_M2L_SPLIT_BF16)
+    ps.tc_layout = layout
     ps.tc_products = products
     ps.load_particles(torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda())
     ps.upward()
