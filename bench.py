@@ -117,7 +117,7 @@ def _peaks() -> dict:
 # DRAM bytes (read + write) per launch of the dominant kernels at the bench
 # workload, scaled from single-launch ncu captures of a 1M-particle case by
 # the units processed (far pairs / particle pairs); see profiles/.
-TRAFFIC_PER_UNIT = {"k_m2l_units": 13.0, "k_m2l_tc": None, "k_leaf_units": None}
+TRAFFIC_PER_UNIT = {"k_m2l_units": 12.1, "k_m2l_tc_units": 12.3, "k_leaf_units": 0.0156}
 
 
 def _traffic(kernel: str, units: float | None = None):
@@ -438,9 +438,9 @@ def main() -> None:
         # tensor-core kernel: algorithmic flops against the measured bf16 peak,
         # and the same work against the FP32 pipe, where its per-pair rotations run
         ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
-        roof = {"kernel": f"k_m2l_tc<{cfg['order']}>", "bound": "tensor", "achieved": ach,
+        roof = {"kernel": f"k_m2l_tc_units<{cfg['order']}>", "bound": "tensor", "achieved": ach,
                 "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": ach / peaks["bf16_tflops"],
-                "traffic": _traffic("k_m2l_tc", topo.num_far_pairs), "fp32_pipe_frac": ach / fp32_peak}
+                "traffic": _traffic("k_m2l_tc_units", topo.num_far_pairs), "fp32_pipe_frac": ach / fp32_peak}
     elif stage_names[dom] == "m2l":
         ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
         roof = {"kernel": f"k_m2l_units<{cfg['order']}>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
