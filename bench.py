@@ -192,6 +192,21 @@ def measure_extras(dev, stream) -> dict:
     from jaccpot_b200.solver import FastMultipoleMethod
 
     out = {}
+    # config 1: uniform cube N=16,384, p=4, leaf 16, 'balanced' theta 0.6, vs FP64 direct sum (all targets)
+    pos, mass = workloads.uniform_cube(16384, 0)
+    fmm1 = FastMultipoleMethod(preset="balanced", G=1.0, softening=0.0, device=dev)
+    st1 = fmm1.prepare_state(pos, mass, leaf_size=16, max_order=4)
+    p1 = st1.pass_
+    ms1 = _events_ms(lambda: p1.run(), stream)
+    acc1 = p1.ws.acc4[:, :3].double().cpu().numpy()
+    all_t = torch.arange(16384, dtype=torch.int32, device=dev)
+    ref1 = torch.empty((16384, 4), device=dev, dtype=torch.float64)
+    _lib.check(_lib.lib().jb_direct_f64(16384, p1.ws.pos4.data_ptr(), 16384, all_t.data_ptr(), 1.0, 0.0,
+                                        ref1.data_ptr(), stream.cuda_stream), "jb_direct_f64")
+    e1 = workloads.relative_errors(acc1, ref1[:, :3].cpu().numpy())
+    out["uniform_16k_p4"] = {"ms": ms1, "particles_per_s": 16384 / (ms1 / 1e3),
+                             "err_vs_fp64_direct_p99": float(np.percentile(e1, 99)),
+                             "note": "whole pass, launch-latency bound at this size"}
     n = 1048576
     pos, mass = workloads.plummer(n, 0)
     fmm = FastMultipoleMethod(preset="large_n_gpu", theta=0.6, G=1.0, softening=0.0, device=dev)
@@ -282,12 +297,14 @@ def main() -> None:
     L = topo.num_leaves
     leaf_lo, leaf_hi = (L * rank) // world, (L * (rank + 1)) // world
 
+    # plain: FP32 M2L + FP32 P2P at the maximum order.  chosen: the learned
+    # per-pair gears + FP32 M2L + Kahan-compensated P2P.  split_bf16 (reported):
+    # the tensor-core split-BF16 M2L + Kahan P2P at the maximum order.
     forms = {
         "plain": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_FP32),
-        "chosen": dict(m2l_mode=_lib.JB_M2L_SPLIT_BF16, p2p_mode=_lib.JB_P2P_KAHAN),
+        "split_bf16": dict(m2l_mode=_lib.JB_M2L_SPLIT_BF16, p2p_mode=_lib.JB_P2P_KAHAN),
+        "chosen": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_KAHAN),
     }
-    if world > 1:  # the tensor-core M2L tiles the whole far list
-        forms["chosen"]["m2l_mode"] = _lib.JB_M2L_FP32
     passes = {k: engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, leaf_range=(leaf_lo, leaf_hi), **v)
               for k, v in forms.items()}
     d_pos = torch.from_numpy(pos).to(dev)
@@ -299,14 +316,12 @@ def main() -> None:
     # pass's force scale (prepare-time, like the reference's gear buckets)
     from jaccpot_b200 import gears as gear_mod
     gear_info = None
-    if gear_mod.DEFAULT_MODEL.exists() and world == 1:
+    if gear_mod.DEFAULT_MODEL.exists():
         model = gear_mod.GearModel.load()
-        passes["gears"] = engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, leaf_range=(leaf_lo, leaf_hi),
-                                      m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_KAHAN)
-        passes["gears"].load_particles(d_pos, d_mass)
+        passes["chosen"].load_particles(d_pos, d_mass)
         torch.cuda.synchronize()
         g0 = time.perf_counter()
-        gsel = gear_mod.apply_gears(passes["gears"], model)
+        gsel = gear_mod.apply_gears(passes["chosen"], model)
         torch.cuda.synchronize()
         gear_info = {"select_s": time.perf_counter() - g0, "budget": model.budget,
                      "fraction": (np.bincount(gsel, minlength=len(model.orders)) / max(1, gsel.size)).tolist(),
@@ -359,10 +374,7 @@ def main() -> None:
         torch.cuda.synchronize()
     # plain, then chosen (clocks sampled over the chosen form's timed region)
     ms_plain, stage_plain = timed(passes["plain"], args.steps)
-    if "gears" in passes:
-        ms_gears, stage_gears = timed(passes["gears"], args.steps)
-        gear_info["ms_per_step"] = ms_gears
-        gear_info["stage_ms"] = dict(zip(["upward", "m2l", "l2l", "leaf_eval", "unsort"], map(float, stage_gears)))
+    ms_split, stage_split = timed(passes["split_bf16"], args.steps)
     with ClockSampler(local) as cs:
         ms_chosen, stage_chosen = timed(passes["chosen"], args.steps)
     clocks = cs.summary()
@@ -376,6 +388,7 @@ def main() -> None:
 
     ms_plain = reduce_max(ms_plain)
     ms_chosen = reduce_max(ms_chosen)
+    ms_split = reduce_max(ms_split)
 
     # accuracy of both forms against an FP64 direct sum on sampled targets
     rng = np.random.default_rng(12345)
@@ -393,9 +406,7 @@ def main() -> None:
         e = workloads.relative_errors(got, ref[:, :3].cpu().numpy())
         errs[name] = {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
                       "p99_first_4096": float(np.percentile(e[:4096], 99))}
-    if gear_info is not None:
-        gear_info["err_vs_fp64_direct"] = errs.pop("gears")
-        gear_info["err_bound_met"] = bool(gear_info["err_vs_fp64_direct"]["p99"] <= ERR_BOUND)
+    split_err = errs.pop("split_bf16")
 
     # e2e through the public API from pinned host buffers
     h_pos = torch.from_numpy(pos).pin_memory()
@@ -433,7 +444,7 @@ def main() -> None:
     fp32_peak = 2.0 * 148 * 8 * 256 * iters * 8 / (pe0.elapsed_time(pe1) / 1e3) / 1e12
     stage_names = ["upward", "m2l", "l2l", "leaf_eval", "unsort"]
     dom = int(np.argmax(stage_chosen))
-    split_m2l = forms["chosen"]["m2l_mode"] == _lib.JB_M2L_SPLIT_BF16
+    split_m2l = False
     if stage_names[dom] == "m2l" and split_m2l:
         # tensor-core kernel: algorithmic flops against the measured bf16 peak,
         # and the same work against the FP32 pipe, where its per-pair rotations run
@@ -473,10 +484,17 @@ def main() -> None:
     launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
     if rank == 0:
         cfg.update({
-            "form": "chosen = split-BF16 M2L on tcgen05 (hi/lo 3-product, FP32 accumulation) + Kahan-compensated "
-                    "P2P; plain = FP32 rotate+scale M2L + FP32 P2P; both at the maximum order (the learned-gear "
-                    "variant, FP32 M2L + gears + Kahan P2P, is reported under 'gears')",
+            "form": ("chosen = learned per-pair gears (2,4,6,8) + FP32 rotate+scale M2L + Kahan-compensated P2P"
+                     if gear_info else "chosen = FP32 rotate+scale M2L + Kahan-compensated P2P")
+                    + "; plain = FP32 M2L + FP32 P2P at the maximum order; split_bf16 = tcgen05 split-BF16 M2L "
+                    "(K product on the tensor cores) + Kahan P2P at the maximum order",
             "gears": gear_info,
+            "split_bf16": {
+                "ms_per_step": ms_split, "particles_per_s": n / (ms_split / 1e3),
+                "stage_ms": dict(zip(stage_names, [float(x) for x in stage_split])),
+                "err_vs_fp64_direct": split_err, "err_bound_met": bool(split_err["p99"] <= ERR_BOUND),
+                "m2l_tensor_frac": m2l_flops / (stage_split[1] / 1e3) / 1e12 / peaks["bf16_tflops"],
+                "m2l_fp32_pipe_frac": m2l_flops / (stage_split[1] / 1e3) / 1e12 / fp32_peak},
             "plain_particles_per_s": n / (ms_plain / 1e3),
             "plain_ms_per_step": ms_plain,
             "stage_ms_chosen": dict(zip(stage_names, [float(x) for x in stage_chosen])),

@@ -134,7 +134,7 @@ JB_API int jb_p2m(int p, const float* pos4, int num_nodes, int num_internal, con
 /* Upward sweep, one level: COM of each internal node in [first, last) from
  * its children and M2M (m2m_real, operators/real_translations.py:531;
  * aggregate_m2m_real_by_level, upward/real_tree_expansions.py:216-364). */
-JB_API int jb_m2m_level(int p, int first, int last, const int* left, const int* right,
+JB_API int jb_m2m_level(int p, int first, int last, const int* left, const int* right, const int* node_ranges,
                         float* centers, float* mult, void* stream);
 
 /* Far field (M2L + accumulation) over work units.  units is int4[num_units]:

@@ -83,7 +83,7 @@ _SIGNATURES = {
     "jb_gather_sorted": [_I64, _P, _P, _P, _P, _P],
     "jb_validate_lists": [_I, _I, _P, _P, _P, _P, _I64, _P, _P, _I64, _P, _P],
     "jb_p2m": [_I, _P, _I, _I, _P, _P, _P, _P],
-    "jb_m2m_level": [_I, _I, _I, _P, _P, _P, _P, _P],
+    "jb_m2m_level": [_I, _I, _I, _P, _P, _P, _P, _P, _P],
     "jb_m2l": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_m2l_gears": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_m2l_split": [_I, _I, _I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P],

@@ -339,10 +339,11 @@ JB_API int jb_p2m(int p, const float* pos4, int num_nodes, int num_internal, con
   return dispatch<RunP2M>(p, pos4, num_nodes, num_internal, node_ranges, centers, mult, ST(stream));
 }
 
-JB_API int jb_m2m_level(int p, int first, int last, const int* left, const int* right, float* centers, float* mult,
-                        void* stream) {
-  if (first < 0 || last < first || (last > first && (!left || !right || !centers || !mult))) return JB_ERR_ARG;
-  return dispatch<RunM2M>(p, first, last, left, right, centers, mult, ST(stream));
+JB_API int jb_m2m_level(int p, int first, int last, const int* left, const int* right, const int* node_ranges,
+                        float* centers, float* mult, void* stream) {
+  if (first < 0 || last < first || (last > first && (!left || !right || !node_ranges || !centers || !mult)))
+    return JB_ERR_ARG;
+  return dispatch<RunM2M>(p, first, last, left, right, node_ranges, centers, mult, ST(stream));
 }
 
 JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float* mult, const float* centers,

@@ -124,8 +124,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_p2m(const float4* __res
 // same sum in both lanes), and the even lane writes the parent.
 template <int P>
 __global__ void __launch_bounds__(128) k_m2m_level(int first, int last, const int* __restrict__ left,
-                                                   const int* __restrict__ right, float4* __restrict__ centers,
-                                                   float* __restrict__ mult) {
+                                                   const int* __restrict__ right, const int2* __restrict__ ranges,
+                                                   float4* __restrict__ centers, float* __restrict__ mult) {
   constexpr int C = csize(P), CS = cstride(P);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = first + (tid >> 1);
@@ -142,7 +142,13 @@ __global__ void __launch_bounds__(128) k_m2m_level(int first, int last, const in
       c = make_float4((ca.w * ca.x + cb.w * cb.x) * inv, (ca.w * ca.y + cb.w * cb.y) * inv,
                       (ca.w * ca.z + cb.w * cb.z) * inv, m);
     } else {
-      c = make_float4(0.5f * (ca.x + cb.x), 0.5f * (ca.y + cb.y), 0.5f * (ca.z + cb.z), 0.f);
+      // no mass below: the mean particle position (mutual/topology.py:500-516),
+      // from the children's means weighted by their particle counts
+      const int2 ra = ranges[a], rb = ranges[b];
+      const float na = (float)(ra.y - ra.x + 1), nb = (float)(rb.y - rb.x + 1);
+      const float inv = 1.f / (na + nb);
+      c = make_float4((na * ca.x + nb * cb.x) * inv, (na * ca.y + nb * cb.y) * inv, (na * ca.z + nb * cb.z) * inv,
+                      0.f);
     }
     const float4 cc = side ? cb : ca;
     const float* src = mult + (size_t)(side ? b : a) * CS;
@@ -607,9 +613,10 @@ struct RunP2M {
 
 template <int P>
 struct RunM2M {
-  static int run(int first, int last, const int* left, const int* right, float* centers, float* mult, cudaStream_t st) {
+  static int run(int first, int last, const int* left, const int* right, const int* ranges, float* centers,
+                 float* mult, cudaStream_t st) {
     if (last <= first) return JB_OK;
-    k_m2m_level<P><<<blocks_for(2 * (int64_t)(last - first), 128), 128, 0, st>>>(first, last, left, right,
+    k_m2m_level<P><<<blocks_for(2 * (int64_t)(last - first), 128), 128, 0, st>>>(first, last, left, right, reinterpret_cast<const int2*>(ranges),
                                                                    reinterpret_cast<float4*>(centers), mult);
     return launch_status();
   }

@@ -185,6 +185,10 @@ __device__ __forceinline__ void scale_degrees(float* v, float s) {
   }
 }
 
+// z-axis M2L in scaled form (defined below).
+template <int P>
+__device__ __forceinline__ void zm2l(float* Mz, float* Lz, float r);
+
 // One M2L in place, delta = target - source, as the chain
 //   Dz(az) -> B -> Dz(-ax) -> r^-k -> K -> r^-(n+1) -> Dz(ax) -> B^T -> Dz(-az)
 // which is the reference's rotate-to-z / z-M2L / rotate-back cascade
@@ -208,15 +212,33 @@ __device__ __forceinline__ void m2l_kfold(float* v, float dx, float dy, float dz
     sax = rho * ir;
   }
   const float s = 1.f / fmaxf(r, 1.0e-30f);
-  dz_rot<P, false>(v, caz, saz);
-  BApply<P, false>::apply(v);
-  dz_rot<P, true>(v, cax, sax);
-  scale_degrees<P, 0>(v, s);
-  KFold<P>::apply(v);
-  scale_degrees<P, 1>(v, s);
-  dz_rot<P, false>(v, cax, sax);
-  BApply<P, true>::apply(v);
-  dz_rot<P, true>(v, caz, saz);
+  if constexpr (P <= 8) {
+    dz_rot<P, false>(v, caz, saz);
+    BApply<P, false>::apply(v);
+    dz_rot<P, true>(v, cax, sax);
+    scale_degrees<P, 0>(v, s);
+    KFold<P>::apply(v);
+    scale_degrees<P, 1>(v, s);
+    dz_rot<P, false>(v, cax, sax);
+    BApply<P, true>::apply(v);
+    dz_rot<P, true>(v, caz, saz);
+  } else {
+    // From order 9 the entries of K are no longer exact in FP32 and the
+    // folded product loses the cancellations that the factored form keeps,
+    // so the three constant factors are applied one after the other.
+    dz_rot<P, false>(v, caz, saz);
+    BApply<P, false>::apply(v);
+    dz_rot<P, true>(v, cax, sax);
+    BApply<P, false>::apply(v);
+    float w[csize(P)];
+    zm2l<P>(v, w, r);
+    BApply<P, true>::apply(w);
+    dz_rot<P, false>(w, cax, sax);
+    BApply<P, true>::apply(w);
+    dz_rot<P, true>(w, caz, saz);
+#pragma unroll
+    for (int k = 0; k < csize(P); ++k) v[k] = w[k];
+  }
 }
 
 // z-M2L in scaled form; Mz is the rotated multipole, Lz the z-frame local.

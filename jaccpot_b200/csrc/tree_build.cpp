@@ -216,9 +216,13 @@ void build_topology(Tree& t, const double* pos, const double* mass) {
     const int a = t.left[i], b = t.right[i];
     const double ma = t.mass[a], mb = t.mass[b], sm = ma + mb;
     double c[3];
+    // massless subtree: mean particle position, from the children's means
+    // weighted by their particle counts (as mutual/topology.py:500-516)
+    const double na = (double)(t.ranges[2 * a + 1] - t.ranges[2 * a] + 1);
+    const double nb = (double)(t.ranges[2 * b + 1] - t.ranges[2 * b] + 1);
     for (int k = 0; k < 3; ++k)
       c[k] = sm > 0 ? (ma * t.com[3 * (size_t)a + k] + mb * t.com[3 * (size_t)b + k]) / sm
-                    : 0.5 * (t.com[3 * (size_t)a + k] + t.com[3 * (size_t)b + k]);
+                    : (na * t.com[3 * (size_t)a + k] + nb * t.com[3 * (size_t)b + k]) / (na + nb);
     double r = 0;
     for (int ch : {a, b}) {
       double d2 = 0;

@@ -157,7 +157,8 @@ class Pass:
         lo = dt.level_offsets
         for lev in range(t.num_levels - 1, -1, -1):
             _lib.check(self.lib.jb_m2m_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
-                                             _ptr(ws.centers), _ptr(ws.mult), s), "jb_m2m_level")
+                                             _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.mult), s),
+                       "jb_m2m_level")
 
     def set_gears(self, gears, orders) -> None:
         """Per-far-pair expansion orders: gears[e] indexes `orders` for pair e

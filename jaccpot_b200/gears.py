@@ -235,8 +235,8 @@ def train(X: np.ndarray, labels: np.ndarray, epochs: int = 8, batch: int = 4096,
     return Wq.cpu().numpy(), norm, hist
 
 
-def predict(model: GearModel, X: np.ndarray) -> np.ndarray:
-    """Host-side gear choice from features (same rule as jb_gear_select), for analysis."""
+def probabilities(model: GearModel, X: np.ndarray) -> np.ndarray:
+    """Host-side softmax over the gears from features (the network of jb_gear_select)."""
     W = model.params.astype(np.float64)
     x = (X - model.norm[:N_IN]) * model.norm[N_IN:]
     from scipy.special import erf
@@ -253,7 +253,12 @@ def predict(model: GearModel, X: np.ndarray) -> np.ndarray:
     h2 = gelu(h1 @ W2.T + b2)
     z = h2 @ W3.T + b3
     pr = np.exp(z - z.max(1, keepdims=True))
-    pr /= pr.sum(1, keepdims=True)
+    return pr / pr.sum(1, keepdims=True)
+
+
+def predict(model: GearModel, X: np.ndarray) -> np.ndarray:
+    """Host-side gear choice from features (same rule as jb_gear_select), for analysis."""
+    pr = probabilities(model, X)
     cum = np.cumsum(pr, axis=1)
     g = np.argmax(cum >= model.conf, axis=1)
     g[pr.max(1) < model.min_top] = N_OUT - 1

@@ -411,8 +411,17 @@ static void com(int64_t N, const T* pos, const T* mass, int num_nodes, const int
       sm += mass[i];
       sx += mass[i] * pos[3 * i]; sy += mass[i] * pos[3 * i + 1]; sz += mass[i] * pos[3 * i + 2];
     }
-    const T inv = sm > 0 ? (T)1 / sm : (T)0;
-    out[3 * n] = sx * inv; out[3 * n + 1] = sy * inv; out[3 * n + 2] = sz * inv;
+    if (sm > 0) {
+      const T inv = (T)1 / sm;
+      out[3 * n] = sx * inv; out[3 * n + 1] = sy * inv; out[3 * n + 2] = sz * inv;
+    } else {  // no mass: mean position (mutual/topology.py:500-516)
+      T mx = 0, my = 0, mz = 0;
+      const int cnt = ranges[2 * n + 1] - ranges[2 * n] + 1;
+      for (int i = ranges[2 * n]; i <= ranges[2 * n + 1]; ++i) {
+        mx += pos[3 * i]; my += pos[3 * i + 1]; mz += pos[3 * i + 2];
+      }
+      out[3 * n] = mx / cnt; out[3 * n + 1] = my / cnt; out[3 * n + 2] = mz / cnt;
+    }
   }
 }
 

@@ -47,7 +47,7 @@ def test_argument_errors_without_a_device():
     assert lib.jb_m2l(8, 0, -1, None, None, None, None, None, None, 0, None, None) == 1
     assert lib.jb_m2l(8, 9, 1, 1, 1, 1, 1, 1, 1, 0, None, None) == 8
     assert lib.jb_leaf_eval(8, 64, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1.0, 0.0, 1, 1, 0, None, None) == 1
-    assert lib.jb_m2m_level(8, 5, 4, None, None, None, None, None) == 1
+    assert lib.jb_m2m_level(8, 5, 4, None, None, None, None, None, None) == 1
     assert lib.jb_gather_sorted(-1, None, None, None, None, None) == 1
     assert lib.jb_direct_f64(0, None, 0, None, 1.0, 0.0, None, None) == 1
     info = _lib.TreeInfo()

@@ -105,5 +105,8 @@ def test_training_on_fmm_labels_reduces_the_loss(system):
     Wq, norm, hist = gears.train(X, lab, epochs=6, batch=2048)
     assert hist[-1] < 0.7 * hist[0]
     model = gears.GearModel(params=Wq, norm=norm, budget=1e-5)
-    acc = (gears.predict(model, X) == lab).mean()
-    assert acc > 0.8
+    # the network learns the labels ...
+    acc = (gears.probabilities(model, X).argmax(1) == lab).mean()
+    assert acc > 0.8, acc
+    # ... and the conservative selection rule rarely picks a gear below the label
+    assert (gears.predict(model, X) < lab).mean() < 0.02
