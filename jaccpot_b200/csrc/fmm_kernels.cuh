@@ -220,14 +220,18 @@ __global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units(int num_units, con
 #pragma unroll
   for (int k = 0; k < C; ++k) acc[k] = 0.f;
   const float4 ct = centers[tgt];
-  int s = far_src[e0];
+  // source ids run two pairs ahead and centres one pair ahead of the row
+  // copies, so no load feeds an address in the same iteration
+  const int s0 = far_src[e0];
+  int s1 = (e0 + 1 < e1) ? far_src[e0 + 1] : s0;
   {
-    const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s * rs);
+    const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s0 * rs);
 #pragma unroll
     for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
     cp_async_commit();
   }
-  float4 cs = centers[s];
+  float4 cs = centers[s0];
+  float4 cs1 = centers[s1];
   for (int e = e0; e < e1; ++e) {
     float v[C];
     cp_async_wait_all();
@@ -240,21 +244,20 @@ __global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units(int num_units, con
       if (4 * k + 3 < C) v[4 * k + 3] = q.w;
     }
     // every value read from `row` is in registers: refill it for the next pair
-    const bool more = e + 1 < e1;
-    const int sn = more ? __ldg(far_src + e + 1) : s;
-    if (more) {
-      const float4* src = reinterpret_cast<const float4*>(mult + (size_t)sn * rs);
+    if (e + 1 < e1) {
+      const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s1 * rs);
 #pragma unroll
       for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
       cp_async_commit();
     }
-    const float4 csn = centers[sn];
+    const int s2 = (e + 2 < e1) ? __ldg(far_src + e + 2) : s1;
     if (NEG) m2l_kfold<P>(v, cs.x - ct.x, cs.y - ct.y, cs.z - ct.z);
     else m2l_kfold<P>(v, ct.x - cs.x, ct.y - cs.y, ct.z - cs.z);
 #pragma unroll
     for (int k = 0; k < C; ++k) acc[k] += v[k];
-    s = sn;
-    cs = csn;
+    cs = cs1;
+    cs1 = centers[s2];
+    s1 = s2;
   }
   float* dst = (slot < 0) ? locals + (size_t)tgt * rs : partials + (size_t)slot * rs;
 #pragma unroll
