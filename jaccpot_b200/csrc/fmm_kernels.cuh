@@ -377,28 +377,48 @@ __device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
   return d;
 }
 
-// One chunk of 32 staged sources for this lane's target: sources j = q*G + h,
-// two per step in packed form; the two partial sums are added at the end of
-// the chunk (and into the compensated accumulator when KAHAN).
+// The 32 sources of one chunk, staged per coordinate in the order the lane
+// groups read them: source j sits at position (j % G) * (32 / G) + j / G, so
+// group h's sources are one contiguous run and four of them load as one
+// 16-byte vector that splits into two packed pairs with no register moves.
+struct alignas(16) NearStage {
+  float x[32], y[32], z[32], m[32];
+};
+
+template <int G>
+__device__ __forceinline__ void stage_source(NearStage& s, int j, float4 v) {
+  const int k = (j % G) * (32 / G) + j / G;
+  s.x[k] = v.x;
+  s.y[k] = v.y;
+  s.z[k] = v.z;
+  s.m[k] = v.w;
+}
+
+// One chunk of 32 staged sources for this lane's target: the lane's 32/G
+// sources (j = q*G + h), two per packed step; the two partial sums are added
+// at the end of the chunk (and into the compensated accumulator when KAHAN).
 template <int G, bool KAHAN, bool POT, bool SELF>
-__device__ __forceinline__ void near_chunk(const float4* __restrict__ sp, float4 ti, int h, int self_j, float eps2,
+__device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h, int self_j, float eps2,
                                            NearAcc<KAHAN>& a) {
+  constexpr int R = 32 / G;
+  const ulonglong2* X = reinterpret_cast<const ulonglong2*>(st.x + h * R);
+  const ulonglong2* Y = reinterpret_cast<const ulonglong2*>(st.y + h * R);
+  const ulonglong2* Z = reinterpret_cast<const ulonglong2*>(st.z + h * R);
+  const ulonglong2* M = reinterpret_cast<const ulonglong2*>(st.m + h * R);
   const f32x2 TX = f2(ti.x, ti.x), TY = f2(ti.y, ti.y), TZ = f2(ti.z, ti.z), E2 = f2(eps2, eps2);
   f32x2 AX = f2(0.f, 0.f), AY = AX, AZ = AX, AW = AX;
-#pragma unroll
-  for (int q = 0; q < 32 / G; q += 2) {
-    const int j0 = q * G + h, j1 = j0 + G;
-    const float4 s0 = sp[j0], s1 = sp[j1];
-    const f32x2 dx = f2_sub(TX, f2(s0.x, s1.x));
-    const f32x2 dy = f2_sub(TY, f2(s0.y, s1.y));
-    const f32x2 dz = f2_sub(TZ, f2(s0.z, s1.z));
+  auto step = [&](f32x2 sx, f32x2 sy, f32x2 sz, f32x2 sm, int q) {
+    const f32x2 dx = f2_sub(TX, sx);
+    const f32x2 dy = f2_sub(TY, sy);
+    const f32x2 dz = f2_sub(TZ, sz);
     const f32x2 d2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, E2)));
     float d2a, d2b;
     f2_split(d2, d2a, d2b);
     const f32x2 ir = f2(rsqrtf(d2a), rsqrtf(d2b));
-    f32x2 mir = f2_mul(f2(s0.w, s1.w), ir);
+    f32x2 mir = f2_mul(sm, ir);
     f32x2 w = f2_mul(mir, f2_mul(ir, ir));
     if (SELF) {
+      const int j0 = q * G + h, j1 = j0 + G;
       float m0, m1, w0, w1;
       f2_split(mir, m0, m1);
       f2_split(w, w0, w1);
@@ -413,6 +433,12 @@ __device__ __forceinline__ void near_chunk(const float4* __restrict__ sp, float4
     AY = f2_fma(w, dy, AY);
     AZ = f2_fma(w, dz, AZ);
     if (POT) AW = f2_add(AW, mir);
+  };
+#pragma unroll
+  for (int v = 0; v < R / 4; ++v) {
+    const ulonglong2 x = X[v], y = Y[v], z = Z[v], m = M[v];
+    step(x.x, y.x, z.x, m.x, 4 * v);
+    step(x.y, y.y, z.y, m.y, 4 * v + 2);
   }
   float x0, x1, y0, y1, z0, z1;
   f2_split(AX, x0, x1);
@@ -431,7 +457,7 @@ __device__ __forceinline__ void near_chunk(const float4* __restrict__ sp, float4
 template <int P, int G, bool KAHAN, bool POT>
 __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
                                           const int2* __restrict__ runs, float4 c, const float* sF,
-                                          float4* sP, int lane, float G_, float eps2, float4* __restrict__ out,
+                                          NearStage& sP, int lane, float G_, float eps2, float4* __restrict__ out,
                                           float4* __restrict__ partial) {
   constexpr int C = csize(P);
   const int tl = lane / G, h = lane % G;
@@ -441,7 +467,7 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
   NearAcc<KAHAN> a;
   const bool first = (aux.y & 1) != 0;
   if (first) {
-    sP[lane] = (lane < nt) ? pos4[rg.x + lane] : JB_PAD4;
+    stage_source<G>(sP, lane, (lane < nt) ? pos4[rg.x + lane] : JB_PAD4);
     __syncwarp();
     near_chunk<G, KAHAN, POT, true>(sP, ti, h, tl, eps2, a);
     __syncwarp();
@@ -460,7 +486,7 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
     };
     float4 qn = fetch(lane);
     for (int base = 0; base < nsrc; base += 32) {
-      sP[lane] = qn;
+      stage_source<G>(sP, lane, qn);
       __syncwarp();
       if (base + 32 < nsrc) qn = fetch(base + 32 + lane);
       near_chunk<G, KAHAN, POT, false>(sP, ti, h, -1, eps2, a);
@@ -499,7 +525,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_units(
     float4* __restrict__ out, float4* __restrict__ partial) {
   constexpr int CS = cstride(P);
   __shared__ float sF[kWarpsPerBlock][CS];
-  __shared__ float4 sP[kWarpsPerBlock][32];
+  __shared__ NearStage sP[kWarpsPerBlock];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int u = blockIdx.x * kWarpsPerBlock + warp;
   if (u >= num_units) return;
