@@ -303,15 +303,17 @@ __global__ void __launch_bounds__(128) k_l2l_level(int first, int last, const in
 }
 
 // ---------------------------------------------------------------------------
-// Leaf evaluation over work units: L2P + P2P, warp per unit.
+// Leaf evaluation over work units: the far field (L2P, k_leaf_l2p, warp per
+// leaf) and then the near field (P2P, k_leaf_units, warp per unit).
 //
 // A unit is one target leaf and a slice of its near list, stored as runs of
 // consecutive source leaves (= contiguous particle ranges, runs[r] = (first
 // particle, count)); units[u] = (leaf, first run, end run, source count),
 // aux[u] = (slot, flags).  flags & 1: the unit also does the leaf's self block
-// (diagonal excluded) and its far field (L2P).  slot < 0: the unit covers the
-// whole leaf and writes out_acc4; otherwise it writes partial[slot][lane] and
-// k_leaf_reduce sums a leaf's slots in order.
+// (diagonal excluded), and k_leaf_l2p evaluates the leaf's far field for it.
+// slot < 0: the unit covers the whole leaf and adds its sum to out_acc4;
+// otherwise it writes partial[slot][lane] and k_leaf_reduce adds a leaf's
+// slots to out_acc4 in order.
 //
 // Sources stream through the warp in packed chunks of 32 (the runs are
 // concatenated; each lane tracks its own run), staged in shared memory and
@@ -454,19 +456,16 @@ __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h
   }
 }
 
-template <int P, int G, bool KAHAN, bool POT>
+template <int G, bool KAHAN, bool POT>
 __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
-                                          const int2* __restrict__ runs, float4 c, const float* sF,
-                                          NearStage& sP, int lane, float G_, float eps2, float4* __restrict__ out,
-                                          float4* __restrict__ partial) {
-  constexpr int C = csize(P);
+                                          const int2* __restrict__ runs, NearStage& sP, int lane, float G_,
+                                          float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
   const int tl = lane / G, h = lane % G;
   const int nt = rg.y - rg.x + 1;
   const bool active = tl < nt;
   const float4 ti = active ? pos4[rg.x + tl] : make_float4(0.f, 0.f, 0.f, 0.f);
   NearAcc<KAHAN> a;
-  const bool first = (aux.y & 1) != 0;
-  if (first) {
+  if (aux.y & 1) {
     stage_source<G>(sP, lane, (lane < nt) ? pos4[rg.x + lane] : JB_PAD4);
     __syncwarp();
     near_chunk<G, KAHAN, POT, true>(sP, ti, h, tl, eps2, a);
@@ -500,55 +499,72 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
     if (G >= 2) v[i] += __shfl_xor_sync(0xffffffffu, v[i], 1);
     if (G >= 4) v[i] += __shfl_xor_sync(0xffffffffu, v[i], 2);
   }
-  float4 res = make_float4(-G_ * v[0], -G_ * v[1], -G_ * v[2], -G_ * v[3]);
-  if (first) {
-    float U_[C];
-    solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
-    float phi, g[3];
-    l2p_eval<P>(SmemF{sF}, U_, &phi, g);
-    res.x -= G_ * g[0];
-    res.y -= G_ * g[1];
-    res.z -= G_ * g[2];
-    res.w -= G_ * phi;
-  }
+  const float4 res = make_float4(-G_ * v[0], -G_ * v[1], -G_ * v[2], -G_ * v[3]);
   if (active && h == 0) {
-    if (aux.x < 0) out[rg.x + tl] = res;
-    else partial[(size_t)aux.x * 32 + tl] = res;
+    if (aux.x < 0) {
+      const float4 f = out[rg.x + tl];  // the far field k_leaf_l2p wrote
+      out[rg.x + tl] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
+    } else {
+      partial[(size_t)aux.x * 32 + tl] = res;
+    }
   }
 }
 
-template <int P, bool KAHAN, bool POT>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_units(
+// Near field (P2P) of the work units, added to the far field already in out
+// (whole leaves) or written to the partial rows (split leaves).
+template <bool KAHAN, bool POT>
+static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_leaf_units(
     const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
-    const int2* __restrict__ aux, const int2* __restrict__ runs, const int2* __restrict__ ranges,
-    const float4* __restrict__ centers, const float* __restrict__ locals, float G, float eps2,
-    float4* __restrict__ out, float4* __restrict__ partial) {
-  constexpr int CS = cstride(P);
-  __shared__ float sF[kWarpsPerBlock][CS];
+    const int2* __restrict__ aux, const int2* __restrict__ runs, const int2* __restrict__ ranges, float G,
+    float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
   __shared__ NearStage sP[kWarpsPerBlock];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int u = blockIdx.x * kWarpsPerBlock + warp;
   if (u >= num_units) return;
   const int4 U = units[u];
   const int2 ax = aux[u];
-  const int node = num_internal + U.x;
-  const int2 rg = ranges[node];
-  const float4 c = centers[node];
-  if (ax.y & 1) {
-    for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
-    __syncwarp();
-  }
+  const int2 rg = ranges[num_internal + U.x];
   const int nt = rg.y - rg.x + 1;
   if (nt <= 8)
-    leaf_unit<P, 4, KAHAN, POT>(pos4, rg, U, ax, runs, c, sF[warp], sP[warp], lane, G, eps2, out, partial);
+    leaf_unit<4, KAHAN, POT>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial);
   else if (nt <= 16)
-    leaf_unit<P, 2, KAHAN, POT>(pos4, rg, U, ax, runs, c, sF[warp], sP[warp], lane, G, eps2, out, partial);
+    leaf_unit<2, KAHAN, POT>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial);
   else
-    leaf_unit<P, 1, KAHAN, POT>(pos4, rg, U, ax, runs, c, sF[warp], sP[warp], lane, G, eps2, out, partial);
+    leaf_unit<1, KAHAN, POT>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial);
+}
+
+// Far field (L2P) of every leaf: warp per leaf (its unit with flags & 1),
+// lane per particle, the local expansion staged in shared memory.  Writes
+// out = -G (grad phi, phi); runs before k_leaf_units, which adds the near
+// field.  Kept out of the near-field kernel so that kernel's register count
+// is set by the P2P loop alone (about half, and twice the resident warps).
+template <int P>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
+    const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
+    const int2* __restrict__ aux, const int2* __restrict__ ranges, const float4* __restrict__ centers,
+    const float* __restrict__ locals, float G, float4* __restrict__ out) {
+  constexpr int C = csize(P), CS = cstride(P);
+  __shared__ float sF[kWarpsPerBlock][CS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarpsPerBlock + warp;
+  if (u >= num_units || !(aux[u].y & 1)) return;
+  const int node = num_internal + units[u].x;
+  const int2 rg = ranges[node];
+  for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
+  __syncwarp();
+  if (rg.x + lane > rg.y) return;
+  const float4 c = centers[node], ti = pos4[rg.x + lane];
+  float U_[C];
+  solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
+  float phi, g[3];
+  l2p_eval<P>(SmemF{sF[warp]}, U_, &phi, g);
+  out[rg.x + lane] = make_float4(-G * g[0], -G * g[1], -G * g[2], -G * phi);
 }
 
 // Sums the partial results of leaves whose work was split: split[i] = (leaf,
 // first slot, number of slots, unused).  Thread per (leaf, particle slot).
+// ACCUM: the sum starts from what out holds (the far field), else from zero.
+template <bool ACCUM>
 static __global__ void __launch_bounds__(256) k_leaf_reduce(int num_split, const int4* __restrict__ split, int num_internal,
                                                      const int2* __restrict__ ranges, const float4* __restrict__ partial,
                                                      float4* __restrict__ out) {
@@ -558,7 +574,7 @@ static __global__ void __launch_bounds__(256) k_leaf_reduce(int num_split, const
   const int4 sp = split[i];
   const int2 rg = ranges[num_internal + sp.x];
   if (rg.x + l > rg.y) return;
-  float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 a = ACCUM ? out[rg.x + l] : make_float4(0.f, 0.f, 0.f, 0.f);
   for (int q = 0; q < sp.z; ++q) {
     const float4 v = partial[(size_t)(sp.y + q) * 32 + l];
     a.x += v.x;
@@ -691,10 +707,10 @@ template <int P>
 struct RunLeafEval {
   template <bool K, bool PT>
   static void go(unsigned nb, cudaStream_t st, const float4* pos4, int num_internal, int num_units, const int4* units,
-                 const int2* aux, const int2* runs, const int2* ranges, const float4* centers, const float* locals,
-                 float G, float eps2, float4* out, float4* partial) {
-    k_leaf_units<P, K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs, ranges,
-                                                               centers, locals, G, eps2, out, partial);
+                 const int2* aux, const int2* runs, const int2* ranges, float G, float eps2, float4* out,
+                 float4* partial) {
+    k_leaf_units<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs, ranges,
+                                                            G, eps2, out, partial);
   }
   static int run(int mode, const float* pos4, int num_internal, int num_units, const int* units, const int* aux,
                  const int* runs, const int* ranges, const float* centers, const float* locals, float G, float eps2,
@@ -706,19 +722,22 @@ struct RunLeafEval {
       auto a2 = reinterpret_cast<const int2*>(aux);
       auto a3 = reinterpret_cast<const int2*>(runs);
       auto a4 = reinterpret_cast<const int2*>(ranges);
-      auto a5 = reinterpret_cast<const float4*>(centers);
       auto o = reinterpret_cast<float4*>(out);
       auto pt = reinterpret_cast<float4*>(partial);
+      k_leaf_l2p<P><<<nb, 32 * kWarpsPerBlock, 0, st>>>(a0, num_internal, num_units, a1, a2, a4,
+                                                        reinterpret_cast<const float4*>(centers), locals, G, o);
+      int rc = launch_status();
+      if (rc) return rc;
       const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
-      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
-      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
-      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
-      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, a5, locals, G, eps2, o, pt);
-      const int rc = launch_status();
+      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
+      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
+      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
+      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
+      rc = launch_status();
       if (rc) return rc;
     }
     if (num_split > 0) {
-      k_leaf_reduce<<<blocks_for((int64_t)num_split * 32, 256), 256, 0, st>>>(
+      k_leaf_reduce<true><<<blocks_for((int64_t)num_split * 32, 256), 256, 0, st>>>(
           num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(ranges),
           reinterpret_cast<const float4*>(partial), reinterpret_cast<float4*>(out));
       return launch_status();
