@@ -99,6 +99,25 @@ JB_API int jb_tree_info(const jb_tree* t, jb_tree_info_t* info);
 JB_API int jb_tree_copy(const jb_tree* t, int field, void* dst);
 JB_API void jb_tree_free(jb_tree* t);
 
+/* The same tree and lists built on the GPU (csrc/tree_gpu.cu), bit for bit
+ * the arrays jb_tree_build returns for the same float64 inputs: Morton codes
+ * + LSD radix sort, breadth-first radix split, FP64 COM / radii, breadth-first
+ * dual walk, CSR by key sort.  Replaces the same yggdrax calls
+ * (runtime/fmm_prepare.py:823, :1411).  pos (n,3) and mass (n,) are DEVICE
+ * float64 arrays; the handle owns device copies of every JB_TREE_* field.
+ * Allocates device memory; synchronises the stream (the walk sizes its
+ * buffers from counts read back level by level).                           */
+typedef struct jb_dtree jb_dtree;
+JB_API int jb_tree_build_device(int64_t n, const double* pos, const double* mass, int leaf_size,
+                                double theta, void* stream, jb_dtree** out);
+JB_API int jb_dtree_info(const jb_dtree* t, jb_tree_info_t* info);
+/* Device pointer of a JB_TREE_* field (NULL for a bad field); valid until
+ * jb_dtree_free. */
+JB_API const void* jb_dtree_field(const jb_dtree* t, int field);
+/* Synchronous device-to-host copy of a field (sizes as for jb_tree_copy). */
+JB_API int jb_dtree_copy(const jb_dtree* t, int field, void* dst);
+JB_API void jb_dtree_free(jb_dtree* t);
+
 /* ------------------------------------------------------------------------ */
 /* Device pass.                                                             */
 /* ------------------------------------------------------------------------ */

@@ -78,6 +78,11 @@ _SIGNATURES = {
     "jb_tree_info": [_P, ctypes.POINTER(TreeInfo)],
     "jb_tree_copy": [_P, _I, _P],
     "jb_tree_free": [_P],
+    "jb_tree_build_device": [_I64, _P, _P, _I, _D, _P, ctypes.POINTER(_P)],
+    "jb_dtree_info": [_P, ctypes.POINTER(TreeInfo)],
+    "jb_dtree_field": [_P, _I],
+    "jb_dtree_copy": [_P, _I, _P],
+    "jb_dtree_free": [_P],
     "jb_coeff_stride": [_I],
     "jb_last_cuda_error": [],
     "jb_gather_sorted": [_I64, _P, _P, _P, _P, _P],
@@ -128,7 +133,8 @@ def lib() -> ctypes.CDLL:
             fn = getattr(lb, name)
             fn.argtypes = args
             fn.restype = ctypes.c_char_p if name == "jb_last_cuda_error" else (
-                None if name == "jb_tree_free" else ctypes.c_int)
+                None if name in ("jb_tree_free", "jb_dtree_free") else (
+                    ctypes.c_void_p if name == "jb_dtree_field" else ctypes.c_int))
         _lib = lb
     return _lib
 

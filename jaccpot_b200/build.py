@@ -83,6 +83,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         obj = OBJ_DIR / f"{name}.o"
         if _stale(obj, _deps(src)):
             jobs_todo.append([nvcc, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+    # The device tree build reproduces the host builder's FP64 arithmetic
+    # operation for operation, so nothing in it may be contracted into an FMA.
+    tg_src, tg_obj = CSRC / "tree_gpu.cu", OBJ_DIR / "tree_gpu.o"
+    if _stale(tg_obj, [tg_src, INCLUDE / "jaccpot_b200.h"]):
+        jobs_todo.append([nvcc, *NVCC_FLAGS, "-fmad=false", "-c", str(tg_src), "-o", str(tg_obj)])
     tb_obj = OBJ_DIR / "tree_build.o"
     if _stale(tb_obj, _deps(CSRC / "tree_build.cpp")):
         jobs_todo.append([_cxx(), "-O3", "-fopenmp", "-fPIC", "-std=c++17", "-I", str(INCLUDE),

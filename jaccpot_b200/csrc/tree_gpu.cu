@@ -1,0 +1,959 @@
+// Device prepare: the tree and the interaction lists of tree_build.cpp, built
+// on the GPU from device arrays, bit for bit the same arrays.
+//
+// Same algorithm as the host stand-in for yggdrax (tree_build.cpp; used where
+// jaccpot calls yggdrax at runtime/fmm_prepare.py:823 and :1411):
+//   1. bounding cube, 63-bit Morton codes (21 bits per axis), stable sort of
+//      (code, input index)                       -> k_bbox_*, k_morton, radix sort;
+//   2. breadth-first radix split: a range of more than leaf_size particles is
+//      split at the highest differing code bit (duplicates at the midpoint);
+//      internal ids in BFS order, leaves renumbered in particle order
+//                                                -> one k_level_* pair per level;
+//   3. FP64 COM and bounding radius, leaves from their particles, internal
+//      nodes from their children, deepest level first -> k_leaf_com, k_internal_com;
+//   4. dual walk from (root, root): (A, A) opens into its children's three
+//      pairs; (A, B) is far when d^2 > 0 and (r_A + r_B)^2 <= theta^2 d^2,
+//      near when both are leaves, else the larger-radius internal node is
+//      split; far and near pairs are emitted in both directions
+//                                                -> breadth-first k_walk_*;
+//   5. target-major CSR with sources ascending   -> key radix sort + row counts.
+// The walk visits the same pairs as the host's depth-first recursion (every
+// decision depends on the pair alone); sorting the emitted pairs gives the
+// host's CSR order.  The floating-point steps are the host's, operation for
+// operation, and this file is compiled with -fmad=false so no multiply-add is
+// contracted: the COM, radii and MAC decisions are the host's to the last bit.
+//
+// Work decomposition: thread per particle / range / node / pair; prefix sums
+// by a three-kernel tile scan; the sort is an LSD radix sort with 8-bit digits
+// whose scatter ranks keys by warp match masks in index order (stable).  The
+// only atomics are shared-memory digit counts, row counts and a max, all
+// order-independent, so every output is run-to-run identical.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "../../include/jaccpot_b200.h"
+
+namespace jb {
+int cuda_status(cudaError_t e);
+}
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Device buffers owned by the builder / the handle.
+// ---------------------------------------------------------------------------
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t alloc(size_t b) {
+    release();
+    if (b == 0) b = 16;
+    const cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    else p = nullptr;
+    return e;
+  }
+  // Grows to at least b bytes, keeping the first `keep` bytes.
+  cudaError_t grow(size_t b, size_t keep, cudaStream_t st) {
+    if (b <= bytes) return cudaSuccess;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, b);
+    if (e != cudaSuccess) return e;
+    if (keep && p) {
+      e = cudaMemcpyAsync(q, p, keep, cudaMemcpyDeviceToDevice, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        cudaFree(q);
+        return e;
+      }
+    }
+    release();
+    p = q;
+    bytes = b;
+    return cudaSuccess;
+  }
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+struct Fail {
+  int rc;
+};
+
+inline void ck(cudaError_t e) {
+  if (e != cudaSuccess) throw Fail{jb::cuda_status(e)};
+}
+inline void ck_launch() { ck(cudaGetLastError()); }
+
+inline unsigned nblocks(int64_t n, int per) { return (unsigned)std::max<int64_t>(1, (n + per - 1) / per); }
+
+// ---------------------------------------------------------------------------
+// Exclusive prefix sum: tiles of 4096 (1024 threads x 4), tile totals scanned
+// recursively, then added back.
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 1024, kScanItems = 4, kScanTile = kScanThreads * kScanItems;
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict__ in, T* __restrict__ out,
+                                                             T* __restrict__ tile_sums, int64_t n) {
+  __shared__ T warp_sums[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  T v[kScanItems];
+  T s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = (base + i < n) ? in[base + i] : T(0);
+    s += v[i];
+  }
+  T incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const T w = warp_sums[lane];
+    T wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(kFull, wi, o);
+      if (lane >= o) wi += y;
+    }
+    warp_sums[lane] = wi - w;
+  }
+  __syncthreads();
+  T run = warp_sums[warp] + incl - s;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n) out[base + i] = run;
+    run += v[i];
+  }
+  if (threadIdx.x == kScanThreads - 1) tile_sums[blockIdx.x] = run;
+}
+
+template <typename T>
+__global__ void k_scan_add(T* __restrict__ out, const T* __restrict__ tile_off, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && i >= kScanTile) out[i] += tile_off[i / kScanTile];
+}
+
+template <typename T>
+__global__ void k_scan_total(const T* __restrict__ in, const T* __restrict__ out, int64_t n, T* __restrict__ total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *total = n > 0 ? out[n - 1] + in[n - 1] : T(0);
+}
+
+// ---------------------------------------------------------------------------
+// LSD radix sort of 64-bit keys (optional int32 values), 8-bit digits.
+// A block owns 2,048 consecutive keys; warp w owns 256 of them, in rounds of
+// 32.  The scatter ranks a key among the same-digit keys before it by the
+// warp's match mask, so equal digits keep their order (stable).
+// ---------------------------------------------------------------------------
+constexpr int kRsThreads = 256, kRsWarps = kRsThreads / 32, kRsRounds = 8, kRsTile = kRsThreads * kRsRounds;
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint64_t* __restrict__ keys, int64_t n, int shift,
+                                                        int* __restrict__ hist, int nblk) {
+  __shared__ int cnt[256];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * kRsTile + warp * (32 * kRsRounds);
+#pragma unroll
+  for (int r = 0; r < kRsRounds; ++r) {
+    const int64_t i = base + r * 32 + lane;
+    if (i < n) atomicAdd(&cnt[(int)((keys[i] >> shift) & 255u)], 1);
+  }
+  __syncthreads();
+  hist[(int64_t)threadIdx.x * nblk + blockIdx.x] = cnt[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint64_t* __restrict__ kin, const int* __restrict__ vin,
+                                                           uint64_t* __restrict__ kout, int* __restrict__ vout, int64_t n,
+                                                           int shift, const int* __restrict__ hist_off, int nblk) {
+  __shared__ int wcnt[kRsWarps][256];
+  for (int t = threadIdx.x; t < kRsWarps * 256; t += kRsThreads) (&wcnt[0][0])[t] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t base = (int64_t)blockIdx.x * kRsTile + warp * (32 * kRsRounds);
+  uint64_t k[kRsRounds];
+  int v[kRsRounds], d[kRsRounds];
+#pragma unroll
+  for (int r = 0; r < kRsRounds; ++r) {
+    const int64_t i = base + r * 32 + lane;
+    const bool ok = i < n;
+    k[r] = ok ? kin[i] : 0ull;
+    v[r] = (ok && vin) ? vin[i] : 0;
+    d[r] = ok ? (int)((k[r] >> shift) & 255u) : 256;
+    const unsigned peers = __match_any_sync(kFull, d[r]);
+    if (d[r] < 256 && lane == __ffs(peers) - 1) wcnt[warp][d[r]] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  {
+    const int t = threadIdx.x;  // one digit per thread
+    int run = hist_off[(int64_t)t * nblk + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < kRsWarps; ++w) {
+      const int c = wcnt[w][t];
+      wcnt[w][t] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kRsRounds; ++r) {
+    const unsigned peers = __match_any_sync(kFull, d[r]);
+    if (d[r] < 256) {
+      const int pos = wcnt[warp][d[r]] + __popc(peers & lt);
+      kout[pos] = k[r];
+      if (vout) vout[pos] = v[r];
+    }
+    __syncwarp();
+    if (d[r] < 256 && lane == __ffs(peers) - 1) wcnt[warp][d[r]] += __popc(peers);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Builder state.
+// ---------------------------------------------------------------------------
+struct Scratch {
+  DBuf scan_tiles;  // tile sums of every recursion level
+  DBuf total;       // 8 x int64 result words
+  DBuf hist;        // radix histograms
+};
+
+// Tile-sum scratch of a scan of n elements: (2 * tiles + 8) words per
+// recursion level.
+template <typename T>
+size_t scan_scratch_bytes(int64_t n) {
+  size_t b = 0;
+  while (n > 0) {
+    const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+    b += (size_t)(2 * tiles + 8) * sizeof(T);
+    if (tiles <= 1) break;
+    n = tiles;
+  }
+  return b;
+}
+
+template <typename T>
+void scan_rec(const T* in, T* out, int64_t n, T* total, T* scratch, cudaStream_t st) {
+  const int64_t tiles = (n + kScanTile - 1) / kScanTile;
+  T* sums = scratch;
+  T* sums_x = sums + tiles;
+  k_scan_tiles<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, sums, n);
+  ck_launch();
+  if (tiles > 1) {
+    scan_rec<T>(sums, sums_x, tiles, nullptr, sums + 2 * tiles + 8, st);
+    k_scan_add<T><<<nblocks(n, 256), 256, 0, st>>>(out, sums_x, n);
+    ck_launch();
+  }
+  if (total) {
+    k_scan_total<T><<<1, 32, 0, st>>>(in, out, n, total);
+    ck_launch();
+  }
+}
+
+// out = exclusive prefix sum of in[0, n); *total (when given) = the sum.
+template <typename T>
+void exclusive_scan(const T* in, T* out, int64_t n, T* total, Scratch& s, cudaStream_t st) {
+  if (n <= 0) {
+    if (total) ck(cudaMemsetAsync(total, 0, sizeof(T), st));
+    return;
+  }
+  const size_t need = scan_scratch_bytes<T>(n);
+  if (need > s.scan_tiles.bytes) ck(s.scan_tiles.grow(std::max(need, 2 * s.scan_tiles.bytes), 0, st));
+  scan_rec<T>(in, out, n, total, s.scan_tiles.as<T>(), st);
+}
+
+template <typename T>
+T read_word(const T* d, cudaStream_t st) {
+  T h;
+  ck(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, st));
+  ck(cudaStreamSynchronize(st));
+  return h;
+}
+
+// Sorts keys[0, n) (and values) on bits [0, bits); the result is left in
+// (k0, v0).  k1 / v1 are scratch of the same size.
+void radix_sort(uint64_t* k0, int* v0, uint64_t* k1, int* v1, int64_t n, int bits, Scratch& s, cudaStream_t st) {
+  if (n <= 1) return;
+  const int nblk = (int)((n + kRsTile - 1) / kRsTile);
+  const size_t hbytes = (size_t)256 * nblk * sizeof(int);
+  if (s.hist.bytes < 2 * hbytes) ck(s.hist.alloc(2 * hbytes));
+  int* hist = s.hist.as<int>();
+  int* hoff = hist + (size_t)256 * nblk;
+  const int passes = (bits + 7) / 8;
+  for (int ps = 0; ps < passes; ++ps) {
+    const int shift = 8 * ps;
+    k_rs_hist<<<nblk, kRsThreads, 0, st>>>(k0, n, shift, hist, nblk);
+    ck_launch();
+    exclusive_scan<int>(hist, hoff, (int64_t)256 * nblk, nullptr, s, st);
+    k_rs_scatter<<<nblk, kRsThreads, 0, st>>>(k0, v0, k1, v1, n, shift, hoff, nblk);
+    ck_launch();
+    std::swap(k0, k1);
+    std::swap(v0, v1);
+  }
+  if (passes & 1) {  // result sits in the scratch pair: copy back
+    ck(cudaMemcpyAsync(k1, k0, (size_t)n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+    if (v0 && v1) ck(cudaMemcpyAsync(v1, v0, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 1. Morton codes.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_bbox_partial(const double* __restrict__ pos, int64_t n, double* __restrict__ part) {
+  __shared__ double sm[6][256];
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < 3; ++k) {
+      const double x = pos[3 * i + k];
+      lo[k] = fmin(lo[k], x);
+      hi[k] = fmax(hi[k], x);
+    }
+  for (int k = 0; k < 3; ++k) {
+    sm[k][threadIdx.x] = lo[k];
+    sm[3 + k][threadIdx.x] = hi[k];
+  }
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int k = 0; k < 3; ++k) {
+        sm[k][threadIdx.x] = fmin(sm[k][threadIdx.x], sm[k][threadIdx.x + w]);
+        sm[3 + k][threadIdx.x] = fmax(sm[3 + k][threadIdx.x], sm[3 + k][threadIdx.x + w]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) part[6 * blockIdx.x + threadIdx.x] = sm[threadIdx.x][0];
+}
+
+__global__ void k_bbox_final(const double* __restrict__ part, int nblk, double* __restrict__ bb) {
+  if (threadIdx.x >= 6) return;
+  const int k = threadIdx.x;
+  double v = part[k];
+  for (int b = 1; b < nblk; ++b) v = (k < 3) ? fmin(v, part[6 * b + k]) : fmax(v, part[6 * b + k]);
+  bb[k] = v;
+}
+
+__device__ __forceinline__ uint64_t spread21(uint64_t v) {
+  v &= 0x1fffffULL;
+  v = (v | (v << 32)) & 0x1f00000000ffffULL;
+  v = (v | (v << 16)) & 0x1f0000ff0000ffULL;
+  v = (v | (v << 8)) & 0x100f00f00f00f00fULL;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ULL;
+  v = (v | (v << 2)) & 0x1249249249249249ULL;
+  return v;
+}
+
+__global__ void k_morton(const double* __restrict__ pos, int64_t n, const double* __restrict__ bb,
+                         uint64_t* __restrict__ codes, int* __restrict__ idx) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double ext = fmax(bb[3] - bb[0], fmax(bb[4] - bb[1], bb[5] - bb[2]));
+  if (!(ext > 0)) ext = 1.0;
+  const double qmax = (double)((1 << 21) - 1);
+  const double scale = qmax / ext;
+  uint64_t q[3];
+  for (int k = 0; k < 3; ++k) {
+    double f = (pos[3 * i + k] - bb[k]) * scale;
+    f = fmin(fmax(f, 0.0), qmax);
+    q[k] = (uint64_t)f;
+  }
+  codes[i] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+  idx[i] = (int)i;
+}
+
+// ---------------------------------------------------------------------------
+// 2. Breadth-first radix split.
+// ---------------------------------------------------------------------------
+struct Pending {
+  int s, e, parent, side;
+};
+
+__device__ __forceinline__ int split_point(const uint64_t* __restrict__ c, int s, int e) {
+  const uint64_t a = c[s], b = c[e];
+  if (a == b) return (int)(((int64_t)s + e + 1) / 2);
+  const int bit = 63 - __clzll((long long)(a ^ b));
+  const uint64_t mask = 1ULL << bit;
+  int lo = s + 1, hi = e;  // first index whose code has `bit` set
+  while (lo < hi) {
+    const int mid = lo + (hi - lo) / 2;
+    if (c[mid] & mask) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+__global__ void k_level_flags(const Pending* __restrict__ fr, int F, int leaf_size, int* __restrict__ flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < F) flag[i] = (fr[i].e - fr[i].s + 1 > leaf_size) ? 1 : 0;
+}
+
+struct LeafRec {
+  int s, e, parent, side, level;
+};
+
+__global__ void k_level_emit(const Pending* __restrict__ fr, int F, const int* __restrict__ flag,
+                             const int* __restrict__ rank, int int_base, int leaf_base, int level,
+                             const uint64_t* __restrict__ codes, int* __restrict__ int_ranges, int* __restrict__ int_parent,
+                             int* __restrict__ int_level, int* __restrict__ left, int* __restrict__ right,
+                             Pending* __restrict__ next, LeafRec* __restrict__ leaves) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F) return;
+  const Pending pd = fr[i];
+  const int r = rank[i];
+  if (flag[i]) {
+    const int id = int_base + r;
+    int_ranges[2 * id] = pd.s;
+    int_ranges[2 * id + 1] = pd.e;
+    int_parent[id] = pd.parent;
+    int_level[id] = level;
+    left[id] = -1;
+    right[id] = -1;
+    if (pd.parent >= 0) (pd.side == 0 ? left : right)[pd.parent] = id;
+    const int sp = split_point(codes, pd.s, pd.e);
+    next[2 * r] = Pending{pd.s, sp - 1, id, 0};
+    next[2 * r + 1] = Pending{sp, pd.e, id, 1};
+  } else {
+    leaves[leaf_base + (i - r)] = LeafRec{pd.s, pd.e, pd.parent, pd.side, level};
+  }
+}
+
+__global__ void k_mark_leaf_starts(const LeafRec* __restrict__ lv, int L, int* __restrict__ flag) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < L) flag[lv[j].s] = 1;
+}
+
+__global__ void k_leaf_of(const int* __restrict__ flag, const int* __restrict__ lidx, int64_t n, int* __restrict__ leaf_of) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) leaf_of[i] = lidx[i] + flag[i] - 1;
+}
+
+__global__ void k_place_leaves(const LeafRec* __restrict__ lv, int L, const int* __restrict__ lidx, int num_internal,
+                               int* __restrict__ ranges, int* __restrict__ parent, int* __restrict__ level,
+                               int* __restrict__ left, int* __restrict__ right) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= L) return;
+  const LeafRec r = lv[j];
+  const int id = num_internal + lidx[r.s];
+  ranges[2 * id] = r.s;
+  ranges[2 * id + 1] = r.e;
+  parent[id] = r.parent;
+  level[id] = r.level;
+  if (r.parent >= 0) (r.side == 0 ? left : right)[r.parent] = id;
+}
+
+__global__ void k_widen_perm(const int* __restrict__ v, int64_t n, int64_t* __restrict__ perm) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) perm[i] = v[i];
+}
+
+__global__ void k_max_occupancy(const int* __restrict__ ranges, int num_internal, int L, int* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= L) return;
+  const int id = num_internal + j;
+  atomicMax(out, ranges[2 * id + 1] - ranges[2 * id] + 1);
+}
+
+// ---------------------------------------------------------------------------
+// 3. COM and bounding radii (FP64, the host's operation order).
+// ---------------------------------------------------------------------------
+__global__ void k_leaf_com(int L, int num_internal, const int* __restrict__ ranges, const int* __restrict__ perm,
+                           const double* __restrict__ pos, const double* __restrict__ mass, double* __restrict__ com,
+                           double* __restrict__ radius, double* __restrict__ nmass) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= L) return;
+  const int id = num_internal + j;
+  const int s = ranges[2 * id], e = ranges[2 * id + 1];
+  double sm = 0, sx = 0, sy = 0, sz = 0;
+  for (int i = s; i <= e; ++i) {
+    const int64_t o = perm[i];
+    const double m = mass[o];
+    sm += m;
+    sx += m * pos[3 * o];
+    sy += m * pos[3 * o + 1];
+    sz += m * pos[3 * o + 2];
+  }
+  double c[3];
+  if (sm > 0) {
+    c[0] = sx / sm;
+    c[1] = sy / sm;
+    c[2] = sz / sm;
+  } else {  // massless leaf: mean position of its particles
+    c[0] = c[1] = c[2] = 0;
+    for (int i = s; i <= e; ++i)
+      for (int k = 0; k < 3; ++k) c[k] += pos[3 * (int64_t)perm[i] + k];
+    for (int k = 0; k < 3; ++k) c[k] /= (double)(e - s + 1);
+  }
+  double rmax = 0;
+  for (int i = s; i <= e; ++i) {
+    const int64_t o = perm[i];
+    const double dx = pos[3 * o] - c[0], dy = pos[3 * o + 1] - c[1], dz = pos[3 * o + 2] - c[2];
+    rmax = fmax(rmax, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+  nmass[id] = sm;
+  radius[id] = rmax;
+  for (int k = 0; k < 3; ++k) com[3 * (int64_t)id + k] = c[k];
+}
+
+__global__ void k_internal_com(int first, int last, const int* __restrict__ left, const int* __restrict__ right,
+                               const int* __restrict__ ranges, double* __restrict__ com, double* __restrict__ radius,
+                               double* __restrict__ nmass) {
+  const int i = first + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= last) return;
+  const int a = left[i], b = right[i];
+  const double ma = nmass[a], mb = nmass[b], sm = ma + mb;
+  const double na = (double)(ranges[2 * a + 1] - ranges[2 * a] + 1);
+  const double nb = (double)(ranges[2 * b + 1] - ranges[2 * b] + 1);
+  double c[3];
+  for (int k = 0; k < 3; ++k)
+    c[k] = sm > 0 ? (ma * com[3 * (int64_t)a + k] + mb * com[3 * (int64_t)b + k]) / sm
+                  : (na * com[3 * (int64_t)a + k] + nb * com[3 * (int64_t)b + k]) / (na + nb);
+  double r = 0;
+  const int ch[2] = {a, b};
+  for (int q = 0; q < 2; ++q) {
+    double d2 = 0;
+    for (int k = 0; k < 3; ++k) {
+      const double dd = com[3 * (int64_t)ch[q] + k] - c[k];
+      d2 += dd * dd;
+    }
+    r = fmax(r, sqrt(d2) + radius[ch[q]]);
+  }
+  nmass[i] = sm;
+  radius[i] = r;
+  for (int k = 0; k < 3; ++k) com[3 * (int64_t)i + k] = c[k];
+}
+
+// ---------------------------------------------------------------------------
+// 4. Dual walk, breadth-first over node pairs.
+// ---------------------------------------------------------------------------
+enum : int { kNone = 0, kSelf = 1, kFar = 2, kNear = 3, kSplitA = 4, kSplitB = 5 };
+
+struct WalkCtx {
+  const int* left;
+  const int* right;
+  const double* com;
+  const double* radius;
+  int num_internal;
+  double theta2;
+};
+
+__device__ __forceinline__ int walk_decide(const WalkCtx& w, int a, int b) {
+  const bool la = a >= w.num_internal, lb = b >= w.num_internal;
+  if (a == b) return la ? kNone : kSelf;
+  double d2 = 0;
+  for (int k = 0; k < 3; ++k) {
+    const double dd = w.com[3 * (int64_t)a + k] - w.com[3 * (int64_t)b + k];
+    d2 += dd * dd;
+  }
+  const double ra = w.radius[a], rb = w.radius[b];
+  const double rs = ra + rb;
+  if (d2 > 0 && rs * rs <= w.theta2 * d2) return kFar;
+  if (la && lb) return kNear;
+  return (!la && (lb || ra >= rb)) ? kSplitA : kSplitB;
+}
+
+__global__ void k_walk_count(const int2* __restrict__ fr, int F, WalkCtx w, int* __restrict__ cc, int* __restrict__ cf,
+                             int* __restrict__ cn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F) return;
+  const int d = walk_decide(w, fr[i].x, fr[i].y);
+  cc[i] = d == kSelf ? 3 : (d >= kSplitA ? 2 : 0);
+  cf[i] = d == kFar ? 2 : 0;
+  cn[i] = d == kNear ? 2 : 0;
+}
+
+__global__ void k_walk_emit(const int2* __restrict__ fr, int F, WalkCtx w, const int* __restrict__ oc,
+                            const int* __restrict__ of, const int* __restrict__ on, int2* __restrict__ next,
+                            uint64_t* __restrict__ far_keys, int far_shift, uint64_t* __restrict__ near_keys,
+                            int near_shift) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F) return;
+  const int a = fr[i].x, b = fr[i].y;
+  const int d = walk_decide(w, a, b);
+  if (d == kSelf) {
+    const int l = w.left[a], r = w.right[a];
+    int2* o = next + oc[i];
+    o[0] = make_int2(l, l);
+    o[1] = make_int2(r, r);
+    o[2] = make_int2(l, r);
+  } else if (d == kSplitA) {
+    next[oc[i]] = make_int2(w.left[a], b);
+    next[oc[i] + 1] = make_int2(w.right[a], b);
+  } else if (d == kSplitB) {
+    next[oc[i]] = make_int2(a, w.left[b]);
+    next[oc[i] + 1] = make_int2(a, w.right[b]);
+  } else if (d == kFar) {
+    far_keys[of[i]] = ((uint64_t)a << far_shift) | (uint64_t)b;
+    far_keys[of[i] + 1] = ((uint64_t)b << far_shift) | (uint64_t)a;
+  } else if (d == kNear) {
+    const uint64_t la = (uint64_t)(a - w.num_internal), lb = (uint64_t)(b - w.num_internal);
+    near_keys[on[i]] = (la << near_shift) | lb;
+    near_keys[on[i] + 1] = (lb << near_shift) | la;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 5. CSR from sorted (row << shift | col) keys.
+// ---------------------------------------------------------------------------
+__global__ void k_csr_cols(const uint64_t* __restrict__ keys, int64_t n, int shift, int* __restrict__ cols,
+                           int64_t* __restrict__ row_cnt) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t k = keys[i];
+  cols[i] = (int)(k & ((1ULL << shift) - 1));
+  atomicAdd(reinterpret_cast<unsigned long long*>(row_cnt + (k >> shift)), 1ull);
+}
+
+inline int bits_for(int64_t v) {  // bits to hold values in [0, v)
+  int b = 1;
+  while (b < 62 && ((int64_t)1 << b) < v) ++b;
+  return b;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The handle: every output array in device memory.
+// ---------------------------------------------------------------------------
+struct jb_dtree {
+  jb_tree_info_t info{};
+  DBuf perm, ranges, left, right, parent, level, level_off, leaf_of, far_off, far_src, near_off, near_src, com, radius;
+};
+
+namespace {
+
+void build(jb_dtree& t, int64_t n, const double* pos, const double* mass, int leaf_size, double theta, cudaStream_t st) {
+  Scratch s;
+  ck(s.total.alloc(64));
+  int64_t* d_total64 = s.total.as<int64_t>();
+  int* d_total32 = reinterpret_cast<int*>(d_total64 + 4);
+
+  // 1. Morton codes, sorted with their input index.
+  DBuf part, bb, k0, k1, v0, v1;
+  const int nb_bb = 296;
+  ck(part.alloc(6 * nb_bb * sizeof(double)));
+  ck(bb.alloc(6 * sizeof(double)));
+  k_bbox_partial<<<nb_bb, 256, 0, st>>>(pos, n, part.as<double>());
+  ck_launch();
+  k_bbox_final<<<1, 32, 0, st>>>(part.as<double>(), nb_bb, bb.as<double>());
+  ck_launch();
+  ck(k0.alloc((size_t)n * 8));
+  ck(k1.alloc((size_t)n * 8));
+  ck(v0.alloc((size_t)n * 4));
+  ck(v1.alloc((size_t)n * 4));
+  k_morton<<<nblocks(n, 256), 256, 0, st>>>(pos, n, bb.as<double>(), k0.as<uint64_t>(), v0.as<int>());
+  ck_launch();
+  radix_sort(k0.as<uint64_t>(), v0.as<int>(), k1.as<uint64_t>(), v1.as<int>(), n, 63, s, st);
+  const uint64_t* codes = k0.as<uint64_t>();
+  const int* sperm = v0.as<int>();  // sorted slot -> input index
+
+  // 2. Breadth-first split, one level at a time.
+  DBuf fr0, fr1, flag, rank, int_ranges, int_parent, int_level, leaves, left, right;
+  ck(fr0.alloc((size_t)n * sizeof(Pending)));
+  ck(fr1.alloc((size_t)n * sizeof(Pending)));
+  ck(flag.alloc((size_t)(n + 1) * 4));
+  ck(rank.alloc((size_t)(n + 1) * 4));
+  ck(int_ranges.alloc((size_t)n * 8));
+  ck(int_parent.alloc((size_t)n * 4));
+  ck(int_level.alloc((size_t)n * 4));
+  ck(left.alloc((size_t)n * 4));
+  ck(right.alloc((size_t)n * 4));
+  ck(leaves.alloc((size_t)n * sizeof(LeafRec)));
+  {
+    const Pending root{0, (int)n - 1, -1, 0};
+    ck(cudaMemcpyAsync(fr0.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+  }
+  Pending* cur = fr0.as<Pending>();
+  Pending* nxt = fr1.as<Pending>();
+  int F = 1, int_base = 0, leaf_base = 0, level = 0;
+  std::vector<int> level_off;
+  while (F > 0) {
+    level_off.push_back(int_base);
+    k_level_flags<<<nblocks(F, 256), 256, 0, st>>>(cur, F, leaf_size, flag.as<int>());
+    ck_launch();
+    exclusive_scan<int>(flag.as<int>(), rank.as<int>(), F, d_total32, s, st);
+    const int n_int = read_word(d_total32, st);
+    k_level_emit<<<nblocks(F, 256), 256, 0, st>>>(cur, F, flag.as<int>(), rank.as<int>(), int_base, leaf_base, level,
+                                                  codes, int_ranges.as<int>(), int_parent.as<int>(), int_level.as<int>(),
+                                                  left.as<int>(), right.as<int>(), nxt, leaves.as<LeafRec>());
+    ck_launch();
+    int_base += n_int;
+    leaf_base += F - n_int;
+    F = 2 * n_int;
+    std::swap(cur, nxt);
+    ++level;
+  }
+  const int NI = int_base, L = leaf_base, NN = NI + L;
+  while (level_off.size() > 1 && level_off.back() == NI) level_off.pop_back();
+  level_off.push_back(NI);
+  int num_levels = NI > 0 ? (int)level_off.size() - 1 : 0;
+  if (NI == 0) level_off.assign(1, 0);
+
+  // Leaves in particle order; node arrays.
+  ck(cudaMemsetAsync(flag.p, 0, (size_t)n * 4, st));
+  k_mark_leaf_starts<<<nblocks(L, 256), 256, 0, st>>>(leaves.as<LeafRec>(), L, flag.as<int>());
+  ck_launch();
+  exclusive_scan<int>(flag.as<int>(), rank.as<int>(), n, nullptr, s, st);
+  ck(t.leaf_of.alloc((size_t)n * 4));
+  k_leaf_of<<<nblocks(n, 256), 256, 0, st>>>(flag.as<int>(), rank.as<int>(), n, t.leaf_of.as<int>());
+  ck_launch();
+  ck(t.ranges.alloc((size_t)NN * 8));
+  ck(t.parent.alloc((size_t)NN * 4));
+  ck(t.level.alloc((size_t)NN * 4));
+  ck(t.left.alloc((size_t)std::max(NI, 1) * 4));
+  ck(t.right.alloc((size_t)std::max(NI, 1) * 4));
+  if (NI > 0) {
+    ck(cudaMemcpyAsync(t.ranges.p, int_ranges.p, (size_t)NI * 8, cudaMemcpyDeviceToDevice, st));
+    ck(cudaMemcpyAsync(t.parent.p, int_parent.p, (size_t)NI * 4, cudaMemcpyDeviceToDevice, st));
+    ck(cudaMemcpyAsync(t.level.p, int_level.p, (size_t)NI * 4, cudaMemcpyDeviceToDevice, st));
+    ck(cudaMemcpyAsync(t.left.p, left.p, (size_t)NI * 4, cudaMemcpyDeviceToDevice, st));
+    ck(cudaMemcpyAsync(t.right.p, right.p, (size_t)NI * 4, cudaMemcpyDeviceToDevice, st));
+  }
+  k_place_leaves<<<nblocks(L, 256), 256, 0, st>>>(leaves.as<LeafRec>(), L, rank.as<int>(), NI, t.ranges.as<int>(),
+                                                  t.parent.as<int>(), t.level.as<int>(), t.left.as<int>(),
+                                                  t.right.as<int>());
+  ck_launch();
+  ck(t.level_off.alloc(level_off.size() * 4));
+  ck(cudaMemcpyAsync(t.level_off.p, level_off.data(), level_off.size() * 4, cudaMemcpyHostToDevice, st));
+  ck(t.perm.alloc((size_t)n * 8));
+  k_widen_perm<<<nblocks(n, 256), 256, 0, st>>>(sperm, n, t.perm.as<int64_t>());
+  ck_launch();
+  ck(cudaMemsetAsync(d_total32, 0, 4, st));
+  k_max_occupancy<<<nblocks(L, 256), 256, 0, st>>>(t.ranges.as<int>(), NI, L, d_total32);
+  ck_launch();
+  const int max_occ = read_word(d_total32, st);
+
+  // 3. COM and radii.
+  DBuf nmass;
+  ck(t.com.alloc((size_t)NN * 3 * 8));
+  ck(t.radius.alloc((size_t)NN * 8));
+  ck(nmass.alloc((size_t)NN * 8));
+  k_leaf_com<<<nblocks(L, 128), 128, 0, st>>>(L, NI, t.ranges.as<int>(), sperm, pos, mass, t.com.as<double>(),
+                                              t.radius.as<double>(), nmass.as<double>());
+  ck_launch();
+  for (int lv = num_levels - 1; lv >= 0; --lv) {
+    const int a = level_off[lv], b = level_off[lv + 1];
+    if (b <= a) continue;
+    k_internal_com<<<nblocks(b - a, 128), 128, 0, st>>>(a, b, t.left.as<int>(), t.right.as<int>(), t.ranges.as<int>(),
+                                                        t.com.as<double>(), t.radius.as<double>(), nmass.as<double>());
+    ck_launch();
+  }
+  // free the split buffers before the walk
+  fr0.release();
+  fr1.release();
+  int_ranges.release();
+  int_parent.release();
+  int_level.release();
+  leaves.release();
+  left.release();
+  right.release();
+  k1.release();
+  v1.release();
+
+  // 4. Dual walk (only when the root is split, as the host).
+  const int far_shift = bits_for(NN), near_shift = bits_for(std::max(L, 1));
+  DBuf w0, w1, cc, cf, cn, oc, of, on, far_keys, near_keys;
+  int64_t n_far = 0, n_near = 0;
+  if (NN > 1) {
+    const WalkCtx w{t.left.as<int>(), t.right.as<int>(), t.com.as<double>(), t.radius.as<double>(), NI, theta * theta};
+    int64_t cap = std::max<int64_t>(1 << 16, 4 * (int64_t)NN);
+    ck(w0.alloc(cap * sizeof(int2)));
+    ck(w1.alloc(cap * sizeof(int2)));
+    for (DBuf* b : {&cc, &cf, &cn, &oc, &of, &on}) ck(b->alloc(cap * 4));
+    ck(far_keys.alloc((size_t)std::max<int64_t>(1 << 16, 64 * (int64_t)NN) * 8));
+    ck(near_keys.alloc((size_t)std::max<int64_t>(1 << 16, 64 * (int64_t)L) * 8));
+    const int2 root = make_int2(0, 0);
+    ck(cudaMemcpyAsync(w0.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    int2* wc = w0.as<int2>();
+    int64_t Fw = 1;
+    while (Fw > 0) {
+      k_walk_count<<<nblocks(Fw, 256), 256, 0, st>>>(wc, (int)Fw, w, cc.as<int>(), cf.as<int>(), cn.as<int>());
+      ck_launch();
+      exclusive_scan<int>(cc.as<int>(), oc.as<int>(), Fw, d_total32, s, st);
+      exclusive_scan<int>(cf.as<int>(), of.as<int>(), Fw, d_total32 + 1, s, st);
+      exclusive_scan<int>(cn.as<int>(), on.as<int>(), Fw, d_total32 + 2, s, st);
+      int tot[3];
+      ck(cudaMemcpyAsync(tot, d_total32, sizeof(tot), cudaMemcpyDeviceToHost, st));
+      ck(cudaStreamSynchronize(st));
+      const int64_t Fn = tot[0];
+      // grow the next frontier, the count arrays and the key buffers as needed
+      int2* wn = (wc == w0.as<int2>()) ? w1.as<int2>() : w0.as<int2>();
+      DBuf& wn_buf = (wc == w0.as<int2>()) ? w1 : w0;
+      if ((size_t)Fn * sizeof(int2) > wn_buf.bytes) {
+        ck(wn_buf.grow((size_t)Fn * 2 * sizeof(int2), 0, st));
+        wn = wn_buf.as<int2>();
+      }
+      const size_t need_far = (size_t)(n_far + tot[1]) * 8, need_near = (size_t)(n_near + tot[2]) * 8;
+      if (need_far > far_keys.bytes) ck(far_keys.grow(std::max(need_far, 2 * far_keys.bytes), (size_t)n_far * 8, st));
+      if (need_near > near_keys.bytes)
+        ck(near_keys.grow(std::max(need_near, 2 * near_keys.bytes), (size_t)n_near * 8, st));
+      k_walk_emit<<<nblocks(Fw, 256), 256, 0, st>>>(wc, (int)Fw, w, oc.as<int>(), of.as<int>(), on.as<int>(), wn,
+                                                    far_keys.as<uint64_t>() + n_far, far_shift,
+                                                    near_keys.as<uint64_t>() + n_near, near_shift);
+      ck_launch();
+      n_far += tot[1];
+      n_near += tot[2];
+      Fw = Fn;
+      wc = wn;
+      if ((size_t)Fw * 4 > cc.bytes)
+        for (DBuf* b : {&cc, &cf, &cn, &oc, &of, &on}) ck(b->alloc((size_t)Fw * 2 * 4));
+    }
+  }
+  w0.release();
+  w1.release();
+  for (DBuf* b : {&cc, &cf, &cn, &oc, &of, &on}) b->release();
+
+  // 5. CSR lists.
+  auto to_csr = [&](DBuf& keys, int64_t m, int shift, int rows, DBuf& off, DBuf& col) {
+    ck(off.alloc((size_t)(rows + 1) * 8));
+    ck(col.alloc((size_t)std::max<int64_t>(m, 1) * 4));
+    DBuf tmp, cnt;
+    ck(tmp.alloc((size_t)std::max<int64_t>(m, 1) * 8));
+    radix_sort(keys.as<uint64_t>(), nullptr, tmp.as<uint64_t>(), nullptr, m, 2 * shift, s, st);
+    ck(cnt.alloc((size_t)(rows + 1) * 8));
+    ck(cudaMemsetAsync(cnt.p, 0, (size_t)(rows + 1) * 8, st));
+    if (m > 0) {
+      k_csr_cols<<<nblocks(m, 256), 256, 0, st>>>(keys.as<uint64_t>(), m, shift, col.as<int>(), cnt.as<int64_t>());
+      ck_launch();
+    }
+    exclusive_scan<int64_t>(cnt.as<int64_t>(), off.as<int64_t>(), rows, off.as<int64_t>() + rows, s, st);
+    ck(cudaStreamSynchronize(st));
+  };
+  if (NN > 1) {
+    to_csr(far_keys, n_far, far_shift, NN, t.far_off, t.far_src);
+    far_keys.release();
+    to_csr(near_keys, n_near, near_shift, L, t.near_off, t.near_src);
+    near_keys.release();
+  } else {
+    ck(t.far_off.alloc((size_t)(NN + 1) * 8));
+    ck(cudaMemsetAsync(t.far_off.p, 0, (size_t)(NN + 1) * 8, st));
+    ck(t.near_off.alloc((size_t)(L + 1) * 8));
+    ck(cudaMemsetAsync(t.near_off.p, 0, (size_t)(L + 1) * 8, st));
+    ck(t.far_src.alloc(4));
+    ck(t.near_src.alloc(4));
+  }
+  ck(cudaStreamSynchronize(st));
+
+  t.info.num_particles = n;
+  t.info.num_nodes = NN;
+  t.info.num_internal = NI;
+  t.info.num_leaves = L;
+  t.info.num_levels = num_levels;
+  t.info.num_far_pairs = n_far;
+  t.info.num_near_pairs = n_near;
+  t.info.max_leaf_occupancy = max_occ;
+}
+
+const DBuf* field_buf(const jb_dtree* t, int field) {
+  switch (field) {
+    case JB_TREE_PERMUTATION: return &t->perm;
+    case JB_TREE_NODE_RANGES: return &t->ranges;
+    case JB_TREE_LEFT_CHILD: return &t->left;
+    case JB_TREE_RIGHT_CHILD: return &t->right;
+    case JB_TREE_PARENT: return &t->parent;
+    case JB_TREE_NODE_LEVEL: return &t->level;
+    case JB_TREE_LEVEL_OFFSETS: return &t->level_off;
+    case JB_TREE_LEAF_OF_PARTICLE: return &t->leaf_of;
+    case JB_TREE_FAR_OFFSETS: return &t->far_off;
+    case JB_TREE_FAR_SOURCES: return &t->far_src;
+    case JB_TREE_NEAR_OFFSETS: return &t->near_off;
+    case JB_TREE_NEAR_SOURCES: return &t->near_src;
+    case JB_TREE_CENTERS_F64: return &t->com;
+    case JB_TREE_RADII_F64: return &t->radius;
+    default: return nullptr;
+  }
+}
+
+size_t field_bytes(const jb_dtree* t, int field) {
+  const jb_tree_info_t& i = t->info;
+  switch (field) {
+    case JB_TREE_PERMUTATION: return (size_t)i.num_particles * 8;
+    case JB_TREE_NODE_RANGES: return (size_t)i.num_nodes * 8;
+    case JB_TREE_LEFT_CHILD:
+    case JB_TREE_RIGHT_CHILD: return (size_t)i.num_internal * 4;
+    case JB_TREE_PARENT:
+    case JB_TREE_NODE_LEVEL: return (size_t)i.num_nodes * 4;
+    case JB_TREE_LEVEL_OFFSETS: return (size_t)(i.num_levels + 1) * 4;
+    case JB_TREE_LEAF_OF_PARTICLE: return (size_t)i.num_particles * 4;
+    case JB_TREE_FAR_OFFSETS: return (size_t)(i.num_nodes + 1) * 8;
+    case JB_TREE_FAR_SOURCES: return (size_t)i.num_far_pairs * 4;
+    case JB_TREE_NEAR_OFFSETS: return (size_t)(i.num_leaves + 1) * 8;
+    case JB_TREE_NEAR_SOURCES: return (size_t)i.num_near_pairs * 4;
+    case JB_TREE_CENTERS_F64: return (size_t)i.num_nodes * 24;
+    case JB_TREE_RADII_F64: return (size_t)i.num_nodes * 8;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+JB_API int jb_tree_build_device(int64_t n, const double* pos, const double* mass, int leaf_size, double theta,
+                                void* stream, jb_dtree** out) {
+  if (!out) return JB_ERR_ARG;
+  *out = nullptr;
+  if (n <= 0 || n > (int64_t)0x7fffffff || !pos || !mass || leaf_size < 1 || !(theta > 0) || !(theta < 1.0))
+    return JB_ERR_ARG;
+  jb_dtree* t = new (std::nothrow) jb_dtree();
+  if (!t) return JB_ERR_ALLOC;
+  try {
+    build(*t, n, pos, mass, leaf_size, theta, reinterpret_cast<cudaStream_t>(stream));
+  } catch (const Fail& f) {
+    delete t;
+    return f.rc;
+  } catch (const std::bad_alloc&) {
+    delete t;
+    return JB_ERR_ALLOC;
+  }
+  *out = t;
+  return JB_OK;
+}
+
+JB_API int jb_dtree_info(const jb_dtree* t, jb_tree_info_t* info) {
+  if (!t || !info) return JB_ERR_ARG;
+  *info = t->info;
+  return JB_OK;
+}
+
+JB_API const void* jb_dtree_field(const jb_dtree* t, int field) {
+  if (!t) return nullptr;
+  const DBuf* b = field_buf(t, field);
+  return b ? b->p : nullptr;
+}
+
+JB_API int jb_dtree_copy(const jb_dtree* t, int field, void* dst) {
+  if (!t || !dst) return JB_ERR_ARG;
+  const DBuf* b = field_buf(t, field);
+  if (!b) return JB_ERR_ARG;
+  const size_t bytes = field_bytes(t, field);
+  if (bytes == 0) return JB_OK;
+  return jb::cuda_status(cudaMemcpy(dst, b->p, bytes, cudaMemcpyDeviceToHost));
+}
+
+JB_API void jb_dtree_free(jb_dtree* t) { delete t; }
+
+}  // extern "C"

@@ -128,7 +128,11 @@ class FastMultipoleMethod:
         mass_np = masses.detach().cpu().numpy() if isinstance(masses, torch.Tensor) else np.asarray(masses)
         if pos_np.ndim != 2 or pos_np.shape[1] != 3 or mass_np.shape != (pos_np.shape[0],):
             raise ValueError("positions must be (N, 3) and masses (N,)")
-        topo = build_topology(pos_np, mass_np, leaf_size=int(leaf_size), theta=th)
+        # tree + lists on the GPU when the solver runs there (the same arrays
+        # as the host build, bit for bit), else on the host
+        topo = build_topology(positions if isinstance(positions, torch.Tensor) else pos_np,
+                              masses if isinstance(masses, torch.Tensor) else mass_np, leaf_size=int(leaf_size),
+                              theta=th, device=self.device if self.device.type == "cuda" else None)
         dt = DeviceTopology(topo, self.device)
         dt.validate()
         ps = Pass(dt, int(max_order), G=self.G, eps2=self.softening ** 2, m2l_mode=self.m2l_mode,

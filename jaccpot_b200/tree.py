@@ -90,42 +90,36 @@ class Topology:
         return int((per_edge_t * src_cnt).sum() + (leaf_cnt * (leaf_cnt - 1)).sum())
 
 
-def build_topology(positions, masses, *, leaf_size: int = 16, theta: float = 0.6) -> Topology:
-    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
-    mass = np.ascontiguousarray(np.asarray(masses, dtype=np.float64).reshape(-1))
-    n = pos.shape[0]
-    if mass.shape[0] != n:
-        raise ValueError("positions and masses disagree in length")
-    lb = _lib.lib()
-    h = ctypes.c_void_p()
-    _lib.check(lb.jb_tree_build(n, pos.ctypes.data, mass.ctypes.data, int(leaf_size), float(theta),
-                                ctypes.byref(h)), "jb_tree_build")
-    try:
-        info = _lib.TreeInfo()
-        _lib.check(lb.jb_tree_info(h, ctypes.byref(info)), "jb_tree_info")
-        sizes = {
-            "permutation": n,
-            "node_ranges": 2 * info.num_nodes,
-            "left_child": info.num_internal,
-            "right_child": info.num_internal,
-            "parent": info.num_nodes,
-            "node_level": info.num_nodes,
-            "level_offsets": info.num_levels + 1,
-            "leaf_of_particle": n,
-            "far_offsets": info.num_nodes + 1,
-            "far_sources": info.num_far_pairs,
-            "near_offsets": info.num_leaves + 1,
-            "near_leaves": info.num_near_pairs,
-            "centers_f64": 3 * info.num_nodes,
-            "radii_f64": info.num_nodes,
-        }
-        arrs = {}
-        for name, (fid, dt) in _lib.TREE_FIELDS.items():
-            a = np.empty(max(sizes[name], 1), dtype=dt)
-            _lib.check(lb.jb_tree_copy(h, fid, a.ctypes.data), f"jb_tree_copy({name})")
-            arrs[name] = a[: sizes[name]]
-    finally:
-        lb.jb_tree_free(h)
+def _field_sizes(n: int, info) -> dict:
+    return {
+        "permutation": n,
+        "node_ranges": 2 * info.num_nodes,
+        "left_child": info.num_internal,
+        "right_child": info.num_internal,
+        "parent": info.num_nodes,
+        "node_level": info.num_nodes,
+        "level_offsets": info.num_levels + 1,
+        "leaf_of_particle": n,
+        "far_offsets": info.num_nodes + 1,
+        "far_sources": info.num_far_pairs,
+        "near_offsets": info.num_leaves + 1,
+        "near_leaves": info.num_near_pairs,
+        "centers_f64": 3 * info.num_nodes,
+        "radii_f64": info.num_nodes,
+    }
+
+
+def _copy_fields(copy_fn, handle, n: int, info) -> dict:
+    sizes = _field_sizes(n, info)
+    arrs = {}
+    for name, (fid, dt) in _lib.TREE_FIELDS.items():
+        a = np.empty(max(sizes[name], 1), dtype=dt)
+        _lib.check(copy_fn(handle, fid, a.ctypes.data), f"tree field copy ({name})")
+        arrs[name] = a[: sizes[name]]
+    return arrs
+
+
+def _topology(n: int, info, arrs: dict, leaf_size: int, theta: float) -> Topology:
     perm = arrs["permutation"]
     inv = np.empty_like(perm)
     inv[perm] = np.arange(n, dtype=np.int64)
@@ -158,3 +152,53 @@ def build_topology(positions, masses, *, leaf_size: int = 16, theta: float = 0.6
         radii_f64=arrs["radii_f64"],
         m2l_targets=tg[order].astype(np.int32),
     )
+
+
+def build_topology(positions, masses, *, leaf_size: int = 16, theta: float = 0.6, device=None) -> Topology:
+    """Tree + lists on the host (``jb_tree_build``), or on the GPU
+    (``jb_tree_build_device``, the same arrays bit for bit) when ``device`` is
+    a CUDA device."""
+    if device is not None and str(device).startswith("cuda"):
+        return build_topology_device(positions, masses, leaf_size=leaf_size, theta=theta, device=device)
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+    mass = np.ascontiguousarray(np.asarray(masses, dtype=np.float64).reshape(-1))
+    n = pos.shape[0]
+    if mass.shape[0] != n:
+        raise ValueError("positions and masses disagree in length")
+    lb = _lib.lib()
+    h = ctypes.c_void_p()
+    _lib.check(lb.jb_tree_build(n, pos.ctypes.data, mass.ctypes.data, int(leaf_size), float(theta),
+                                ctypes.byref(h)), "jb_tree_build")
+    try:
+        info = _lib.TreeInfo()
+        _lib.check(lb.jb_tree_info(h, ctypes.byref(info)), "jb_tree_info")
+        arrs = _copy_fields(lb.jb_tree_copy, h, n, info)
+    finally:
+        lb.jb_tree_free(h)
+    return _topology(n, info, arrs, leaf_size, theta)
+
+
+def build_topology_device(positions, masses, *, leaf_size: int = 16, theta: float = 0.6, device="cuda") -> Topology:
+    """The tree and lists built on the GPU by ``jb_tree_build_device``
+    (csrc/tree_gpu.cu) from float64 copies of the inputs on ``device``; the
+    arrays are copied back into the same :class:`Topology` the host build
+    returns."""
+    import torch
+
+    pos = torch.as_tensor(positions).to(device=device, dtype=torch.float64).reshape(-1, 3).contiguous()
+    mass = torch.as_tensor(masses).to(device=device, dtype=torch.float64).reshape(-1).contiguous()
+    n = pos.shape[0]
+    if mass.shape[0] != n:
+        raise ValueError("positions and masses disagree in length")
+    lb = _lib.lib()
+    h = ctypes.c_void_p()
+    stream = torch.cuda.current_stream(pos.device).cuda_stream
+    _lib.check(lb.jb_tree_build_device(n, pos.data_ptr(), mass.data_ptr(), int(leaf_size), float(theta), stream,
+                                       ctypes.byref(h)), "jb_tree_build_device")
+    try:
+        info = _lib.TreeInfo()
+        _lib.check(lb.jb_dtree_info(h, ctypes.byref(info)), "jb_dtree_info")
+        arrs = _copy_fields(lb.jb_dtree_copy, h, n, info)
+    finally:
+        lb.jb_dtree_free(h)
+    return _topology(n, info, arrs, leaf_size, theta)
