@@ -105,8 +105,11 @@ JB_API void jb_tree_free(jb_tree* t);
  * dual walk, CSR by key sort.  Replaces the same yggdrax calls
  * (runtime/fmm_prepare.py:823, :1411).  pos (n,3) and mass (n,) are DEVICE
  * float64 arrays; the handle owns device copies of every JB_TREE_* field.
- * Allocates device memory; synchronises the stream (the walk sizes its
- * buffers from counts read back level by level).                           */
+ * Device memory comes stream-ordered from a library pool per device that
+ * keeps up to 4 GiB cached between builds; the handle's arrays are freed on
+ * the build's stream by jb_dtree_free (free it before destroying the
+ * stream).  Synchronises the stream (the split and the walk size their next
+ * step from counts read back level by level).                              */
 typedef struct jb_dtree jb_dtree;
 JB_API int jb_tree_build_device(int64_t n, const double* pos, const double* mass, int leaf_size,
                                 double theta, void* stream, jb_dtree** out);

@@ -32,6 +32,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -46,45 +47,81 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---------------------------------------------------------------------------
-// Device buffers owned by the builder / the handle.
+// Device buffers owned by the builder / the handle, stream-ordered from a
+// library memory pool per device that keeps up to 4 GiB cached between
+// builds (a rebuild on a moved particle set allocates nothing new).
 // ---------------------------------------------------------------------------
+cudaError_t tree_pool(cudaMemPool_t* out) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps pr = {};
+    pr.allocType = cudaMemAllocationTypePinned;
+    pr.handleTypes = cudaMemHandleTypeNone;
+    pr.location.type = cudaMemLocationTypeDevice;
+    pr.location.id = dev;
+    e = cudaMemPoolCreate(&pools[dev], &pr);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = 4ull << 30;
+    e = cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+  }
+  *out = pools[dev];
+  return cudaSuccess;
+}
+
+thread_local cudaStream_t tl_stream = nullptr;  // the stream of the build in progress on this thread
+
 struct DBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  cudaStream_t st = nullptr;
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     bytes = 0;
   }
   cudaError_t alloc(size_t b) {
     release();
     if (b == 0) b = 16;
-    const cudaError_t e = cudaMalloc(&p, b);
+    cudaMemPool_t pool;
+    cudaError_t e = tree_pool(&pool);
+    if (e != cudaSuccess) return e;
+    st = tl_stream;
+    e = cudaMallocFromPoolAsync(&p, b, pool, st);
     if (e == cudaSuccess) bytes = b;
     else p = nullptr;
     return e;
   }
-  // Grows to at least b bytes, keeping the first `keep` bytes.
-  cudaError_t grow(size_t b, size_t keep, cudaStream_t st) {
+  // Grows to at least b bytes, keeping the first `keep` bytes (stream-ordered).
+  cudaError_t grow(size_t b, size_t keep, cudaStream_t) {
     if (b <= bytes) return cudaSuccess;
+    cudaMemPool_t pool;
+    cudaError_t e = tree_pool(&pool);
+    if (e != cudaSuccess) return e;
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, b);
+    e = cudaMallocFromPoolAsync(&q, b, pool, tl_stream);
     if (e != cudaSuccess) return e;
     if (keep && p) {
-      e = cudaMemcpyAsync(q, p, keep, cudaMemcpyDeviceToDevice, st);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      e = cudaMemcpyAsync(q, p, keep, cudaMemcpyDeviceToDevice, tl_stream);
       if (e != cudaSuccess) {
-        cudaFree(q);
+        cudaFreeAsync(q, tl_stream);
         return e;
       }
     }
     release();
     p = q;
     bytes = b;
+    st = tl_stream;
     return cudaSuccess;
   }
   template <typename T>
@@ -110,24 +147,50 @@ inline unsigned nblocks(int64_t n, int per) { return (unsigned)std::max<int64_t>
 // ---------------------------------------------------------------------------
 constexpr int kScanThreads = 1024, kScanItems = 4, kScanTile = kScanThreads * kScanItems;
 
+// Three counters scanned together (the dual walk's children / far / near).
+struct I3 {
+  int a, b, c;
+};
+__device__ __forceinline__ I3 operator+(I3 x, I3 y) { return I3{x.a + y.a, x.b + y.b, x.c + y.c}; }
+__device__ __forceinline__ I3 operator-(I3 x, I3 y) { return I3{x.a - y.a, x.b - y.b, x.c - y.c}; }
+template <typename T>
+__device__ __forceinline__ T zero() {
+  return T(0);
+}
+template <>
+__device__ __forceinline__ I3 zero<I3>() {
+  return I3{0, 0, 0};
+}
+template <typename T>
+__device__ __forceinline__ T shfl_up(T v, int o) {
+  return __shfl_up_sync(kFull, v, o);
+}
+template <>
+__device__ __forceinline__ I3 shfl_up<I3>(I3 v, int o) {
+  return I3{__shfl_up_sync(kFull, v.a, o), __shfl_up_sync(kFull, v.b, o), __shfl_up_sync(kFull, v.c, o)};
+}
+
+// Exclusive scan of one tile per block; the tile's sum goes to tile_sums
+// (and to *total when the whole input is one tile).
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict__ in, T* __restrict__ out,
-                                                             T* __restrict__ tile_sums, int64_t n) {
+                                                             T* __restrict__ tile_sums, T* __restrict__ total,
+                                                             int64_t n) {
   __shared__ T warp_sums[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   T v[kScanItems];
-  T s = 0;
+  T s = zero<T>();
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    v[i] = (base + i < n) ? in[base + i] : T(0);
-    s += v[i];
+    v[i] = (base + i < n) ? in[base + i] : zero<T>();
+    s = s + v[i];
   }
   T incl = s;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const T y = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += y;
+    const T y = shfl_up<T>(incl, o);
+    if (lane >= o) incl = incl + y;
   }
   if (lane == 31) warp_sums[warp] = incl;
   __syncthreads();
@@ -136,8 +199,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict
     T wi = w;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const T y = __shfl_up_sync(kFull, wi, o);
-      if (lane >= o) wi += y;
+      const T y = shfl_up<T>(wi, o);
+      if (lane >= o) wi = wi + y;
     }
     warp_sums[lane] = wi - w;
   }
@@ -146,20 +209,18 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const T* __restrict
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     if (base + i < n) out[base + i] = run;
-    run += v[i];
+    run = run + v[i];
   }
-  if (threadIdx.x == kScanThreads - 1) tile_sums[blockIdx.x] = run;
+  if (threadIdx.x == kScanThreads - 1) {
+    tile_sums[blockIdx.x] = run;
+    if (total && gridDim.x == 1) *total = run;
+  }
 }
 
 template <typename T>
 __global__ void k_scan_add(T* __restrict__ out, const T* __restrict__ tile_off, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && i >= kScanTile) out[i] += tile_off[i / kScanTile];
-}
-
-template <typename T>
-__global__ void k_scan_total(const T* __restrict__ in, const T* __restrict__ out, int64_t n, T* __restrict__ total) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) *total = n > 0 ? out[n - 1] + in[n - 1] : T(0);
+  if (i < n && i >= kScanTile) out[i] = out[i] + tile_off[i / kScanTile];
 }
 
 // ---------------------------------------------------------------------------
@@ -262,15 +323,11 @@ void scan_rec(const T* in, T* out, int64_t n, T* total, T* scratch, cudaStream_t
   const int64_t tiles = (n + kScanTile - 1) / kScanTile;
   T* sums = scratch;
   T* sums_x = sums + tiles;
-  k_scan_tiles<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, sums, n);
+  k_scan_tiles<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, sums, total, n);
   ck_launch();
-  if (tiles > 1) {
-    scan_rec<T>(sums, sums_x, tiles, nullptr, sums + 2 * tiles + 8, st);
+  if (tiles > 1) {  // the tile sums' total is the total
+    scan_rec<T>(sums, sums_x, tiles, total, sums + 2 * tiles + 8, st);
     k_scan_add<T><<<nblocks(n, 256), 256, 0, st>>>(out, sums_x, n);
-    ck_launch();
-  }
-  if (total) {
-    k_scan_total<T><<<1, 32, 0, st>>>(in, out, n, total);
     ck_launch();
   }
 }
@@ -575,56 +632,65 @@ __device__ __forceinline__ int walk_decide(const WalkCtx& w, int a, int b) {
   return (!la && (lb || ra >= rb)) ? kSplitA : kSplitB;
 }
 
-__global__ void k_walk_count(const int2* __restrict__ fr, int F, WalkCtx w, int* __restrict__ cc, int* __restrict__ cf,
-                             int* __restrict__ cn) {
+__global__ void k_walk_count(const int2* __restrict__ fr, int F, WalkCtx w, I3* __restrict__ cnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= F) return;
   const int d = walk_decide(w, fr[i].x, fr[i].y);
-  cc[i] = d == kSelf ? 3 : (d >= kSplitA ? 2 : 0);
-  cf[i] = d == kFar ? 2 : 0;
-  cn[i] = d == kNear ? 2 : 0;
+  cnt[i] = I3{d == kSelf ? 3 : (d >= kSplitA ? 2 : 0), d == kFar ? 2 : 0, d == kNear ? 2 : 0};
 }
 
-__global__ void k_walk_emit(const int2* __restrict__ fr, int F, WalkCtx w, const int* __restrict__ oc,
-                            const int* __restrict__ of, const int* __restrict__ on, int2* __restrict__ next,
-                            uint64_t* __restrict__ far_keys, int far_shift, uint64_t* __restrict__ near_keys,
-                            int near_shift) {
+__global__ void k_walk_emit(const int2* __restrict__ fr, int F, WalkCtx w, const I3* __restrict__ off,
+                            int2* __restrict__ next, uint64_t* __restrict__ far_keys, int far_shift,
+                            uint64_t* __restrict__ near_keys, int near_shift) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= F) return;
+  const I3 o3 = off[i];
   const int a = fr[i].x, b = fr[i].y;
   const int d = walk_decide(w, a, b);
   if (d == kSelf) {
     const int l = w.left[a], r = w.right[a];
-    int2* o = next + oc[i];
+    int2* o = next + o3.a;
     o[0] = make_int2(l, l);
     o[1] = make_int2(r, r);
     o[2] = make_int2(l, r);
   } else if (d == kSplitA) {
-    next[oc[i]] = make_int2(w.left[a], b);
-    next[oc[i] + 1] = make_int2(w.right[a], b);
+    next[o3.a] = make_int2(w.left[a], b);
+    next[o3.a + 1] = make_int2(w.right[a], b);
   } else if (d == kSplitB) {
-    next[oc[i]] = make_int2(a, w.left[b]);
-    next[oc[i] + 1] = make_int2(a, w.right[b]);
+    next[o3.a] = make_int2(a, w.left[b]);
+    next[o3.a + 1] = make_int2(a, w.right[b]);
   } else if (d == kFar) {
-    far_keys[of[i]] = ((uint64_t)a << far_shift) | (uint64_t)b;
-    far_keys[of[i] + 1] = ((uint64_t)b << far_shift) | (uint64_t)a;
+    far_keys[o3.b] = ((uint64_t)a << far_shift) | (uint64_t)b;
+    far_keys[o3.b + 1] = ((uint64_t)b << far_shift) | (uint64_t)a;
   } else if (d == kNear) {
     const uint64_t la = (uint64_t)(a - w.num_internal), lb = (uint64_t)(b - w.num_internal);
-    near_keys[on[i]] = (la << near_shift) | lb;
-    near_keys[on[i] + 1] = (lb << near_shift) | la;
+    near_keys[o3.c] = (la << near_shift) | lb;
+    near_keys[o3.c + 1] = (lb << near_shift) | la;
   }
 }
 
 // ---------------------------------------------------------------------------
 // 5. CSR from sorted (row << shift | col) keys.
 // ---------------------------------------------------------------------------
-__global__ void k_csr_cols(const uint64_t* __restrict__ keys, int64_t n, int shift, int* __restrict__ cols,
-                           int64_t* __restrict__ row_cnt) {
+// keys sorted; thread i writes column i and, where the row changes between
+// keys i-1 and i, the offsets of the rows in between; rows before the first
+// key start at 0, rows after the last at n.
+__global__ void k_csr(const uint64_t* __restrict__ keys, int64_t n, int shift, int rows, int* __restrict__ cols,
+                      int64_t* __restrict__ off) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t k = keys[i];
-  cols[i] = (int)(k & ((1ULL << shift) - 1));
-  atomicAdd(reinterpret_cast<unsigned long long*>(row_cnt + (k >> shift)), 1ull);
+  if (i <= rows) {
+    const int64_t r0 = (int64_t)(keys[0] >> shift), r1 = (int64_t)(keys[n - 1] >> shift);
+    if (i <= r0) off[i] = 0;
+    else if (i > r1) off[i] = n;
+  }
+  if (i < n) {
+    const uint64_t k = keys[i];
+    cols[i] = (int)(k & ((1ULL << shift) - 1));
+    if (i > 0) {
+      const int64_t r = (int64_t)(k >> shift), rp = (int64_t)(keys[i - 1] >> shift);
+      for (int64_t q = rp + 1; q <= r; ++q) off[q] = i;
+    }
+  }
 }
 
 inline int bits_for(int64_t v) {  // bits to hold values in [0, v)
@@ -646,6 +712,7 @@ struct jb_dtree {
 namespace {
 
 void build(jb_dtree& t, int64_t n, const double* pos, const double* mass, int leaf_size, double theta, cudaStream_t st) {
+  tl_stream = st;
   Scratch s;
   ck(s.total.alloc(64));
   int64_t* d_total64 = s.total.as<int64_t>();
@@ -775,72 +842,67 @@ void build(jb_dtree& t, int64_t n, const double* pos, const double* mass, int le
 
   // 4. Dual walk (only when the root is split, as the host).
   const int far_shift = bits_for(NN), near_shift = bits_for(std::max(L, 1));
-  DBuf w0, w1, cc, cf, cn, oc, of, on, far_keys, near_keys;
+  DBuf w0, w1, cnt3, off3, far_keys, near_keys;
   int64_t n_far = 0, n_near = 0;
   if (NN > 1) {
     const WalkCtx w{t.left.as<int>(), t.right.as<int>(), t.com.as<double>(), t.radius.as<double>(), NI, theta * theta};
-    int64_t cap = std::max<int64_t>(1 << 16, 4 * (int64_t)NN);
+    const int64_t cap = std::max<int64_t>(1 << 16, 4 * (int64_t)NN);
     ck(w0.alloc(cap * sizeof(int2)));
     ck(w1.alloc(cap * sizeof(int2)));
-    for (DBuf* b : {&cc, &cf, &cn, &oc, &of, &on}) ck(b->alloc(cap * 4));
-    ck(far_keys.alloc((size_t)std::max<int64_t>(1 << 16, 64 * (int64_t)NN) * 8));
-    ck(near_keys.alloc((size_t)std::max<int64_t>(1 << 16, 64 * (int64_t)L) * 8));
+    ck(cnt3.alloc(cap * sizeof(I3)));
+    ck(off3.alloc(cap * sizeof(I3)));
+    ck(far_keys.alloc((size_t)std::max<int64_t>(1 << 16, 256 * (int64_t)NN) * 8));
+    ck(near_keys.alloc((size_t)std::max<int64_t>(1 << 16, 256 * (int64_t)L) * 8));
+    I3* d_tot3 = reinterpret_cast<I3*>(d_total32);
     const int2 root = make_int2(0, 0);
     ck(cudaMemcpyAsync(w0.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
-    int2* wc = w0.as<int2>();
+    DBuf* wc = &w0;
+    DBuf* wn = &w1;
     int64_t Fw = 1;
     while (Fw > 0) {
-      k_walk_count<<<nblocks(Fw, 256), 256, 0, st>>>(wc, (int)Fw, w, cc.as<int>(), cf.as<int>(), cn.as<int>());
-      ck_launch();
-      exclusive_scan<int>(cc.as<int>(), oc.as<int>(), Fw, d_total32, s, st);
-      exclusive_scan<int>(cf.as<int>(), of.as<int>(), Fw, d_total32 + 1, s, st);
-      exclusive_scan<int>(cn.as<int>(), on.as<int>(), Fw, d_total32 + 2, s, st);
-      int tot[3];
-      ck(cudaMemcpyAsync(tot, d_total32, sizeof(tot), cudaMemcpyDeviceToHost, st));
-      ck(cudaStreamSynchronize(st));
-      const int64_t Fn = tot[0];
-      // grow the next frontier, the count arrays and the key buffers as needed
-      int2* wn = (wc == w0.as<int2>()) ? w1.as<int2>() : w0.as<int2>();
-      DBuf& wn_buf = (wc == w0.as<int2>()) ? w1 : w0;
-      if ((size_t)Fn * sizeof(int2) > wn_buf.bytes) {
-        ck(wn_buf.grow((size_t)Fn * 2 * sizeof(int2), 0, st));
-        wn = wn_buf.as<int2>();
+      if ((size_t)Fw * sizeof(I3) > cnt3.bytes) {
+        ck(cnt3.alloc((size_t)Fw * 2 * sizeof(I3)));
+        ck(off3.alloc((size_t)Fw * 2 * sizeof(I3)));
       }
-      const size_t need_far = (size_t)(n_far + tot[1]) * 8, need_near = (size_t)(n_near + tot[2]) * 8;
+      k_walk_count<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, cnt3.as<I3>());
+      ck_launch();
+      exclusive_scan<I3>(cnt3.as<I3>(), off3.as<I3>(), Fw, d_tot3, s, st);
+      const I3 tot = read_word(d_tot3, st);
+      // grow the next frontier and the key buffers as needed (stream-ordered)
+      ck(wn->grow((size_t)tot.a * 2 * sizeof(int2), 0, st));
+      const size_t need_far = (size_t)(n_far + tot.b) * 8, need_near = (size_t)(n_near + tot.c) * 8;
       if (need_far > far_keys.bytes) ck(far_keys.grow(std::max(need_far, 2 * far_keys.bytes), (size_t)n_far * 8, st));
       if (need_near > near_keys.bytes)
         ck(near_keys.grow(std::max(need_near, 2 * near_keys.bytes), (size_t)n_near * 8, st));
-      k_walk_emit<<<nblocks(Fw, 256), 256, 0, st>>>(wc, (int)Fw, w, oc.as<int>(), of.as<int>(), on.as<int>(), wn,
+      k_walk_emit<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, off3.as<I3>(), wn->as<int2>(),
                                                     far_keys.as<uint64_t>() + n_far, far_shift,
                                                     near_keys.as<uint64_t>() + n_near, near_shift);
       ck_launch();
-      n_far += tot[1];
-      n_near += tot[2];
-      Fw = Fn;
-      wc = wn;
-      if ((size_t)Fw * 4 > cc.bytes)
-        for (DBuf* b : {&cc, &cf, &cn, &oc, &of, &on}) ck(b->alloc((size_t)Fw * 2 * 4));
+      n_far += tot.b;
+      n_near += tot.c;
+      Fw = tot.a;
+      std::swap(wc, wn);
     }
   }
   w0.release();
   w1.release();
-  for (DBuf* b : {&cc, &cf, &cn, &oc, &of, &on}) b->release();
+  cnt3.release();
+  off3.release();
 
   // 5. CSR lists.
   auto to_csr = [&](DBuf& keys, int64_t m, int shift, int rows, DBuf& off, DBuf& col) {
     ck(off.alloc((size_t)(rows + 1) * 8));
     ck(col.alloc((size_t)std::max<int64_t>(m, 1) * 4));
-    DBuf tmp, cnt;
-    ck(tmp.alloc((size_t)std::max<int64_t>(m, 1) * 8));
-    radix_sort(keys.as<uint64_t>(), nullptr, tmp.as<uint64_t>(), nullptr, m, 2 * shift, s, st);
-    ck(cnt.alloc((size_t)(rows + 1) * 8));
-    ck(cudaMemsetAsync(cnt.p, 0, (size_t)(rows + 1) * 8, st));
-    if (m > 0) {
-      k_csr_cols<<<nblocks(m, 256), 256, 0, st>>>(keys.as<uint64_t>(), m, shift, col.as<int>(), cnt.as<int64_t>());
-      ck_launch();
+    if (m == 0) {
+      ck(cudaMemsetAsync(off.p, 0, (size_t)(rows + 1) * 8, st));
+      return;
     }
-    exclusive_scan<int64_t>(cnt.as<int64_t>(), off.as<int64_t>(), rows, off.as<int64_t>() + rows, s, st);
-    ck(cudaStreamSynchronize(st));
+    DBuf tmp;
+    ck(tmp.alloc((size_t)m * 8));
+    radix_sort(keys.as<uint64_t>(), nullptr, tmp.as<uint64_t>(), nullptr, m, 2 * shift, s, st);
+    k_csr<<<nblocks(std::max<int64_t>(m, rows + 1), 256), 256, 0, st>>>(keys.as<uint64_t>(), m, shift, rows,
+                                                                       col.as<int>(), off.as<int64_t>());
+    ck_launch();
   };
   if (NN > 1) {
     to_csr(far_keys, n_far, far_shift, NN, t.far_off, t.far_src);
