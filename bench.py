@@ -181,6 +181,47 @@ def _events_ms(fn, stream, reps=10, warm=3):
     return float(np.median(ts))
 
 
+def measure_prepare(pos, mass, cfg, dev, with_host: bool) -> dict:
+    """Prepare-time tree + interaction lists for the headline workload: the GPU
+    build (jb_tree_build_device; wall time around the call, which syncs: first
+    call and the median of three more) and, with_host, the host build of the
+    same arrays, checked identical field by field."""
+    import ctypes
+
+    import torch
+
+    from jaccpot_b200 import _lib, tree
+
+    lb = _lib.lib()
+    p = torch.from_numpy(np.asarray(pos)).to(dev).double()
+    m = torch.from_numpy(np.asarray(mass)).to(dev).double()
+    st = torch.cuda.current_stream(dev).cuda_stream
+    times = []
+    for _ in range(4):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        h = ctypes.c_void_p()
+        _lib.check(lb.jb_tree_build_device(p.shape[0], p.data_ptr(), m.data_ptr(), int(cfg["leaf_size"]),
+                                           float(cfg["theta"]), st, ctypes.byref(h)), "jb_tree_build_device")
+        torch.cuda.synchronize(dev)
+        times.append((time.perf_counter() - t0) * 1e3)
+        lb.jb_dtree_free(h)
+    out = {"tree_gpu_ms_first": times[0], "tree_gpu_ms": float(np.median(times[1:])),
+           "what": "Morton sort + radix split + FP64 COM/radii + dual walk + CSR lists, on the GPU"}
+    if with_host:
+        dev_topo = tree.build_topology(p, m, leaf_size=cfg["leaf_size"], theta=cfg["theta"], device=dev)
+        t0 = time.perf_counter()
+        host = tree.build_topology(pos, mass, leaf_size=cfg["leaf_size"], theta=cfg["theta"])
+        out["tree_host_s"] = time.perf_counter() - t0
+        out["tree_host_threads"] = os.cpu_count()
+        out["identical_to_host"] = all(
+            np.array_equal(getattr(dev_topo, f), getattr(host, f))
+            for f in ("permutation", "node_ranges", "left_child", "right_child", "parent", "node_level",
+                      "level_offsets", "leaf_of_particle", "far_offsets", "far_sources", "near_offsets",
+                      "near_leaves", "centers_f64", "radii_f64"))
+    return out
+
+
 def measure_extras(dev, stream) -> dict:
     """The other BASELINE configs on the same GPU, reported beside the headline:
     Plummer N=1,048,576, p=6, leaf 32: evaluate_prepared_state on 65,536
@@ -481,6 +522,7 @@ def main() -> None:
                "sample": f"one float32 pass of the oracle on clustered N={ns} (same generator/order/leaf/theta)"}
 
     extras = measure_extras(dev, stream) if (rank == 0 and world == 1 and not args.no_extras) else None
+    prep = measure_prepare(pos, mass, cfg, dev, with_host=not args.no_extras) if rank == 0 else None
     launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
     if rank == 0:
         cfg.update({
@@ -503,6 +545,7 @@ def main() -> None:
             "err_targets": int(tg.size),
             "err_bound_met": bool(errs["chosen"]["p99"] <= ERR_BOUND),
             "prepare_s": prep_s,
+            "prepare": prep,
             "num_nodes": topo.num_nodes,
             "far_pairs": topo.num_far_pairs,
             "near_leaf_pairs": topo.num_near_pairs,

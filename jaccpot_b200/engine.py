@@ -10,6 +10,8 @@ only; every arithmetic step is a kernel of libjaccpot_b200.so.
 
 from __future__ import annotations
 
+import copy
+
 from dataclasses import dataclass
 
 import numpy as np
@@ -138,6 +140,21 @@ class Pass:
         self.d_leaf_runs = up(self.leaf_sched.runs)
         self.d_leaf_split = up(self.leaf_sched.split)
         self.leaf_partials = torch.empty((max(self.leaf_sched.num_slots, 1) * 32, 4), device=dev, dtype=torch.float32)
+
+    def fork(self) -> "Pass":
+        """A pass over the same topology and work-unit schedules (shared,
+        read-only) with its own workspace and scratch rows, so the two can run
+        side by side; lazily built tensor-core and adjoint state is rebuilt on
+        first use."""
+        q = copy.copy(self)
+        q.ws = Workspace.allocate(self.dt, self.p)
+        q.m2l_partials = torch.empty_like(self.m2l_partials)
+        q.leaf_partials = torch.empty_like(self.leaf_partials)
+        if getattr(self, "gear_sched", None) is not None:
+            q.gear_partials = torch.empty_like(self.gear_partials)
+        for name in ("_tc", "_tc_status", "_adj", "_adj_sched", "_adj_m2l"):
+            q.__dict__.pop(name, None)
+        return q
 
     # -- stages -------------------------------------------------------------
     def load_particles(self, positions: torch.Tensor, masses: torch.Tensor, stream=None) -> None:

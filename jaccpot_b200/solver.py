@@ -133,6 +133,10 @@ class FastMultipoleMethod:
         topo = build_topology(positions if isinstance(positions, torch.Tensor) else pos_np,
                               masses if isinstance(masses, torch.Tensor) else mass_np, leaf_size=int(leaf_size),
                               theta=th, device=self.device if self.device.type == "cuda" else None)
+        return self._prepare_from_topology(topo, positions, masses, int(max_order), th, int(leaf_size))
+
+    def _prepare_from_topology(self, topo: Topology, positions, masses, max_order: int, th: float,
+                               leaf_size: int) -> FMMPreparedState:
         dt = DeviceTopology(topo, self.device)
         dt.validate()
         ps = Pass(dt, int(max_order), G=self.G, eps2=self.softening ** 2, m2l_mode=self.m2l_mode,
@@ -150,10 +154,96 @@ class FastMultipoleMethod:
         ps.upward()
         ps.downward()
         st = FMMPreparedState(topology=topo, device_topology=dt, pass_=ps, max_order=int(max_order), theta=th,
-                              leaf_size=int(leaf_size), num_particles=int(pos_np.shape[0]),
+                              leaf_size=int(leaf_size), num_particles=int(topo.num_particles),
                               input_dtype=positions.dtype if hasattr(positions, "dtype") else np.float64)
         self._last_state = st
         return st
+
+    # ------------------------------------------------------------------ refresh
+    def refresh_prepared_state(self, prepared_state: FMMPreparedState, positions, masses, *, bounds=None,
+                               leaf_size: Optional[int] = None, max_order: Optional[int] = None,
+                               theta: Optional[float] = None, fused_device_mode: bool = False) -> FMMPreparedState:
+        """Rebinds a prepared state to new particle data without a full prepare
+        (solver.py:1604 / runtime/fmm_strict_run.py:54-200 there, whose fast path
+        is _refresh_large_n_same_topology :1152).
+
+        Same-topology fast path: the tree and lists of the new particles are
+        built on the GPU and compared there with the state's (Morton order,
+        node ranges, far and near lists).  When they are identical the state's
+        work-unit schedules are reused and only the numeric payloads --
+        particles, centres, multipoles, locals (and the gears, when adaptive)
+        -- are recomputed, which gives exactly what ``prepare_state`` would.
+        Otherwise, or when leaf_size / max_order / theta change, it is a full
+        ``prepare_state``.  Returns a new state; the old one stays valid.
+        ``refresh_stats`` counts attempts, hits and the reason of each miss.
+        ``bounds`` and ``fused_device_mode`` are accepted for signature
+        compatibility (the state is always device resident)."""
+        from dataclasses import replace
+
+        from .tree import DeviceTree
+
+        st = prepared_state
+        stats = self.__dict__.setdefault("refresh_stats", {"attempts": 0, "hits": 0, "miss_config": 0,
+                                                             "miss_topology": 0})
+        stats["attempts"] += 1
+        leaf = st.leaf_size if leaf_size is None else int(leaf_size)
+        order = st.max_order if max_order is None else int(max_order)
+        th = st.theta if theta is None else float(theta)
+        if (leaf, order, th) != (st.leaf_size, st.max_order, st.theta) or self.device.type != "cuda":
+            stats["miss_config"] += 1
+            return self.prepare_state(positions, masses, bounds=bounds, leaf_size=leaf, max_order=order, theta=th)
+        dt = st.device_topology
+        t = st.topology
+        with DeviceTree(positions, masses, leaf_size=leaf, theta=th, device=self.device) as nt:
+            i = nt.info
+            same = (i.num_nodes, i.num_internal, i.num_far_pairs, i.num_near_pairs) == (
+                t.num_nodes, t.num_internal, t.num_far_pairs, t.num_near_pairs)
+            if same:
+                same = (torch.equal(nt.field("permutation"), dt.perm)
+                        and torch.equal(nt.field("node_ranges"), dt.node_ranges)
+                        and torch.equal(nt.field("far_offsets"), dt.far_off)
+                        and torch.equal(nt.field("near_offsets"), dt.near_off)
+                        and (t.num_far_pairs == 0 or torch.equal(nt.field("far_sources"), dt.far_src))
+                        and (t.num_near_pairs == 0 or torch.equal(nt.field("near_leaves"), dt.near_src)))
+            if not same:
+                stats["miss_topology"] += 1
+                topo = nt.topology()
+            else:
+                centers = nt.field("centers_f64").reshape(-1, 3).cpu().numpy()
+                radii = nt.field("radii_f64").cpu().numpy()
+        if not same:
+            return self._prepare_from_topology(topo, positions, masses, order, th, leaf)
+        stats["hits"] += 1
+        ps = st.pass_.fork()
+        ps.load_particles(_to_torch(positions, self.device, torch.float32),
+                          _to_torch(masses, self.device, torch.float32))
+        if self.adaptive_order:
+            from . import gears as _gears
+
+            model = self.gear_model if self.gear_model is not None else _gears.GearModel.load()
+            _gears.apply_gears(ps, model)
+        ps.upward()
+        ps.downward()
+        new = FMMPreparedState(topology=replace(t, centers_f64=centers, radii_f64=radii), device_topology=dt,
+                               pass_=ps, max_order=st.max_order, theta=st.theta, leaf_size=st.leaf_size,
+                               num_particles=st.num_particles,
+                               input_dtype=positions.dtype if hasattr(positions, "dtype") else np.float64)
+        self._last_state = new
+        return new
+
+    def strict_prepare_refresh_and_evaluate(self, prepared_state: Optional[FMMPreparedState], positions, masses, *,
+                                            bounds=None, leaf_size: int = 16, max_order: int = 4,
+                                            theta: Optional[float] = None, jit_traversal=True):
+        """Prepare when ``prepared_state`` is None, refresh it otherwise, then
+        evaluate every particle (solver.py:1664 there): a time-stepping loop
+        calls this unconditionally.  Returns (state, accelerations)."""
+        if prepared_state is None:
+            st = self.prepare_state(positions, masses, bounds=bounds, leaf_size=leaf_size, max_order=max_order,
+                                    theta=theta)
+        else:
+            st = self.refresh_prepared_state(prepared_state, positions, masses, bounds=bounds,
+                                             leaf_size=leaf_size, max_order=max_order, theta=theta)
+        return st, self.evaluate_prepared_state(st, as_numpy=not isinstance(positions, torch.Tensor))
 
     # ----------------------------------------------------------------- evaluate
     def evaluate_prepared_state(self, state: FMMPreparedState, *, target_indices=None,

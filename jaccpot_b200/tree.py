@@ -178,27 +178,73 @@ def build_topology(positions, masses, *, leaf_size: int = 16, theta: float = 0.6
     return _topology(n, info, arrs, leaf_size, theta)
 
 
+class DeviceTree:
+    """Owner of a ``jb_tree_build_device`` handle: the tree and lists of a
+    particle set, resident on the GPU.  ``field(name)`` is a zero-copy torch
+    view of one array (valid while the handle lives); ``topology()`` copies
+    everything back into a :class:`Topology`.  Use as a context manager or
+    call ``free()``."""
+
+    _DTYPES = {np.dtype(np.int64): "<i8", np.dtype(np.int32): "<i4", np.dtype(np.float64): "<f8"}
+
+    def __init__(self, positions, masses, *, leaf_size: int = 16, theta: float = 0.6, device="cuda"):
+        import torch
+
+        self._torch = torch
+        pos = torch.as_tensor(positions).to(device=device, dtype=torch.float64).reshape(-1, 3).contiguous()
+        mass = torch.as_tensor(masses).to(device=device, dtype=torch.float64).reshape(-1).contiguous()
+        n = pos.shape[0]
+        if mass.shape[0] != n:
+            raise ValueError("positions and masses disagree in length")
+        self.n, self.leaf_size, self.theta, self.device = int(n), int(leaf_size), float(theta), pos.device
+        self._lb = _lib.lib()
+        self._h = ctypes.c_void_p()
+        stream = torch.cuda.current_stream(pos.device).cuda_stream
+        _lib.check(self._lb.jb_tree_build_device(n, pos.data_ptr(), mass.data_ptr(), self.leaf_size, self.theta,
+                                                 stream, ctypes.byref(self._h)), "jb_tree_build_device")
+        self.info = _lib.TreeInfo()
+        _lib.check(self._lb.jb_dtree_info(self._h, ctypes.byref(self.info)), "jb_dtree_info")
+        self.sizes = _field_sizes(self.n, self.info)
+
+    def field(self, name: str):
+        fid, dt = _lib.TREE_FIELDS[name]
+        ptr = self._lb.jb_dtree_field(self._h, fid)
+        n = self.sizes[name]
+
+        class _View:  # __cuda_array_interface__ v3 over the handle's memory
+            __cuda_array_interface__ = {"shape": (n,), "typestr": DeviceTree._DTYPES[np.dtype(dt)],
+                                        "data": (int(ptr or 0), False), "version": 3, "strides": None}
+
+        if n == 0:
+            return self._torch.zeros(0, dtype=self._torch.from_numpy(np.zeros(0, dt)).dtype, device=self.device)
+        return self._torch.as_tensor(_View(), device=self.device)
+
+    def topology(self) -> Topology:
+        arrs = _copy_fields(self._lb.jb_dtree_copy, self._h, self.n, self.info)
+        return _topology(self.n, self.info, arrs, self.leaf_size, self.theta)
+
+    def free(self) -> None:
+        if self._h:
+            self._lb.jb_dtree_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:  # interpreter shutdown
+            pass
+
+
 def build_topology_device(positions, masses, *, leaf_size: int = 16, theta: float = 0.6, device="cuda") -> Topology:
     """The tree and lists built on the GPU by ``jb_tree_build_device``
     (csrc/tree_gpu.cu) from float64 copies of the inputs on ``device``; the
     arrays are copied back into the same :class:`Topology` the host build
     returns."""
-    import torch
-
-    pos = torch.as_tensor(positions).to(device=device, dtype=torch.float64).reshape(-1, 3).contiguous()
-    mass = torch.as_tensor(masses).to(device=device, dtype=torch.float64).reshape(-1).contiguous()
-    n = pos.shape[0]
-    if mass.shape[0] != n:
-        raise ValueError("positions and masses disagree in length")
-    lb = _lib.lib()
-    h = ctypes.c_void_p()
-    stream = torch.cuda.current_stream(pos.device).cuda_stream
-    _lib.check(lb.jb_tree_build_device(n, pos.data_ptr(), mass.data_ptr(), int(leaf_size), float(theta), stream,
-                                       ctypes.byref(h)), "jb_tree_build_device")
-    try:
-        info = _lib.TreeInfo()
-        _lib.check(lb.jb_dtree_info(h, ctypes.byref(info)), "jb_dtree_info")
-        arrs = _copy_fields(lb.jb_dtree_copy, h, n, info)
-    finally:
-        lb.jb_dtree_free(h)
-    return _topology(n, info, arrs, leaf_size, theta)
+    with DeviceTree(positions, masses, leaf_size=leaf_size, theta=theta, device=device) as dtree:
+        return dtree.topology()
