@@ -121,6 +121,42 @@ JB_API const void* jb_dtree_field(const jb_dtree* t, int field);
 JB_API int jb_dtree_copy(const jb_dtree* t, int field, void* dst);
 JB_API void jb_dtree_free(jb_dtree* t);
 
+/* Work-unit schedules built on the GPU (csrc/schedule_gpu.cu) from device
+ * lists, entry for entry the arrays of the host builders in schedule.py
+ * (m2l_schedule, leaf_schedule, gear_m2l_schedule); the prepare-time
+ * planning that the reference does for its M2L chunks
+ * (runtime/kernels/_m2l.py:1667) and near-field schedules
+ * (nearfield/_schedules.py:271).  All pointers are DEVICE memory; the handle
+ * owns its outputs (pool memory, freed on the build stream).  The calls
+ * synchronise the stream.                                                   */
+typedef struct jb_dsched jb_dsched;
+typedef struct {
+  int64_t num_units, num_split, num_slots, num_runs, num_targets;
+} jb_sched_info_t;
+enum {
+  JB_SCHED_UNITS = 0,          /* int32[num_units][4] */
+  JB_SCHED_AUX = 1,            /* int32[num_units][2] (leaf schedule) */
+  JB_SCHED_RUNS = 2,           /* int32[num_runs][2] (leaf schedule) */
+  JB_SCHED_SPLIT = 3,          /* int32[num_split][4] */
+  JB_SCHED_FAR_SOURCES = 4,    /* int32[num_far] regrouped by gear (gear schedule) */
+  JB_SCHED_GEAR_OFFSETS = 5,   /* int64[num_gears+1] (gear schedule) */
+  JB_SCHED_TARGETS = 6,        /* int32[num_targets] (M2L schedule) */
+  JB_SCHED_PAIRS_PER_GEAR = 7  /* int64[num_gears] (gear schedule) */
+};
+/* targets == NULL: every node with far pairs, longest list first. */
+JB_API int jb_m2l_schedule_device(int num_nodes, const int64_t* far_off, int max_pairs, int num_targets,
+                                  const int* targets, void* stream, jb_dsched** out);
+/* Leaves [leaf_lo, leaf_hi); max_sources >= 1. */
+JB_API int jb_leaf_schedule_device(int num_internal, int num_leaves, const int* node_ranges, const int64_t* near_off,
+                                   const int* near_src, int leaf_lo, int leaf_hi, int max_sources, void* stream,
+                                   jb_dsched** out);
+/* gears: int32 per far pair in [0, num_gears) (JB_ERR_INDEX otherwise). */
+JB_API int jb_gear_schedule_device(int num_nodes, const int64_t* far_off, const int* far_src, const int* gears,
+                                   int num_gears, int max_pairs, void* stream, jb_dsched** out);
+JB_API int jb_dsched_info(const jb_dsched* d, jb_sched_info_t* info);
+JB_API const void* jb_dsched_field(const jb_dsched* d, int field);
+JB_API void jb_dsched_free(jb_dsched* d);
+
 /* ------------------------------------------------------------------------ */
 /* Device pass.                                                             */
 /* ------------------------------------------------------------------------ */

@@ -28,6 +28,8 @@ JB_MAX_ORDER = 10
 JB_M2L_FP32, JB_M2L_SPLIT_BF16 = 0, 1
 JB_P2P_FP32, JB_P2P_KAHAN, JB_P2P_POTENTIAL = 0, 1, 2
 JB_LEAF_EVAL_NOALLOC_MAX_SLOTS = 32768
+(JB_SCHED_UNITS, JB_SCHED_AUX, JB_SCHED_RUNS, JB_SCHED_SPLIT, JB_SCHED_FAR_SOURCES, JB_SCHED_GEAR_OFFSETS,
+ JB_SCHED_TARGETS, JB_SCHED_PAIRS_PER_GEAR) = range(8)
 
 # jb_tree_copy field ids
 TREE_FIELDS = {
@@ -83,6 +85,12 @@ _SIGNATURES = {
     "jb_dtree_field": [_P, _I],
     "jb_dtree_copy": [_P, _I, _P],
     "jb_dtree_free": [_P],
+    "jb_m2l_schedule_device": [_I, _P, _I, _I, _P, _P, ctypes.POINTER(_P)],
+    "jb_leaf_schedule_device": [_I, _I, _P, _P, _P, _I, _I, _I, _P, ctypes.POINTER(_P)],
+    "jb_gear_schedule_device": [_I, _P, _P, _P, _I, _I, _P, ctypes.POINTER(_P)],
+    "jb_dsched_info": [_P, _P],
+    "jb_dsched_field": [_P, _I],
+    "jb_dsched_free": [_P],
     "jb_coeff_stride": [_I],
     "jb_last_cuda_error": [],
     "jb_gather_sorted": [_I64, _P, _P, _P, _P, _P],
@@ -133,8 +141,8 @@ def lib() -> ctypes.CDLL:
             fn = getattr(lb, name)
             fn.argtypes = args
             fn.restype = ctypes.c_char_p if name == "jb_last_cuda_error" else (
-                None if name in ("jb_tree_free", "jb_dtree_free") else (
-                    ctypes.c_void_p if name == "jb_dtree_field" else ctypes.c_int))
+                None if name in ("jb_tree_free", "jb_dtree_free", "jb_dsched_free") else (
+                    ctypes.c_void_p if name in ("jb_dtree_field", "jb_dsched_field") else ctypes.c_int))
         _lib = lb
     return _lib
 

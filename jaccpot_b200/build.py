@@ -86,8 +86,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     # The device tree build reproduces the host builder's FP64 arithmetic
     # operation for operation, so nothing in it may be contracted into an FMA.
     tg_src, tg_obj = CSRC / "tree_gpu.cu", OBJ_DIR / "tree_gpu.o"
-    if _stale(tg_obj, [tg_src, INCLUDE / "jaccpot_b200.h"]):
+    if _stale(tg_obj, [tg_src, CSRC / "dev_prims.cuh", INCLUDE / "jaccpot_b200.h"]):
         jobs_todo.append([nvcc, *NVCC_FLAGS, "-fmad=false", "-c", str(tg_src), "-o", str(tg_obj)])
+    sg_src, sg_obj = CSRC / "schedule_gpu.cu", OBJ_DIR / "schedule_gpu.o"
+    if _stale(sg_obj, [sg_src, CSRC / "dev_prims.cuh", INCLUDE / "jaccpot_b200.h"]):
+        jobs_todo.append([nvcc, *NVCC_FLAGS, "-c", str(sg_src), "-o", str(sg_obj)])
     tb_obj = OBJ_DIR / "tree_build.o"
     if _stale(tb_obj, _deps(CSRC / "tree_build.cpp")):
         jobs_todo.append([_cxx(), "-O3", "-fopenmp", "-fPIC", "-std=c++17", "-I", str(INCLUDE),

@@ -18,7 +18,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .schedule import gear_m2l_schedule, leaf_schedule, m2l_schedule, tc_m2l_schedule
+from .schedule import (gear_m2l_schedule, gear_m2l_schedule_device, leaf_schedule, leaf_schedule_device,
+                       m2l_schedule, m2l_schedule_device, tc_m2l_schedule)
 from .tree import Topology
 
 
@@ -93,6 +94,18 @@ class Workspace:
         )
 
 
+def _up(a, dev) -> torch.Tensor:
+    """Schedule array on the device (a dummy row when empty, so the pointer
+    handed to the library is never null)."""
+    if torch.is_tensor(a):
+        return a if a.numel() else torch.zeros(4, dtype=torch.int32, device=dev)
+    return torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+
+
+def _on_gpu(dt) -> bool:
+    return torch.device(dt.device).type == "cuda"
+
+
 class Pass:
     """One evaluation pass over a resident topology; every method enqueues
     kernels on `stream` (default: torch's current stream) and returns."""
@@ -127,10 +140,16 @@ class Pass:
             hi = int(t.node_ranges[t.num_internal + self.leaf_range[1] - 1, 1])
             tg = t.m2l_targets
             targets = tg[(t.node_ranges[tg, 1] >= lo) & (t.node_ranges[tg, 0] <= hi)]
-        self.m2l_sched = m2l_schedule(t, max_pairs=m2l_unit_pairs, targets=targets)
-        self.leaf_sched = leaf_schedule(t, max_sources=leaf_unit_sources, leaf_range=self.leaf_range)
+        # work-unit schedules: built on the GPU from the resident lists when
+        # the pass runs there (the host builders give the same arrays)
+        if _on_gpu(dt):
+            self.m2l_sched = m2l_schedule_device(dt, max_pairs=m2l_unit_pairs, targets=targets)
+            self.leaf_sched = leaf_schedule_device(dt, max_sources=leaf_unit_sources, leaf_range=self.leaf_range)
+        else:
+            self.m2l_sched = m2l_schedule(t, max_pairs=m2l_unit_pairs, targets=targets)
+            self.leaf_sched = leaf_schedule(t, max_sources=leaf_unit_sources, leaf_range=self.leaf_range)
         dev = dt.device
-        up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+        up = lambda a: _up(a, dev)
         self.d_m2l_units = up(self.m2l_sched.units)
         self.d_m2l_split = up(self.m2l_sched.split)
         self.m2l_partials = torch.empty((max(self.m2l_sched.num_slots, 1), self.ws.stride), device=dev,
@@ -186,9 +205,12 @@ class Pass:
         orders = tuple(int(o) for o in orders)
         if max(orders) > self.p or min(orders) < 1:
             raise ValueError(f"gear orders must lie in [1, {self.p}]")
-        gs = gear_m2l_schedule(self.dt.topo, np.asarray(gears), orders)
+        if _on_gpu(self.dt):
+            gs = gear_m2l_schedule_device(self.dt, gears, orders)
+        else:
+            gs = gear_m2l_schedule(self.dt.topo, np.asarray(gears), orders)
         dev = self.dt.device
-        up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+        up = lambda a: _up(a, dev)
         self.gear_sched = gs
         self.d_gear_units = up(gs.units)
         self.d_gear_split = up(gs.split)
@@ -323,8 +345,9 @@ class Pass:
             if not t.near_lists_symmetric():
                 raise ValueError("the near-field adjoint needs symmetric neighbour lists")
             # full near list of every leaf (the forward schedule may be a leaf range)
-            self._adj_sched = leaf_schedule(t, max_sources=4096)
-            up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dev)
+            self._adj_sched = (leaf_schedule_device(self.dt, max_sources=4096) if _on_gpu(self.dt)
+                               else leaf_schedule(t, max_sources=4096))
+            up = lambda a: _up(a, dev)
             self._adj["units"] = up(self._adj_sched.units)
             self._adj["aux"] = up(self._adj_sched.aux)
             self._adj["runs"] = up(self._adj_sched.runs)
@@ -367,10 +390,12 @@ class Pass:
             _lib.check(lb.jb_adj_l2l_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
                                            _ptr(ws.centers), _ptr(ws.locals), _ptr(A["lbar"]), _ptr(A["cbar4"]), s),
                        "jb_adj_l2l_level")
-        msc = m2l_schedule(t, max_pairs=64) if not hasattr(self, "_adj_m2l") else self._adj_m2l
-        if not hasattr(self, "_adj_m2l"):
+        if hasattr(self, "_adj_m2l"):
+            msc = self._adj_m2l
+        else:
+            msc = m2l_schedule_device(dt, max_pairs=64) if _on_gpu(dt) else m2l_schedule(t, max_pairs=64)
             self._adj_m2l = msc
-            up = lambda a: torch.from_numpy(a if a.size else np.zeros(4, np.int32)).to(dt.device)
+            up = lambda a: _up(a, dt.device)
             A["m2l_units"], A["m2l_split"] = up(msc.units), up(msc.split)
             A["m2l_partials"] = torch.empty((max(msc.num_slots, 1), ws.stride), device=dt.device,
                                             dtype=torch.float32)

@@ -131,9 +131,9 @@ def apply_gears(ps: engine.Pass, model: GearModel) -> np.ndarray:
     ps.run()
     ctx = GearContext(ps)
     ctx.node_features()
-    gears = ctx.select(model).cpu().numpy()
+    gears = ctx.select(model)
     ps.set_gears(gears, model.orders)
-    return gears
+    return gears.cpu().numpy()
 
 
 # ---------------------------------------------------------------------------

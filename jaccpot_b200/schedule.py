@@ -241,3 +241,119 @@ def leaf_schedule(topo: Topology, max_sources: int = 4096, leaf_range: tuple[int
                      axis=1).astype(np.int32)
     return LeafSchedule(np.ascontiguousarray(units[srt]), np.ascontiguousarray(aux[srt]),
                         np.ascontiguousarray(runs), np.ascontiguousarray(split), int((slot >= 0).sum()))
+
+
+# ---------------------------------------------------------------------------
+# The same schedules built on the GPU (csrc/schedule_gpu.cu).  They take the
+# device-resident lists of an engine.DeviceTopology and return the same
+# dataclasses with torch tensors (on the device) in place of the index arrays;
+# gear_offsets and pairs_per_gear stay on the host (kernel launch bounds).
+# ---------------------------------------------------------------------------
+def _sched_info_cls():
+    import ctypes
+
+    class SchedInfo(ctypes.Structure):
+        _fields_ = [("num_units", ctypes.c_int64), ("num_split", ctypes.c_int64), ("num_slots", ctypes.c_int64),
+                    ("num_runs", ctypes.c_int64), ("num_targets", ctypes.c_int64)]
+
+    return SchedInfo
+
+
+_SchedInfo = None
+
+
+def _run_device(fn_name: str, args: list, device):
+    """Calls one jb_*_schedule_device builder; returns (info, field getter, free)."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+    from .tree import device_view
+
+    global _SchedInfo
+    if _SchedInfo is None:
+        _SchedInfo = _sched_info_cls()
+    lb = _lib.lib()
+    h = ctypes.c_void_p()
+    stream = torch.cuda.current_stream(device).cuda_stream
+    _lib.check(getattr(lb, fn_name)(*args, stream, ctypes.byref(h)), fn_name)
+    info = _SchedInfo()
+    _lib.check(lb.jb_dsched_info(h, ctypes.byref(info)), "jb_dsched_info")
+
+    def field(fid: int, shape, dtype):
+        return device_view(lb.jb_dsched_field(h, fid), shape, dtype, device).clone()
+
+    return info, field, (lambda: lb.jb_dsched_free(h))
+
+
+def _ptr(t) -> int:
+    return int(t.data_ptr())
+
+
+def m2l_schedule_device(dt, max_pairs: int = 64, targets=None) -> M2LSchedule:
+    """GPU twin of :func:`m2l_schedule` over ``dt`` (engine.DeviceTopology)."""
+    import torch
+
+    from . import _lib
+
+    t = dt.topo
+    tg = None
+    if targets is not None:
+        tg = torch.as_tensor(np.asarray(targets, dtype=np.int32)).to(dt.device)
+    info, field, free = _run_device("jb_m2l_schedule_device",
+                                    [t.num_nodes, _ptr(dt.far_off), int(max_pairs),
+                                     -1 if tg is None else int(tg.numel()), None if tg is None else _ptr(tg)],
+                                    dt.device)
+    try:
+        units = field(_lib.JB_SCHED_UNITS, (info.num_units, 4), np.int32)
+        split = field(_lib.JB_SCHED_SPLIT, (info.num_split, 4), np.int32)
+    finally:
+        free()
+    return M2LSchedule(units, split, int(info.num_slots))
+
+
+def leaf_schedule_device(dt, max_sources: int = 4096, leaf_range: tuple[int, int] | None = None) -> LeafSchedule:
+    """GPU twin of :func:`leaf_schedule` over ``dt`` (engine.DeviceTopology)."""
+    from . import _lib
+
+    t = dt.topo
+    lo, hi = (0, t.num_leaves) if leaf_range is None else (int(leaf_range[0]), int(leaf_range[1]))
+    info, field, free = _run_device("jb_leaf_schedule_device",
+                                    [t.num_internal, t.num_leaves, _ptr(dt.node_ranges), _ptr(dt.near_off),
+                                     _ptr(dt.near_src), lo, hi, int(max_sources)], dt.device)
+    try:
+        units = field(_lib.JB_SCHED_UNITS, (info.num_units, 4), np.int32)
+        aux = field(_lib.JB_SCHED_AUX, (info.num_units, 2), np.int32)
+        runs = field(_lib.JB_SCHED_RUNS, (info.num_runs, 2), np.int32)
+        split = field(_lib.JB_SCHED_SPLIT, (info.num_split, 4), np.int32)
+    finally:
+        free()
+    return LeafSchedule(units, aux, runs, split, int(info.num_slots))
+
+
+def gear_m2l_schedule_device(dt, gears, orders, max_pairs: int = 64) -> GearM2LSchedule:
+    """GPU twin of :func:`gear_m2l_schedule`; ``gears`` is one int per far pair
+    (numpy or torch)."""
+    import torch
+
+    from . import _lib
+
+    t = dt.topo
+    g = torch.as_tensor(gears).to(device=dt.device, dtype=torch.int32).reshape(-1).contiguous()
+    if g.numel() != t.num_far_pairs:
+        raise ValueError("one gear per far pair is required")
+    ng = len(orders)
+    info, field, free = _run_device("jb_gear_schedule_device",
+                                    [t.num_nodes, _ptr(dt.far_off), _ptr(dt.far_src), _ptr(g), ng, int(max_pairs)],
+                                    dt.device)
+    try:
+        units = field(_lib.JB_SCHED_UNITS, (info.num_units, 4), np.int32)
+        split = field(_lib.JB_SCHED_SPLIT, (info.num_split, 4), np.int32)
+        far_src = field(_lib.JB_SCHED_FAR_SOURCES, (t.num_far_pairs,), np.int32)
+        gear_offsets = field(_lib.JB_SCHED_GEAR_OFFSETS, (ng + 1,), np.int64).cpu().numpy()
+        ppg = field(_lib.JB_SCHED_PAIRS_PER_GEAR, (ng,), np.int64).cpu().numpy()
+    finally:
+        free()
+    return GearM2LSchedule(units, split, int(info.num_slots), far_src, gear_offsets, tuple(int(o) for o in orders),
+                           ppg)

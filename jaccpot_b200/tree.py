@@ -178,14 +178,29 @@ def build_topology(positions, masses, *, leaf_size: int = 16, theta: float = 0.6
     return _topology(n, info, arrs, leaf_size, theta)
 
 
+def device_view(ptr, shape, dtype, device):
+    """Zero-copy torch view (``__cuda_array_interface__`` v3) of device memory
+    owned by a library handle; valid while the handle lives."""
+    import torch
+
+    dtype = np.dtype(dtype)
+    shape = tuple(int(x) for x in shape)
+    if int(np.prod(shape)) == 0:
+        return torch.zeros(shape, dtype=torch.from_numpy(np.zeros(0, dtype)).dtype, device=device)
+
+    class _View:
+        __cuda_array_interface__ = {"shape": shape, "typestr": dtype.str, "data": (int(ptr), False), "version": 3,
+                                    "strides": None}
+
+    return torch.as_tensor(_View(), device=device)
+
+
 class DeviceTree:
     """Owner of a ``jb_tree_build_device`` handle: the tree and lists of a
     particle set, resident on the GPU.  ``field(name)`` is a zero-copy torch
     view of one array (valid while the handle lives); ``topology()`` copies
     everything back into a :class:`Topology`.  Use as a context manager or
     call ``free()``."""
-
-    _DTYPES = {np.dtype(np.int64): "<i8", np.dtype(np.int32): "<i4", np.dtype(np.float64): "<f8"}
 
     def __init__(self, positions, masses, *, leaf_size: int = 16, theta: float = 0.6, device="cuda"):
         import torch
@@ -208,16 +223,7 @@ class DeviceTree:
 
     def field(self, name: str):
         fid, dt = _lib.TREE_FIELDS[name]
-        ptr = self._lb.jb_dtree_field(self._h, fid)
-        n = self.sizes[name]
-
-        class _View:  # __cuda_array_interface__ v3 over the handle's memory
-            __cuda_array_interface__ = {"shape": (n,), "typestr": DeviceTree._DTYPES[np.dtype(dt)],
-                                        "data": (int(ptr or 0), False), "version": 3, "strides": None}
-
-        if n == 0:
-            return self._torch.zeros(0, dtype=self._torch.from_numpy(np.zeros(0, dt)).dtype, device=self.device)
-        return self._torch.as_tensor(_View(), device=self.device)
+        return device_view(self._lb.jb_dtree_field(self._h, fid), (self.sizes[name],), dt, self.device)
 
     def topology(self) -> Topology:
         arrs = _copy_fields(self._lb.jb_dtree_copy, self._h, self.n, self.info)
