@@ -478,18 +478,26 @@ void build_leaf(jb_dsched& d, int num_internal, const int* ranges, const int64_t
 // ---------------------------------------------------------------------------
 // A gear outside [0, num_gears) is counted in *bad and sorts as gear 0 (the
 // call then fails with JB_ERR_INDEX).
-__global__ void k_gear_keys(const int* __restrict__ row, const int* __restrict__ gears, int64_t P, int gb,
-                            int num_gears, uint64_t* __restrict__ key, unsigned long long* __restrict__ ppg,
-                            int* __restrict__ bad) {
+// Per-gear pair counts go through a shared-memory histogram (one global add
+// per block and gear), since every pair hits one of a few counters.
+__global__ void __launch_bounds__(256) k_gear_keys(const int* __restrict__ row, const int* __restrict__ gears, int64_t P,
+                                                   int gb, int num_gears, uint64_t* __restrict__ key,
+                                                   unsigned long long* __restrict__ ppg, int* __restrict__ bad) {
+  __shared__ unsigned int hist[64];
+  if (threadIdx.x < 64) hist[threadIdx.x] = 0;
+  __syncthreads();
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= P) return;
-  int g = gears[e];
-  if (g < 0 || g >= num_gears) {
-    atomicAdd(bad, 1);
-    g = 0;
+  if (e < P) {
+    int g = gears[e];
+    if (g < 0 || g >= num_gears) {
+      atomicAdd(bad, 1);
+      g = 0;
+    }
+    key[e] = ((uint64_t)row[e] << gb) | (uint64_t)g;
+    atomicAdd(&hist[g], 1u);
   }
-  key[e] = ((uint64_t)row[e] << gb) | (uint64_t)g;
-  atomicAdd(&ppg[g], 1ull);
+  __syncthreads();
+  if ((int)threadIdx.x < num_gears && hist[threadIdx.x]) atomicAdd(&ppg[threadIdx.x], (unsigned long long)hist[threadIdx.x]);
 }
 
 __global__ void k_seg_brk(const uint64_t* __restrict__ key, int64_t P, int* __restrict__ brk) {
@@ -508,24 +516,31 @@ struct GearUnit {
   int t, g, s, e;
 };
 
-__global__ void k_gear_units(const int* __restrict__ sfirst, int NS, int64_t P, const uint64_t* __restrict__ key, int gb,
-                             int max_pairs, const int* __restrict__ nu, const int* __restrict__ unit_off,
-                             GearUnit* __restrict__ gu, int* __restrict__ n_per, int* __restrict__ tfirst,
-                             int* __restrict__ gcount) {
+__global__ void __launch_bounds__(128) k_gear_units(const int* __restrict__ sfirst, int NS, int64_t P,
+                                                    const uint64_t* __restrict__ key, int gb, int max_pairs,
+                                                    const int* __restrict__ nu, const int* __restrict__ unit_off,
+                                                    GearUnit* __restrict__ gu, int* __restrict__ n_per,
+                                                    int* __restrict__ tfirst, int* __restrict__ gcount) {
+  __shared__ int hist[64];
+  if (threadIdx.x < 64) hist[threadIdx.x] = 0;
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= NS) return;
-  const int64_t a = sfirst[i], b = (i + 1 < NS) ? sfirst[i + 1] : P;
-  const uint64_t k = key[a];
-  const int t = (int)(k >> gb), g = (int)(k & ((1ull << gb) - 1));
-  const int n = nu[i];
-  const bool first_seg_of_target = (i == 0) || (int)(key[sfirst[i - 1]] >> gb) != t;
-  if (first_seg_of_target) tfirst[t] = unit_off[i];
-  for (int q = 0; q < n; ++q) {
-    const int64_t s = a + (int64_t)q * max_pairs, e = min(s + (int64_t)max_pairs, b);
-    gu[unit_off[i] + q] = GearUnit{t, g, (int)s, (int)e};
+  if (i < NS) {
+    const int64_t a = sfirst[i], b = (i + 1 < NS) ? sfirst[i + 1] : P;
+    const uint64_t k = key[a];
+    const int t = (int)(k >> gb), g = (int)(k & ((1ull << gb) - 1));
+    const int n = nu[i];
+    const bool first_seg_of_target = (i == 0) || (int)(key[sfirst[i - 1]] >> gb) != t;
+    if (first_seg_of_target) tfirst[t] = unit_off[i];
+    for (int q = 0; q < n; ++q) {
+      const int64_t s = a + (int64_t)q * max_pairs, e = min(s + (int64_t)max_pairs, b);
+      gu[unit_off[i] + q] = GearUnit{t, g, (int)s, (int)e};
+    }
+    atomicAdd(&n_per[t], n);
+    atomicAdd(&hist[g], n);
   }
-  atomicAdd(&n_per[t], n);
-  atomicAdd(&gcount[g], n);
+  __syncthreads();
+  if (threadIdx.x < 64 && hist[threadIdx.x]) atomicAdd(&gcount[threadIdx.x], hist[threadIdx.x]);
 }
 
 __global__ void k_node_multi(const int* __restrict__ n_per, int nodes, int* __restrict__ mnp, int* __restrict__ sflag) {
