@@ -161,6 +161,12 @@ JB_API void jb_dsched_free(jb_dsched* d);
 /* Device pass.                                                             */
 /* ------------------------------------------------------------------------ */
 
+/* Level sweeps: levels with at most m2m_max_parents (l2l_max_parents)
+ * parents run the M2M (L2L) translations with each translation's degrees
+ * split over four warps (shorter chains), wider levels with one thread per
+ * translation.  Same operations either way.  Process-wide setting.          */
+JB_API int jb_set_level_split(int m2m_max_parents, int l2l_max_parents);
+
 /* Row stride (floats) of a coefficient array of order p: (p+1)^2 rounded up
  * to a multiple of 4.  Returns 0 for an unsupported order. */
 JB_API int jb_coeff_stride(int p);

@@ -85,6 +85,7 @@ _SIGNATURES = {
     "jb_dtree_field": [_P, _I],
     "jb_dtree_copy": [_P, _I, _P],
     "jb_dtree_free": [_P],
+    "jb_set_level_split": [_I, _I],
     "jb_m2l_schedule_device": [_I, _P, _I, _I, _P, _P, ctypes.POINTER(_P)],
     "jb_leaf_schedule_device": [_I, _I, _P, _P, _P, _I, _I, _I, _P, ctypes.POINTER(_P)],
     "jb_gear_schedule_device": [_I, _P, _P, _P, _I, _I, _P, ctypes.POINTER(_P)],

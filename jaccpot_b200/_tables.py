@@ -252,6 +252,33 @@ def generate_bu_code(out_path: Path, max_order: int = MAX_ORDER) -> Path:
                 lines.append("    }")
             lines.append("  }")
             lines.append("};")
+    # the same blocks one degree at a time (the level kernels split the
+    # degrees of one translation over several warps)
+    lines.append("template <int L, bool TR> struct BDeg;")
+    for ell in range(0, max_order + 1):
+        for tr in (False, True):
+            lines.append(f"template <> struct BDeg<{ell}, {'true' if tr else 'false'}> {{")
+            lines.append("  static __device__ __forceinline__ void apply(float* v) {")
+            if ell > 0:
+                b = bu_matrix(ell)
+                if tr:
+                    b = b.T
+                w = 2 * ell + 1
+                o = ell * ell
+                lines.append("    " + " ".join(f"const float i{j} = v[{o + j}];" for j in range(w)))
+                for i in range(w):
+                    terms = [(j, b[i, j]) for j in range(w) if abs(b[i, j]) > 1e-12]
+                    if not terms:
+                        lines.append(f"    v[{o + i}] = 0.f;")
+                        continue
+                    expr = f"{_flit(terms[0][1])} * i{terms[0][0]}"
+                    for j, val in terms[1:]:
+                        expr = f"fmaf({_flit(val)}, i{j}, {expr})"
+                    lines.append(f"    v[{o + i}] = {expr};")
+            else:
+                lines.append("    (void)v;")
+            lines.append("  }")
+            lines.append("};")
     lines.append("}  // namespace jb")
     text = "\n".join(lines) + "\n"
     out_path.parent.mkdir(parents=True, exist_ok=True)

@@ -7,6 +7,7 @@ JB_ORDERS(JB_DECLARE_ORDER)
 namespace jb {
 
 static thread_local char g_err[256] = {0};
+int g_split_max_parents[2] = {1 << 30, 2048};  // measured at clustered N=4M, p=8
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return JB_OK;
@@ -282,6 +283,13 @@ using namespace jb;
 #define ST(s) reinterpret_cast<cudaStream_t>(s)
 
 extern "C" {
+
+JB_API int jb_set_level_split(int m2m_max_parents, int l2l_max_parents) {
+  if (m2m_max_parents < 0 || l2l_max_parents < 0) return JB_ERR_ARG;
+  jb::g_split_max_parents[0] = m2m_max_parents;
+  jb::g_split_max_parents[1] = l2l_max_parents;
+  return JB_OK;
+}
 
 JB_API int jb_coeff_stride(int p) { return (p >= 1 && p <= JB_MAX_ORDER) ? cstride(p) : 0; }
 

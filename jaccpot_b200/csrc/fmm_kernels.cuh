@@ -19,6 +19,7 @@
 #include <stdio.h>
 
 #include <cstring>
+#include <type_traits>
 
 #include "../../include/jaccpot_b200.h"
 #include "fmm_ops.cuh"
@@ -27,6 +28,10 @@ namespace jb {
 
 // Defined in fmm_capi.cu.
 int cuda_status(cudaError_t e);
+// Levels with at most this many parents use the degree-split M2M [0] / L2L
+// [1] kernels, wider ones the thread-per-translation kernels
+// (jb_set_level_split).
+extern int g_split_max_parents[2];
 inline int launch_status() { return cuda_status(cudaGetLastError()); }
 
 // ---------------------------------------------------------------------------
@@ -277,6 +282,244 @@ static __global__ void __launch_bounds__(256) k_m2l_reduce(int num_split, const 
   float a = 0.f;
   for (int q = 0; q < sp.z; ++q) a += partials[(size_t)(sp.y + q) * CS + k];
   locals[(size_t)sp.x * CS + k] = a;
+}
+
+// ---------------------------------------------------------------------------
+// M2M / L2L, one level, degrees split over four warps.
+//
+// A translation's rotations and B products act on each degree separately;
+// only the z-shift mixes degrees.  So a block of four warps takes 32
+// translations (lane = translation) and warp q works on a fixed set of
+// degrees (kDegSet: the degrees dealt greedily by (2l+1)^2, largest first, so
+// the four chains are about equally long), exchanging the rotated vectors
+// once through shared memory for the z-shift.  Each warp's chain is about a
+// quarter of the single-thread one, which is what bounds these levels: even
+// the widest level here holds only ~31 k translations, far too few for the
+// single-thread form to fill the GPU.  The operations, their order and their
+// constants are those of m2m_pair / l2l_pair.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr unsigned kDegSet(int P, int q) {
+  int tot[4] = {0, 0, 0, 0};
+  unsigned mask[4] = {0u, 0u, 0u, 0u};
+  for (int l = P; l >= 0; --l) {
+    int best = 0;
+    for (int k = 1; k < 4; ++k)
+      if (tot[k] < tot[best]) best = k;
+    tot[best] += (2 * l + 1) * (2 * l + 1);
+    mask[best] |= 1u << l;
+  }
+  return mask[q];
+}
+
+// f(integral_constant<int, l>) for every degree l <= P in MASK, ascending.
+template <int P, unsigned MASK, int L = 0>
+struct ForDeg {
+  template <typename F>
+  static __device__ __forceinline__ void run(F&& f) {
+    if constexpr (L <= P) {
+      if constexpr (((MASK >> L) & 1u) != 0u) f(std::integral_constant<int, L>{});
+      ForDeg<P, MASK, L + 1>::run(f);
+    }
+  }
+};
+
+// dz_rot restricted to degree L (the same angle recurrence, so the same values).
+template <int L, bool NEG>
+__device__ __forceinline__ void dz_rot_deg(float* v, float c1, float s1) {
+  const float sa = NEG ? -s1 : s1;
+  float c = c1, s = sa;
+#pragma unroll
+  for (int m = 1; m <= L; ++m) {
+    if (m > 1) {
+      const float cn = c * c1 - s * sa;
+      s = fmaf(s, c1, c * sa);
+      c = cn;
+    }
+    const int ip = shi(L, m), im = shi(L, -m);
+    const float vp = v[ip], vm = v[im];
+    v[ip] = c * vp - s * vm;
+    v[im] = fmaf(s, vp, c * vm);
+  }
+}
+
+constexpr int kSplitItems = 32;  // translations per block (lane = translation)
+__host__ __device__ constexpr int xrow(int P) { return csize(P) | 1; }  // odd row: conflict-free exchange
+
+// One translation's degrees MASK of v (indexed by the full packed layout):
+// IS_M2M selects m2m_pair's chain (delta = child - parent), else l2l_pair's
+// (delta = parent - child).  xr: this translation's exchange row.
+template <int P, unsigned MASK, bool IS_M2M>
+__device__ __forceinline__ void split_translate(float* v, float dx, float dy, float dz, float* xr) {
+  float caz, saz, cax, sax, r;
+  align_cs(dx, dy, dz, caz, saz, cax, sax, r);
+  const float d = r < 1e-30f ? 0.f : r;
+  ForDeg<P, MASK>::run([&](auto lc) {
+    constexpr int L = decltype(lc)::value;
+    dz_rot_deg<L, false>(v, caz, saz);
+    BDeg<L, !IS_M2M>::apply(v);
+    dz_rot_deg<L, true>(v, cax, sax);
+    BDeg<L, !IS_M2M>::apply(v);
+#pragma unroll
+    for (int m = -L; m <= L; ++m) xr[shi(L, m)] = v[shi(L, m)];
+  });
+  __syncthreads();
+  float dk[P + 1];
+  dk[0] = 1.f;
+#pragma unroll
+  for (int k = 1; k <= P; ++k) dk[k] = dk[k - 1] * d * (float)(1.0 / (double)k);
+  ForDeg<P, MASK>::run([&](auto lc) {
+    constexpr int n = decltype(lc)::value;
+#pragma unroll
+    for (int m = -n; m <= n; ++m) {
+      float acc = v[shi(n, m)];
+      if (IS_M2M) {
+#pragma unroll
+        for (int k = 1; k <= n - iabs(m); ++k) acc = fmaf(dk[k], xr[shi(n - k, m)], acc);
+      } else {
+#pragma unroll
+        for (int k = 1; k <= P - n; ++k) acc = fmaf(dk[k], xr[shi(n + k, m)], acc);
+      }
+      v[shi(n, m)] = acc;
+    }
+    BDeg<n, !IS_M2M>::apply(v);
+    dz_rot_deg<n, false>(v, cax, sax);
+    BDeg<n, !IS_M2M>::apply(v);
+    dz_rot_deg<n, true>(v, caz, saz);
+  });
+}
+
+// Item i of the level: parent first + i/2, child side i&1 (as the
+// single-thread kernels).  Inactive items still reach the block barrier.
+template <int P, unsigned MASK>
+__device__ __forceinline__ void m2m_split_warp(int first, int last, const int* __restrict__ left,
+                                               const int* __restrict__ right, const int2* __restrict__ ranges,
+                                               float4* __restrict__ centers, float* __restrict__ mult, float* xr,
+                                               bool write_center) {
+  constexpr int C = csize(P), CS = cstride(P);
+  const int lane = threadIdx.x & 31;
+  const int i = first + (int)(blockIdx.x * kSplitItems + lane) / 2;
+  const bool ok = i < last;
+  const int side = lane & 1;
+  float v[C];
+  float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 cc = c;
+  if (ok) {
+    const int a = left[i], b = right[i];
+    const float4 ca = centers[a], cb = centers[b];
+    const float m = ca.w + cb.w;
+    if (m > 0.f) {
+      const float inv = 1.f / m;
+      c = make_float4((ca.w * ca.x + cb.w * cb.x) * inv, (ca.w * ca.y + cb.w * cb.y) * inv,
+                      (ca.w * ca.z + cb.w * cb.z) * inv, m);
+    } else {
+      const int2 ra = ranges[a], rb = ranges[b];
+      const float na = (float)(ra.y - ra.x + 1), nb = (float)(rb.y - rb.x + 1);
+      const float inv = 1.f / (na + nb);
+      c = make_float4((na * ca.x + nb * cb.x) * inv, (na * ca.y + nb * cb.y) * inv, (na * ca.z + nb * cb.z) * inv,
+                      0.f);
+    }
+    cc = side ? cb : ca;
+    const float* src = mult + (size_t)(side ? b : a) * CS;
+    ForDeg<P, MASK>::run([&](auto lc) {
+      constexpr int L = decltype(lc)::value;
+#pragma unroll
+      for (int m = -L; m <= L; ++m) v[shi(L, m)] = src[shi(L, m)];
+    });
+  } else {
+    ForDeg<P, MASK>::run([&](auto lc) {
+      constexpr int L = decltype(lc)::value;
+#pragma unroll
+      for (int m = -L; m <= L; ++m) v[shi(L, m)] = 0.f;
+    });
+  }
+  split_translate<P, MASK, true>(v, cc.x - c.x, cc.y - c.y, cc.z - c.z, xr);
+  ForDeg<P, MASK>::run([&](auto lc) {
+    constexpr int L = decltype(lc)::value;
+#pragma unroll
+    for (int m = -L; m <= L; ++m) v[shi(L, m)] += __shfl_xor_sync(0xffffffffu, v[shi(L, m)], 1);
+  });
+  if (ok && side == 0) {
+    float* dst = mult + (size_t)i * CS;
+    ForDeg<P, MASK>::run([&](auto lc) {
+      constexpr int L = decltype(lc)::value;
+#pragma unroll
+      for (int m = -L; m <= L; ++m) dst[shi(L, m)] = v[shi(L, m)];
+    });
+    if (write_center) {
+      centers[i] = c;
+#pragma unroll
+      for (int k = C; k < CS; ++k) dst[k] = 0.f;
+    }
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) k_m2m_level_split(int first, int last, const int* __restrict__ left,
+                                                         const int* __restrict__ right, const int2* __restrict__ ranges,
+                                                         float4* __restrict__ centers, float* __restrict__ mult) {
+  __shared__ float xs[kSplitItems * xrow(P)];
+  float* xr = xs + (threadIdx.x & 31) * xrow(P);
+  switch (threadIdx.x >> 5) {
+    case 0: m2m_split_warp<P, kDegSet(P, 0)>(first, last, left, right, ranges, centers, mult, xr, true); break;
+    case 1: m2m_split_warp<P, kDegSet(P, 1)>(first, last, left, right, ranges, centers, mult, xr, false); break;
+    case 2: m2m_split_warp<P, kDegSet(P, 2)>(first, last, left, right, ranges, centers, mult, xr, false); break;
+    default: m2m_split_warp<P, kDegSet(P, 3)>(first, last, left, right, ranges, centers, mult, xr, false); break;
+  }
+}
+
+template <int P, unsigned MASK>
+__device__ __forceinline__ void l2l_split_warp(int first, int last, const int* __restrict__ left,
+                                               const int* __restrict__ right, const float4* __restrict__ centers,
+                                               float* __restrict__ locals, float* xr) {
+  constexpr int C = csize(P), CS = cstride(P);
+  const int lane = threadIdx.x & 31;
+  const int i = first + (int)(blockIdx.x * kSplitItems + lane) / 2;
+  const bool ok = i < last;
+  float v[C];
+  int ch = 0;
+  float4 cp = make_float4(0.f, 0.f, 0.f, 0.f), cc = cp;
+  if (ok) {
+    ch = (lane & 1) ? right[i] : left[i];
+    cp = centers[i];
+    cc = centers[ch];
+    const float* src = locals + (size_t)i * CS;
+    ForDeg<P, MASK>::run([&](auto lc) {
+      constexpr int L = decltype(lc)::value;
+#pragma unroll
+      for (int m = -L; m <= L; ++m) v[shi(L, m)] = src[shi(L, m)];
+    });
+  } else {
+    ForDeg<P, MASK>::run([&](auto lc) {
+      constexpr int L = decltype(lc)::value;
+#pragma unroll
+      for (int m = -L; m <= L; ++m) v[shi(L, m)] = 0.f;
+    });
+  }
+  split_translate<P, MASK, false>(v, cp.x - cc.x, cp.y - cc.y, cp.z - cc.z, xr);
+  if (ok) {
+    float* dst = locals + (size_t)ch * CS;
+    ForDeg<P, MASK>::run([&](auto lc) {
+      constexpr int L = decltype(lc)::value;
+#pragma unroll
+      for (int m = -L; m <= L; ++m) dst[shi(L, m)] += v[shi(L, m)];
+    });
+  }
+  (void)C;
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) k_l2l_level_split(int first, int last, const int* __restrict__ left,
+                                                         const int* __restrict__ right,
+                                                         const float4* __restrict__ centers,
+                                                         float* __restrict__ locals) {
+  __shared__ float xs[kSplitItems * xrow(P)];
+  float* xr = xs + (threadIdx.x & 31) * xrow(P);
+  switch (threadIdx.x >> 5) {
+    case 0: l2l_split_warp<P, kDegSet(P, 0)>(first, last, left, right, centers, locals, xr); break;
+    case 1: l2l_split_warp<P, kDegSet(P, 1)>(first, last, left, right, centers, locals, xr); break;
+    case 2: l2l_split_warp<P, kDegSet(P, 2)>(first, last, left, right, centers, locals, xr); break;
+    default: l2l_split_warp<P, kDegSet(P, 3)>(first, last, left, right, centers, locals, xr); break;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -661,8 +904,13 @@ struct RunM2M {
   static int run(int first, int last, const int* left, const int* right, const int* ranges, float* centers,
                  float* mult, cudaStream_t st) {
     if (last <= first) return JB_OK;
-    k_m2m_level<P><<<blocks_for(2 * (int64_t)(last - first), 128), 128, 0, st>>>(first, last, left, right, reinterpret_cast<const int2*>(ranges),
-                                                                   reinterpret_cast<float4*>(centers), mult);
+    if (last - first <= g_split_max_parents[0]) {
+      k_m2m_level_split<P><<<blocks_for(2 * (int64_t)(last - first), kSplitItems), 128, 0, st>>>(
+          first, last, left, right, reinterpret_cast<const int2*>(ranges), reinterpret_cast<float4*>(centers), mult);
+    } else {
+      k_m2m_level<P><<<blocks_for(2 * (int64_t)(last - first), 128), 128, 0, st>>>(
+          first, last, left, right, reinterpret_cast<const int2*>(ranges), reinterpret_cast<float4*>(centers), mult);
+    }
     return launch_status();
   }
 };
@@ -697,8 +945,13 @@ struct RunL2L {
   static int run(int first, int last, const int* left, const int* right, const float* centers, float* locals,
                  cudaStream_t st) {
     if (last <= first) return JB_OK;
-    k_l2l_level<P><<<blocks_for(2 * (int64_t)(last - first), 128), 128, 0, st>>>(
-        first, last, left, right, reinterpret_cast<const float4*>(centers), locals);
+    if (last - first <= g_split_max_parents[1]) {
+      k_l2l_level_split<P><<<blocks_for(2 * (int64_t)(last - first), kSplitItems), 128, 0, st>>>(
+          first, last, left, right, reinterpret_cast<const float4*>(centers), locals);
+    } else {
+      k_l2l_level<P><<<blocks_for(2 * (int64_t)(last - first), 128), 128, 0, st>>>(
+          first, last, left, right, reinterpret_cast<const float4*>(centers), locals);
+    }
     return launch_status();
   }
 };
