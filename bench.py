@@ -362,7 +362,16 @@ def main() -> None:
         passes["chosen"].load_particles(d_pos, d_mass)
         torch.cuda.synchronize()
         g0 = time.perf_counter()
-        gsel = gear_mod.apply_gears(passes["chosen"], model)
+        if world > 1:
+            # the selector reads the force scale of every node, so it runs on a
+            # whole-tree pass; the rank's pass keeps the units of its targets
+            full = engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, **forms["chosen"])
+            full.load_particles(d_pos, d_mass)
+            gsel = gear_mod.apply_gears(full, model)
+            passes["chosen"].set_gears(gsel, model.orders)
+            del full
+        else:
+            gsel = gear_mod.apply_gears(passes["chosen"], model)
         torch.cuda.synchronize()
         gear_info = {"select_s": time.perf_counter() - g0, "budget": model.budget,
                      "fraction": (np.bincount(gsel, minlength=len(model.orders)) / max(1, gsel.size)).tolist(),
@@ -440,10 +449,17 @@ def main() -> None:
     _lib.check(_lib.lib().jb_direct_f64(n, ps0.ws.pos4.data_ptr(), tg.size, ts.data_ptr(), 1.0, 0.0,
                                         ref.data_ptr(), stream.cuda_stream), "jb_direct_f64")
     errs = {}
+    ts_long = ts.long()
     for name, ps in passes.items():
         step(ps)
         torch.cuda.synchronize()
-        got = acc_out[torch.from_numpy(tg).to(dev)].double().cpu().numpy()
+        if world > 1:  # every rank's sorted slice, reassembled (one all_gather)
+            from jaccpot_b200 import sharding
+            b, e = sharding.particle_range(topo, leaf_lo, leaf_hi)
+            full_acc = sharding.gather_sorted(ps.ws.acc4[b:e].contiguous(), topo)
+        else:
+            full_acc = ps.ws.acc4
+        got = full_acc[ts_long, :3].double().cpu().numpy()
         e = workloads.relative_errors(got, ref[:, :3].cpu().numpy())
         errs[name] = {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
                       "p99_first_4096": float(np.percentile(e[:4096], 99))}

@@ -106,6 +106,33 @@ def _on_gpu(dt) -> bool:
     return torch.device(dt.device).type == "cuda"
 
 
+def _restrict_gears(gs, targets, num_nodes: int, dev):
+    """The gear schedule's units and split entries of the given target nodes
+    only (a leaf range's M2L), the per-gear unit ranges recounted.  Units keep
+    their order and slots, so every kept target gets exactly the rows it has
+    in the full schedule."""
+    from .schedule import GearM2LSchedule
+
+    units = torch.as_tensor(gs.units).to(dev)
+    split = torch.as_tensor(gs.split).to(dev)
+    offs = torch.as_tensor(np.asarray(gs.gear_offsets, dtype=np.int64)).to(dev)
+    keep = torch.zeros(num_nodes, dtype=torch.bool, device=dev)
+    keep[torch.as_tensor(np.asarray(targets, dtype=np.int64)).to(dev)] = True
+    ng = int(offs.numel()) - 1
+    if units.shape[0]:
+        gear_of = torch.bucketize(torch.arange(units.shape[0], device=dev), offs[1:], right=True)
+        mask = keep[units[:, 0].long()]
+        units = units[mask].contiguous()
+        counts = torch.bincount(gear_of[mask], minlength=ng)
+    else:
+        counts = torch.zeros(ng, dtype=torch.int64, device=dev)
+    new_offs = torch.zeros(ng + 1, dtype=torch.int64)
+    new_offs[1:] = torch.cumsum(counts.cpu(), 0)
+    if split.shape[0]:
+        split = split[keep[split[:, 0].long()]].contiguous()
+    return GearM2LSchedule(units, split, gs.num_slots, gs.far_src, new_offs.numpy(), gs.orders, gs.pairs_per_gear)
+
+
 class Pass:
     """One evaluation pass over a resident topology; every method enqueues
     kernels on `stream` (default: torch's current stream) and returns."""
@@ -140,6 +167,7 @@ class Pass:
             hi = int(t.node_ranges[t.num_internal + self.leaf_range[1] - 1, 1])
             tg = t.m2l_targets
             targets = tg[(t.node_ranges[tg, 1] >= lo) & (t.node_ranges[tg, 0] <= hi)]
+        self._range_targets = targets
         # work-unit schedules: built on the GPU from the resident lists when
         # the pass runs there (the host builders give the same arrays)
         if _on_gpu(dt):
@@ -209,6 +237,8 @@ class Pass:
             gs = gear_m2l_schedule_device(self.dt, gears, orders)
         else:
             gs = gear_m2l_schedule(self.dt.topo, np.asarray(gears), orders)
+        if getattr(self, "_range_targets", None) is not None:
+            gs = _restrict_gears(gs, self._range_targets, self.dt.topo.num_nodes, self.dt.device)
         dev = self.dt.device
         up = lambda a: _up(a, dev)
         self.gear_sched = gs
