@@ -56,7 +56,9 @@ enum {
 enum {
   JB_P2P_FP32 = 0,
   JB_P2P_KAHAN = 1,     /* compensated per-target sums */
-  JB_P2P_POTENTIAL = 2  /* also accumulate the potential (else out.w holds only the far part) */
+  JB_P2P_POTENTIAL = 2, /* also accumulate the potential (else out.w holds only the far part) */
+  JB_P2P_FAR_ONLY = 4,  /* jb_leaf_eval: the far field (L2P) alone, no P2P */
+  JB_P2P_NEAR_ONLY = 8  /* jb_leaf_eval: the near field (P2P) alone, no L2P */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -153,6 +155,11 @@ JB_API int jb_leaf_schedule_device(int num_internal, int num_leaves, const int* 
 /* gears: int32 per far pair in [0, num_gears) (JB_ERR_INDEX otherwise). */
 JB_API int jb_gear_schedule_device(int num_nodes, const int64_t* far_off, const int* far_src, const int* gears,
                                    int num_gears, int max_pairs, void* stream, jb_dsched** out);
+/* rev[e] = index of the reverse pair (s <- t) of every far pair e = (t <- s)
+ * of a symmetric CSR far list (device arrays; rows sorted, as jb_tree_build
+ * emits them); JB_ERR_INDEX when some pair has no reverse.  The host twin is
+ * Topology.far_reverse_index in tree.py.  Synchronises the stream.           */
+JB_API int jb_far_reverse_index(int num_nodes, const int64_t* far_off, const int* far_src, int* rev, void* stream);
 JB_API int jb_dsched_info(const jb_dsched* d, jb_sched_info_t* info);
 JB_API const void* jb_dsched_field(const jb_dsched* d, int field);
 JB_API void jb_dsched_free(jb_dsched* d);

@@ -26,7 +26,7 @@ ERRORS = {
 }
 JB_MAX_ORDER = 10
 JB_M2L_FP32, JB_M2L_SPLIT_BF16 = 0, 1
-JB_P2P_FP32, JB_P2P_KAHAN, JB_P2P_POTENTIAL = 0, 1, 2
+JB_P2P_FP32, JB_P2P_KAHAN, JB_P2P_POTENTIAL, JB_P2P_FAR_ONLY, JB_P2P_NEAR_ONLY = 0, 1, 2, 4, 8
 JB_LEAF_EVAL_NOALLOC_MAX_SLOTS = 32768
 (JB_SCHED_UNITS, JB_SCHED_AUX, JB_SCHED_RUNS, JB_SCHED_SPLIT, JB_SCHED_FAR_SOURCES, JB_SCHED_GEAR_OFFSETS,
  JB_SCHED_TARGETS, JB_SCHED_PAIRS_PER_GEAR) = range(8)
@@ -86,6 +86,7 @@ _SIGNATURES = {
     "jb_dtree_copy": [_P, _I, _P],
     "jb_dtree_free": [_P],
     "jb_set_level_split": [_I, _I],
+    "jb_far_reverse_index": [_I, _P, _P, _P, _P],
     "jb_m2l_schedule_device": [_I, _P, _I, _I, _P, _P, ctypes.POINTER(_P)],
     "jb_leaf_schedule_device": [_I, _I, _P, _P, _P, _I, _I, _I, _P, ctypes.POINTER(_P)],
     "jb_gear_schedule_device": [_I, _P, _P, _P, _I, _I, _P, ctypes.POINTER(_P)],

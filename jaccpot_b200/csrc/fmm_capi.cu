@@ -406,7 +406,8 @@ JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal
       (num_units > 0 && (!pos4 || !units || !aux || !runs || !node_ranges || !centers || !locals || !out_acc4)) ||
       (num_split > 0 && (!split || !partials || !out_acc4 || !node_ranges)))
     return JB_ERR_ARG;
-  if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL)) return JB_ERR_ARG;
+  if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL | JB_P2P_FAR_ONLY | JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
+  if ((p2p_mode & JB_P2P_FAR_ONLY) && (p2p_mode & JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
   return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, num_units, units, aux, runs, node_ranges, centers,
                                locals, G, eps2, out_acc4, partials, num_split, split, ST(stream));
 }

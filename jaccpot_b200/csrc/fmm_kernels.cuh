@@ -781,11 +781,12 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
 // out = -G (grad phi, phi); runs before k_leaf_units, which adds the near
 // field.  Kept out of the near-field kernel so that kernel's register count
 // is set by the P2P loop alone (about half, and twice the resident warps).
+// zero: write zeros instead (the near field alone, JB_P2P_NEAR_ONLY).
 template <int P>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
     const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
     const int2* __restrict__ aux, const int2* __restrict__ ranges, const float4* __restrict__ centers,
-    const float* __restrict__ locals, float G, float4* __restrict__ out) {
+    const float* __restrict__ locals, float G, float4* __restrict__ out, bool zero) {
   constexpr int C = csize(P), CS = cstride(P);
   __shared__ float sF[kWarpsPerBlock][CS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -796,6 +797,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
   for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
   __syncwarp();
   if (rg.x + lane > rg.y) return;
+  if (zero) {  // near field alone: the sums start from zero
+    out[rg.x + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
   const float4 c = centers[node], ti = pos4[rg.x + lane];
   float U_[C];
   solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
@@ -977,10 +982,13 @@ struct RunLeafEval {
       auto a4 = reinterpret_cast<const int2*>(ranges);
       auto o = reinterpret_cast<float4*>(out);
       auto pt = reinterpret_cast<float4*>(partial);
+      const bool far_only = (mode & JB_P2P_FAR_ONLY) != 0, near_only = (mode & JB_P2P_NEAR_ONLY) != 0;
       k_leaf_l2p<P><<<nb, 32 * kWarpsPerBlock, 0, st>>>(a0, num_internal, num_units, a1, a2, a4,
-                                                        reinterpret_cast<const float4*>(centers), locals, G, o);
+                                                        reinterpret_cast<const float4*>(centers), locals, G, o,
+                                                        near_only);
       int rc = launch_status();
       if (rc) return rc;
+      if (far_only) return JB_OK;
       const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
       if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
       else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);

@@ -680,6 +680,32 @@ void build_gears(jb_dsched& d, int num_nodes, const int64_t* far_off, const int*
   ck(cudaStreamSynchronize(st));
 }
 
+// ---------------------------------------------------------------------------
+// Reverse index of a symmetric far list: rev[e] for the pair e = (t <- s) is
+// the entry (s <- t), found by binary search in row s (rows are sorted).
+// Thread per row; a missing reverse is counted in *bad.
+// ---------------------------------------------------------------------------
+__global__ void k_far_reverse(const int64_t* __restrict__ off, int num_nodes, const int* __restrict__ src,
+                              int* __restrict__ rev, int* __restrict__ bad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= num_nodes) return;
+  for (int64_t e = off[t]; e < off[t + 1]; ++e) {
+    const int s = src[e];
+    int64_t lo = off[s], hi = off[s + 1];
+    while (lo < hi) {
+      const int64_t mid = lo + (hi - lo) / 2;
+      if (src[mid] < t) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < off[s + 1] && src[lo] == t) {
+      rev[e] = (int)lo;
+    } else {
+      rev[e] = -1;
+      atomicAdd(bad, 1);
+    }
+  }
+}
+
 const DBuf* sched_field(const jb_dsched* d, int field) {
   switch (field) {
     case JB_SCHED_UNITS: return &d->units;
@@ -747,6 +773,25 @@ JB_API int jb_gear_schedule_device(int num_nodes, const int64_t* far_off, const 
   return run_builder(out, st, [&](jb_dsched& d) {
     build_gears(d, num_nodes, far_off, far_src, gears, num_gears, max_pairs, st);
   });
+}
+
+JB_API int jb_far_reverse_index(int num_nodes, const int64_t* far_off, const int* far_src, int* rev, void* stream) {
+  if (num_nodes < 0 || !far_off || !far_src || !rev) return JB_ERR_ARG;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  tl_stream = st;
+  try {
+    DBuf bad;
+    ck(bad.alloc(4));
+    ck(cudaMemsetAsync(bad.p, 0, 4, st));
+    if (num_nodes > 0) {
+      k_far_reverse<<<nblocks(num_nodes, 128), 128, 0, st>>>(far_off, num_nodes, far_src, rev, bad.as<int>());
+      ck_launch();
+    }
+    if (read_word(bad.as<int>(), st) != 0) return JB_ERR_INDEX;
+  } catch (const Fail& f) {
+    return f.rc;
+  }
+  return JB_OK;
 }
 
 JB_API int jb_dsched_info(const jb_dsched* d, jb_sched_info_t* info) {

@@ -55,6 +55,21 @@ class DeviceTopology:
         self.num_m2l_targets = int(topo.m2l_targets.size)
         self.level_offsets = [int(x) for x in topo.level_offsets]
 
+    def far_reverse_index(self) -> torch.Tensor:
+        """int32[num_far] on the device: the reverse pair (s <- t) of every far
+        pair (t <- s) (jb_far_reverse_index; computed once)."""
+        rev = getattr(self, "_far_rev", None)
+        if rev is None:
+            n = self.topo.num_far_pairs
+            rev = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+            _lib.check(_lib.lib().jb_far_reverse_index(self.topo.num_nodes, self.far_off.data_ptr(),
+                                                       self.far_src.data_ptr(), rev.data_ptr(),
+                                                       torch.cuda.current_stream(self.device).cuda_stream),
+                       "jb_far_reverse_index")
+            rev = rev[:n]
+            self._far_rev = rev
+        return rev
+
     def validate(self) -> None:
         """Device-side range check of every list entry (jb_validate_lists)."""
         t = self.topo
@@ -317,9 +332,13 @@ class Pass:
             _lib.check(self.lib.jb_l2l_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
                                              _ptr(ws.centers), _ptr(ws.locals), s), "jb_l2l_level")
 
-    def evaluate(self, stream=None, potential: bool = False) -> torch.Tensor:
+    def evaluate(self, stream=None, potential: bool = False, part: str | None = None) -> torch.Tensor:
+        """L2P + P2P into ws.acc4 (sorted order); part="near" / "far" keeps
+        only the P2P / only the L2P contribution."""
         t, dt, ws, sc = self.dt.topo, self.dt, self.ws, self.leaf_sched
         mode = self.p2p_mode | (_lib.JB_P2P_POTENTIAL if potential else 0)
+        if part is not None:
+            mode |= {"near": _lib.JB_P2P_NEAR_ONLY, "far": _lib.JB_P2P_FAR_ONLY}[part]
         _lib.check(self.lib.jb_leaf_eval(self.p, mode, _ptr(ws.pos4), t.num_internal, int(sc.units.shape[0]),
                                          _ptr(self.d_leaf_units), _ptr(self.d_leaf_aux), _ptr(self.d_leaf_runs),
                                          _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.locals), self.G,

@@ -122,9 +122,13 @@ class GearContext:
         return gear[:n]
 
 
-def apply_gears(ps: engine.Pass, model: GearModel) -> np.ndarray:
+def apply_gears(ps: engine.Pass, model: GearModel, symmetric: bool = False) -> np.ndarray:
     """Runs the plain pass on the loaded particles (force scale), selects the
-    gears with the network and installs them on ``ps``; returns them."""
+    gears with the network and installs them on ``ps``; returns them.
+
+    symmetric: each pair and its reverse get the higher of their two gears, so
+    the far-field forces between two nodes stay equal and opposite and the
+    pass conserves momentum to round-off (jaccpot_b200.mutual)."""
     if ps.p != max(model.orders):
         raise ValueError(f"the selector's top gear is {max(model.orders)}, the pass order is {ps.p}")
     ps.set_gears(None, None)
@@ -132,6 +136,8 @@ def apply_gears(ps: engine.Pass, model: GearModel) -> np.ndarray:
     ctx = GearContext(ps)
     ctx.node_features()
     gears = ctx.select(model)
+    if symmetric and gears.numel():
+        gears = torch.maximum(gears, gears[ps.dt.far_reverse_index().long()])
     ps.set_gears(gears, model.orders)
     return gears.cpu().numpy()
 
