@@ -389,7 +389,8 @@ class Pass:
                 "cbar4": torch.empty((t.num_nodes, 4), **f32),
                 "g4": torch.empty((max(t.num_far_pairs, 1), 4), **f32),
                 "pair_tgt": torch.from_numpy(t.far_pair_targets() if t.num_far_pairs else np.zeros(1, np.int32)).to(dev),
-                "rev": torch.from_numpy(t.far_reverse_index() if t.num_far_pairs else np.zeros(1, np.int32)).to(dev),
+                "rev": (self.dt.far_reverse_index() if _on_gpu(self.dt) and t.num_far_pairs else
+                        torch.from_numpy(t.far_reverse_index() if t.num_far_pairs else np.zeros(1, np.int32)).to(dev)),
             }
             if not t.near_lists_symmetric():
                 raise ValueError("the near-field adjoint needs symmetric neighbour lists")
