@@ -232,6 +232,13 @@ JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float*
  * far_src is the source list regrouped so no unit mixes gears.  Rows of
  * mult / locals / partials have stride jb_coeff_stride(p_max); a gear reads
  * the degrees <= its order and writes zeros above them. */
+/* jb_m2l with far pair e's contribution scaled by far_w[e] (device float per
+ * CSR far entry): the block-step weighted far field of the mutual lane
+ * (jaccpot/mutual/force.py:920 _far_pair_weights there: a pair's weight is
+ * that of its finer node's level, the same for both directions). FP32.    */
+JB_API int jb_m2l_weighted(int p, int num_units, const int* units, const float* mult, const float* centers,
+                           const int* far_src, const float* far_w, float* locals, float* partials, int num_split,
+                           const int* split, void* stream);
 JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orders, const int64_t* gear_unit_offsets,
                         const int* units, const float* mult, const float* centers, const int* far_src,
                         float* locals, float* partials, int num_split, const int* split, void* stream);
@@ -282,6 +289,17 @@ JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* 
  * float4 at partials[32*slot] (scratch), then split int4[num_split] = (leaf,
  * first slot, slot count, 0) is summed into out_acc4.  out_acc4[i] = (ax, ay,
  * az, potential) in sorted order; p2p_mode is a JB_P2P_* flag set. */
+/* jb_leaf_eval with every particle pair scaled by
+ * level_weights[max(rung_i, rung_j)] (rung: int32 per SORTED particle,
+ * clamped to [0, num_level_weights); num_level_weights <= 32; device
+ * arrays): the block-step weighted near field of the mutual lane
+ * (jaccpot/mutual/nearfield.py:140 _pair_weights there).  The far part is
+ * whatever the locals hold (weighted by jb_m2l_weighted).                  */
+JB_API int jb_leaf_eval_weighted(int p, int p2p_mode, const float* pos4, const int* rung, int num_level_weights,
+                                 const float* level_weights, int num_internal, int num_units, const int* units,
+                                 const int* aux, const int* runs, const int* node_ranges, const float* centers,
+                                 const float* locals, float G, float eps2, float* out_acc4, float* partials,
+                                 int num_split, const int* split, void* stream);
 JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_units, const int* units,
                         const int* aux, const int* runs, const int* node_ranges, const float* centers,
                         const float* locals, float G, float eps2, float* out_acc4, float* partials, int num_split,

@@ -366,6 +366,17 @@ JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float*
                           ST(stream));
 }
 
+JB_API int jb_m2l_weighted(int p, int num_units, const int* units, const float* mult, const float* centers,
+                           const int* far_src, const float* far_w, float* locals, float* partials, int num_split,
+                           const int* split, void* stream) {
+  if (num_units < 0 || num_split < 0 ||
+      (num_units > 0 && (!units || !mult || !centers || !far_src || !far_w || !locals)) ||
+      (num_split > 0 && (!split || !partials || !locals)))
+    return JB_ERR_ARG;
+  return dispatch<RunM2L>(p, num_units, units, mult, centers, far_src, locals, partials, num_split, split,
+                          ST(stream), false, 0, far_w);
+}
+
 JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orders, const int64_t* gear_unit_offsets,
                         const int* units, const float* mult, const float* centers, const int* far_src,
                         float* locals, float* partials, int num_split, const int* split, void* stream) {
@@ -396,6 +407,23 @@ JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* 
                         float* locals, void* stream) {
   if (first < 0 || last < first || (last > first && (!left || !right || !centers || !locals))) return JB_ERR_ARG;
   return dispatch<RunL2L>(p, first, last, left, right, centers, locals, ST(stream));
+}
+
+JB_API int jb_leaf_eval_weighted(int p, int p2p_mode, const float* pos4, const int* rung, int num_level_weights,
+                                 const float* level_weights, int num_internal, int num_units, const int* units,
+                                 const int* aux, const int* runs, const int* node_ranges, const float* centers,
+                                 const float* locals, float G, float eps2, float* out_acc4, float* partials,
+                                 int num_split, const int* split, void* stream) {
+  if (num_units < 0 || num_split < 0 || num_internal < 0 || !rung || !level_weights || num_level_weights < 1 ||
+      num_level_weights > 32 ||
+      (num_units > 0 && (!pos4 || !units || !aux || !runs || !node_ranges || !centers || !locals || !out_acc4)) ||
+      (num_split > 0 && (!split || !partials || !out_acc4 || !node_ranges)))
+    return JB_ERR_ARG;
+  if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL | JB_P2P_FAR_ONLY | JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
+  if ((p2p_mode & JB_P2P_FAR_ONLY) && (p2p_mode & JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
+  return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, num_units, units, aux, runs, node_ranges, centers,
+                               locals, G, eps2, out_acc4, partials, num_split, split, ST(stream), rung,
+                               level_weights, num_level_weights);
 }
 
 JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_units, const int* units,

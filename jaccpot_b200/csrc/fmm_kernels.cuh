@@ -205,13 +205,17 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the reverse pair), which is what the adjoint's transposed M2L needs: the
 // real M2L matrix is symmetric, so sum_v M2L(c_v - c_u)^T Lbar_v is this
 // kernel run over u's own list with Lbar in place of the multipoles.
-template <int P, bool NEG>
+//
+// W: pair e's contribution is scaled by far_w[e] (the block-step level weight
+// of the mutual lane); the unweighted instantiations do not read it.
+template <int P, bool NEG, bool W = false>
 __global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units(int num_units, const int4* __restrict__ units,
                                                               const float* __restrict__ mult,
                                                               const float4* __restrict__ centers,
                                                               const int* __restrict__ far_src,
                                                               float* __restrict__ locals,
-                                                              float* __restrict__ partials, int rs) {
+                                                              float* __restrict__ partials, int rs,
+                                                              const float* __restrict__ far_w = nullptr) {
   // rs: row stride (floats) of mult / locals / partials, >= cstride(P); a
   // lower-order pass (gear) reads the prefix of each row (degrees <= P).
   constexpr int C = csize(P), CS = cstride(P), R4 = row4(P);
@@ -258,8 +262,14 @@ __global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units(int num_units, con
     const int s2 = (e + 2 < e1) ? __ldg(far_src + e + 2) : s1;
     if (NEG) m2l_kfold<P>(v, cs.x - ct.x, cs.y - ct.y, cs.z - ct.z);
     else m2l_kfold<P>(v, ct.x - cs.x, ct.y - cs.y, ct.z - cs.z);
+    if (W) {
+      const float wt = __ldg(far_w + e);
 #pragma unroll
-    for (int k = 0; k < C; ++k) acc[k] += v[k];
+      for (int k = 0; k < C; ++k) acc[k] = fmaf(wt, v[k], acc[k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < C; ++k) acc[k] += v[k];
+    }
     cs = cs1;
     cs1 = centers[s2];
     s1 = s2;
@@ -628,6 +638,7 @@ __device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
 // 16-byte vector that splits into two packed pairs with no register moves.
 struct alignas(16) NearStage {
   float x[32], y[32], z[32], m[32];
+  int r[32];  // block-step rung of each staged source (weighted form only)
 };
 
 template <int G>
@@ -639,12 +650,25 @@ __device__ __forceinline__ void stage_source(NearStage& s, int j, float4 v) {
   s.m[k] = v.w;
 }
 
+template <int G>
+__device__ __forceinline__ void stage_rung(NearStage& s, int j, int r) {
+  s.r[(j % G) * (32 / G) + j / G] = r;
+}
+
+// Level weights of the mutual lane's block-step form: a particle pair belongs
+// to the level of its finer endpoint, max(rung_i, rung_j), and is scaled by
+// that level's weight (rungs clamped to the table when staged).
+struct PairWeights {
+  const float* tbl;  // shared memory, one weight per level
+  int rt;            // this lane's target rung
+};
+
 // One chunk of 32 staged sources for this lane's target: the lane's 32/G
 // sources (j = q*G + h), two per packed step; the two partial sums are added
 // at the end of the chunk (and into the compensated accumulator when KAHAN).
-template <int G, bool KAHAN, bool POT, bool SELF>
+template <int G, bool KAHAN, bool POT, bool SELF, bool W = false>
 __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h, int self_j, float eps2,
-                                           NearAcc<KAHAN>& a) {
+                                           NearAcc<KAHAN>& a, PairWeights pw = PairWeights{nullptr, 0}) {
   constexpr int R = 32 / G;
   const ulonglong2* X = reinterpret_cast<const ulonglong2*>(st.x + h * R);
   const ulonglong2* Y = reinterpret_cast<const ulonglong2*>(st.y + h * R);
@@ -662,6 +686,12 @@ __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h
     const f32x2 ir = f2(rsqrtf(d2a), rsqrtf(d2b));
     f32x2 mir = f2_mul(sm, ir);
     f32x2 w = f2_mul(mir, f2_mul(ir, ir));
+    if (W) {
+      const int k0 = h * R + q;
+      const f32x2 lw = f2(pw.tbl[max(pw.rt, st.r[k0])], pw.tbl[max(pw.rt, st.r[k0 + 1])]);
+      mir = f2_mul(mir, lw);
+      w = f2_mul(w, lw);
+    }
     if (SELF) {
       const int j0 = q * G + h, j1 = j0 + G;
       float m0, m1, w0, w1;
@@ -699,39 +729,52 @@ __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h
   }
 }
 
-template <int G, bool KAHAN, bool POT>
+template <int G, bool KAHAN, bool POT, bool W = false>
 __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
                                           const int2* __restrict__ runs, NearStage& sP, int lane, float G_,
-                                          float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
+                                          float eps2, float4* __restrict__ out, float4* __restrict__ partial,
+                                          const int* __restrict__ rung = nullptr, const float* tbl = nullptr,
+                                          int nlw = 1) {
   const int tl = lane / G, h = lane % G;
   const int nt = rg.y - rg.x + 1;
   const bool active = tl < nt;
   const float4 ti = active ? pos4[rg.x + tl] : make_float4(0.f, 0.f, 0.f, 0.f);
+  auto clamp_rung = [&](int r) { return min(max(r, 0), nlw - 1); };
+  PairWeights pw{tbl, 0};
+  if (W) pw.rt = active ? clamp_rung(rung[rg.x + tl]) : 0;
   NearAcc<KAHAN> a;
   if (aux.y & 1) {
     stage_source<G>(sP, lane, (lane < nt) ? pos4[rg.x + lane] : JB_PAD4);
+    if (W) stage_rung<G>(sP, lane, (lane < nt) ? clamp_rung(rung[rg.x + lane]) : 0);
     __syncwarp();
-    near_chunk<G, KAHAN, POT, true>(sP, ti, h, tl, eps2, a);
+    near_chunk<G, KAHAN, POT, true, W>(sP, ti, h, tl, eps2, a, pw);
     __syncwarp();
   }
   const int nsrc = U.w;
   if (nsrc > 0) {
     int r = U.y, rbase = 0;
     int2 run = runs[r];
-    auto fetch = [&](int f) -> float4 {
+    auto fetch_index = [&](int f) -> int {  // particle of source f, -1 past the end
       while (f >= rbase + run.y && r + 1 < U.z) {
         rbase += run.y;
         ++r;
         run = runs[r];
       }
-      return (f < nsrc) ? pos4[run.x + (f - rbase)] : JB_PAD4;
+      return (f < nsrc) ? run.x + (f - rbase) : -1;
     };
-    float4 qn = fetch(lane);
+    int qi = fetch_index(lane);
+    float4 qn = qi >= 0 ? pos4[qi] : JB_PAD4;
+    int qr = (W && qi >= 0) ? clamp_rung(rung[qi]) : 0;
     for (int base = 0; base < nsrc; base += 32) {
       stage_source<G>(sP, lane, qn);
+      if (W) stage_rung<G>(sP, lane, qr);
       __syncwarp();
-      if (base + 32 < nsrc) qn = fetch(base + 32 + lane);
-      near_chunk<G, KAHAN, POT, false>(sP, ti, h, -1, eps2, a);
+      if (base + 32 < nsrc) {
+        qi = fetch_index(base + 32 + lane);
+        qn = qi >= 0 ? pos4[qi] : JB_PAD4;
+        if (W) qr = qi >= 0 ? clamp_rung(rung[qi]) : 0;
+      }
+      near_chunk<G, KAHAN, POT, false, W>(sP, ti, h, -1, eps2, a, pw);
       __syncwarp();
     }
   }
@@ -755,12 +798,21 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
 
 // Near field (P2P) of the work units, added to the far field already in out
 // (whole leaves) or written to the partial rows (split leaves).
-template <bool KAHAN, bool POT>
+//
+// W: the block-step weighted form of the mutual lane -- every pair scaled by
+// lw[max(rung_i, rung_j)] (rung: per sorted particle, lw: nlw <= 32 weights).
+template <bool KAHAN, bool POT, bool W = false>
 static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_leaf_units(
     const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
     const int2* __restrict__ aux, const int2* __restrict__ runs, const int2* __restrict__ ranges, float G,
-    float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
+    float eps2, float4* __restrict__ out, float4* __restrict__ partial, const int* __restrict__ rung = nullptr,
+    const float* __restrict__ lw = nullptr, int nlw = 1) {
   __shared__ NearStage sP[kWarpsPerBlock];
+  __shared__ float tbl[32];
+  if (W) {
+    if (threadIdx.x < 32) tbl[threadIdx.x] = threadIdx.x < (unsigned)nlw ? lw[threadIdx.x] : 0.f;
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int u = blockIdx.x * kWarpsPerBlock + warp;
   if (u >= num_units) return;
@@ -769,11 +821,11 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
   const int2 rg = ranges[num_internal + U.x];
   const int nt = rg.y - rg.x + 1;
   if (nt <= 8)
-    leaf_unit<4, KAHAN, POT>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial);
+    leaf_unit<4, KAHAN, POT, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
   else if (nt <= 16)
-    leaf_unit<2, KAHAN, POT>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial);
+    leaf_unit<2, KAHAN, POT, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
   else
-    leaf_unit<1, KAHAN, POT>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial);
+    leaf_unit<1, KAHAN, POT, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
 }
 
 // Far field (L2P) of every leaf: warp per leaf (its unit with flags & 1),
@@ -924,15 +976,15 @@ template <int P>
 struct RunM2L {
   static int run(int num_units, const int* units, const float* mult, const float* centers, const int* far_src,
                  float* locals, float* partials, int num_split, const int* split, cudaStream_t st, bool neg = false,
-                 int rs = 0) {
+                 int rs = 0, const float* far_w = nullptr) {
     if (rs <= 0) rs = cstride(P);
     if (num_units > 0) {
       const size_t sm = sizeof(float4) * kM2LThreads * row4(P);
-      auto kern = neg ? k_m2l_units<P, true> : k_m2l_units<P, false>;
+      auto kern = far_w ? k_m2l_units<P, false, true> : (neg ? k_m2l_units<P, true> : k_m2l_units<P, false>);
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
           num_units, reinterpret_cast<const int4*>(units), mult, reinterpret_cast<const float4*>(centers), far_src,
-          locals, partials, rs);
+          locals, partials, rs, far_w);
       const int rc = launch_status();
       if (rc) return rc;
     }
@@ -966,13 +1018,18 @@ struct RunLeafEval {
   template <bool K, bool PT>
   static void go(unsigned nb, cudaStream_t st, const float4* pos4, int num_internal, int num_units, const int4* units,
                  const int2* aux, const int2* runs, const int2* ranges, float G, float eps2, float4* out,
-                 float4* partial) {
-    k_leaf_units<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs, ranges,
-                                                            G, eps2, out, partial);
+                 float4* partial, const int* rung, const float* lw, int nlw) {
+    if (rung)
+      k_leaf_units<K, PT, true><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs,
+                                                                    ranges, G, eps2, out, partial, rung, lw, nlw);
+    else
+      k_leaf_units<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs, ranges,
+                                                              G, eps2, out, partial);
   }
   static int run(int mode, const float* pos4, int num_internal, int num_units, const int* units, const int* aux,
                  const int* runs, const int* ranges, const float* centers, const float* locals, float G, float eps2,
-                 float* out, float* partial, int num_split, const int* split, cudaStream_t st) {
+                 float* out, float* partial, int num_split, const int* split, cudaStream_t st,
+                 const int* rung = nullptr, const float* lw = nullptr, int nlw = 1) {
     if (num_units > 0) {
       const unsigned nb = blocks_for(num_units, kWarpsPerBlock);
       auto a0 = reinterpret_cast<const float4*>(pos4);
@@ -990,10 +1047,10 @@ struct RunLeafEval {
       if (rc) return rc;
       if (far_only) return JB_OK;
       const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
-      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
-      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
-      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
-      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt);
+      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
+      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
+      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
+      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
       rc = launch_status();
       if (rc) return rc;
     }

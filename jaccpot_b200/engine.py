@@ -283,6 +283,38 @@ class Pass:
                                    _ptr(self.m2l_partials), int(sc.split.shape[0]), _ptr(self.d_m2l_split), s),
                    "jb_m2l")
 
+    def m2l_weighted(self, far_w: torch.Tensor, stream=None) -> None:
+        """FP32 M2L at the pass order with far pair e scaled by far_w[e]
+        (float32 per CSR far entry, on the device)."""
+        ws, s, sc = self.ws, _stream_handle(stream), self.m2l_sched
+        w = far_w.to(device=self.dt.device, dtype=torch.float32).contiguous()
+        if w.numel() != self.dt.topo.num_far_pairs:
+            raise ValueError("one weight per far pair is required")
+        ws.locals.zero_()
+        _lib.check(self.lib.jb_m2l_weighted(self.p, int(sc.units.shape[0]), _ptr(self.d_m2l_units), _ptr(ws.mult),
+                                            _ptr(ws.centers), _ptr(self.dt.far_src), _ptr(w) if w.numel() else None,
+                                            _ptr(ws.locals), _ptr(self.m2l_partials), int(sc.split.shape[0]),
+                                            _ptr(self.d_m2l_split), s), "jb_m2l_weighted")
+
+    def evaluate_weighted(self, rung_sorted: torch.Tensor, level_weights: torch.Tensor, stream=None,
+                          part: str | None = None) -> torch.Tensor:
+        """evaluate() with every near pair scaled by
+        level_weights[max(rung_i, rung_j)] (rung per sorted particle)."""
+        t, dt, ws, sc = self.dt.topo, self.dt, self.ws, self.leaf_sched
+        r = rung_sorted.to(device=dt.device, dtype=torch.int32).contiguous()
+        lw = level_weights.to(device=dt.device, dtype=torch.float32).contiguous()
+        mode = self.p2p_mode
+        if part is not None:
+            mode |= {"near": _lib.JB_P2P_NEAR_ONLY, "far": _lib.JB_P2P_FAR_ONLY}[part]
+        _lib.check(self.lib.jb_leaf_eval_weighted(self.p, mode, _ptr(ws.pos4), _ptr(r), int(lw.numel()), _ptr(lw),
+                                                  t.num_internal, int(sc.units.shape[0]), _ptr(self.d_leaf_units),
+                                                  _ptr(self.d_leaf_aux), _ptr(self.d_leaf_runs),
+                                                  _ptr(dt.node_ranges), _ptr(ws.centers), _ptr(ws.locals), self.G,
+                                                  self.eps2, _ptr(ws.acc4), _ptr(self.leaf_partials),
+                                                  int(sc.split.shape[0]), _ptr(self.d_leaf_split),
+                                                  _stream_handle(stream)), "jb_leaf_eval_weighted")
+        return ws.acc4
+
     def _m2l_split(self, s) -> None:
         """Split-BF16 M2L on the tensor cores."""
         if self.tc_layout == "units":

@@ -32,8 +32,10 @@ build_mutual_state(...), mutual_accelerations / mutual_weighted_accelerations
 (with return_parts -> MutualForceResult), mutual_near_field_forces and
 mutual_far_field_forces.  Forces are F = m a of the pass's accelerations; the
 accelerations of massless particles are reported as zero, as the reference's
-force / mass does.  The block-step rung weighting (level_weights, rung) is not
-provided.
+force / mass does.  The block-step form (rung, level_weights;
+mutual_level_accelerations and the boundary-weight helpers) scales each pair
+by its level's weight inside the kernels (jb_m2l_weighted,
+jb_leaf_eval_weighted), the same weight for both directions.
 """
 
 from __future__ import annotations
@@ -167,30 +169,73 @@ def _unsort(sorted_rows: torch.Tensor, perm: torch.Tensor) -> torch.Tensor:
     return out
 
 
+def _node_rungs(dt: DeviceTopology, rung_sorted: torch.Tensor) -> torch.Tensor:
+    """Rung of every node: the finest (largest) rung of its particles, leaves
+    first, then up the levels (force.py:885 _cell_rungs there)."""
+    t = dt.topo
+    node = torch.full((t.num_nodes,), -1, dtype=torch.int32, device=rung_sorted.device)
+    leaf = torch.full((t.num_leaves,), -1, dtype=torch.int32, device=rung_sorted.device)
+    leaf = leaf.scatter_reduce(0, dt.leaf_of.long(), rung_sorted, reduce="amax", include_self=True)
+    node[t.num_internal:] = leaf
+    left, right, lo = dt.left.long(), dt.right.long(), dt.level_offsets
+    for lev in range(t.num_levels - 1, -1, -1):
+        a, b = lo[lev], lo[lev + 1]
+        if b > a:
+            node[a:b] = torch.maximum(node[left[a:b]], node[right[a:b]])
+    return node
+
+
+def _far_pair_weights(dt: DeviceTopology, node_rung: torch.Tensor, lw: torch.Tensor) -> torch.Tensor:
+    """Weight of every directed far entry: lw[max(rung_a, rung_b)], the same
+    for both directions of a pair (force.py:920 there)."""
+    t = dt.topo
+    counts = (dt.far_off[1:] - dt.far_off[:-1]).long()
+    tgt = torch.repeat_interleave(torch.arange(t.num_nodes, device=lw.device), counts)
+    src = dt.far_src[: t.num_far_pairs].long()
+    lev = torch.maximum(node_rung[tgt], node_rung[src]).clamp(0, lw.numel() - 1).long()
+    return lw[lev]
+
+
 def mutual_weighted_accelerations(state: MutualFMMState, positions, masses, *, rung=None, level_weights=None,
                                   return_parts: bool = False):
-    """The full mutual acceleration in the caller's particle order
-    (force.py:985 there); return_parts adds the near and far forces.  Arrays
-    come back as the inputs' kind (numpy in, numpy out)."""
-    if rung is not None or level_weights is not None:
-        raise NotImplementedError("rung-weighted (block-step) evaluation is not provided")
+    """sum_k level_weights[k] * a_k in one traversal (force.py:985 there):
+    a pair belongs to the level of its finer endpoint -- max(rung_i, rung_j)
+    for particles, the nodes' finest rungs for a far pair -- and is scaled by
+    that level's weight, the same for both directions, so momentum stays
+    conserved for any weights.  Without rung / level_weights this is the full
+    acceleration.  return_parts adds the near and far forces.  Arrays come
+    back as the inputs' kind (numpy in, numpy out)."""
+    if (rung is None) != (level_weights is None):
+        raise ValueError("rung and level_weights go together")
     ps = state.pass_
-    dev = state.device_topology.device
+    dt = state.device_topology
+    dev = dt.device
     want_np = not isinstance(positions, torch.Tensor)
     pos = torch.as_tensor(positions).to(device=dev, dtype=torch.float32)
     mass = torch.as_tensor(masses).to(device=dev, dtype=torch.float32)
+    perm = dt.perm
     ps.load_particles(pos, mass)
     ps.upward()
-    ps.m2l()
-    ps.l2l()
-    perm = state.device_topology.perm
+    if rung is None:
+        ps.m2l()
+        ps.l2l()
+        ev = lambda part=None: ps.evaluate(part=part)
+    else:
+        lw = torch.as_tensor(np.asarray(level_weights, dtype=np.float32) if not isinstance(level_weights, torch.Tensor)
+                             else level_weights).to(device=dev, dtype=torch.float32).reshape(-1)
+        if not 1 <= lw.numel() <= 32:
+            raise ValueError("between 1 and 32 level weights")
+        r_sorted = torch.as_tensor(rung).to(device=dev, dtype=torch.int32).reshape(-1)[perm].contiguous()
+        ps.m2l_weighted(_far_pair_weights(dt, _node_rungs(dt, r_sorted), lw))
+        ps.l2l()
+        ev = lambda part=None: ps.evaluate_weighted(r_sorted, lw, part=part)
     m_sorted = mass[perm]
     if return_parts:
-        near_a = ps.evaluate(part="near")[:, :3].clone()
-        far_a = ps.evaluate(part="far")[:, :3].clone()
+        near_a = ev("near")[:, :3].clone()
+        far_a = ev("far")[:, :3].clone()
         acc = near_a + far_a
     else:
-        acc = ps.evaluate()[:, :3].clone()
+        acc = ev()[:, :3].clone()
     acc = torch.where(m_sorted[:, None] > 0, acc, torch.zeros_like(acc))
     out = _unsort(acc, perm)
     if not return_parts:
@@ -205,6 +250,50 @@ def mutual_weighted_accelerations(state: MutualFMMState, positions, masses, *, r
 def mutual_accelerations(state: MutualFMMState, positions, masses, **kwargs):
     """mutual_weighted_accelerations with unit weights (force.py:1071 there)."""
     return mutual_weighted_accelerations(state, positions, masses, **kwargs)
+
+
+def mutual_level_accelerations(state: MutualFMMState, positions, masses, *, rung, level: int, k_max: int):
+    """The accelerations of the level-``level`` interactions alone
+    (force.py:1096 there); summed over levels 0 .. k_max they give the full
+    acceleration."""
+    w = np.zeros(int(k_max) + 1, dtype=np.float32)
+    w[int(level)] = 1.0
+    return mutual_weighted_accelerations(state, positions, masses, rung=rung, level_weights=w)
+
+
+# Block-step bookkeeping (force.py:685-883 there): 2**k_max sub-steps per base
+# step; boundary s kicks the levels at or above its floor.
+def n_sub(k_max: int) -> int:
+    return 1 << int(k_max)
+
+
+def is_sync_boundary(s: int, k_max: int) -> bool:
+    return int(s) == 0 or int(s) == (1 << int(k_max))
+
+
+def active_level_floor(s: int, k_max: int) -> int:
+    s, k_max = int(s), int(k_max)
+    if is_sync_boundary(s, k_max):
+        return 0
+    return k_max - ((s & -s).bit_length() - 1)
+
+
+def level_weights_from_floor(active_floor: int, k_max: int, dt_max: float, *, half: float = 1.0,
+                             dtype=np.float64) -> np.ndarray:
+    """Level k is kicked with half * dt_max / 2**k; levels below the floor get 0."""
+    return np.asarray([(float(half) * float(dt_max) / float(1 << k)) if k >= int(active_floor) else 0.0
+                       for k in range(int(k_max) + 1)], dtype=dtype)
+
+
+def boundary_level_weights(s: int, k_max: int, dt_max: float, *, dtype=np.float64) -> np.ndarray:
+    """The kick weights at boundary s: half = 0.5 at the synchronised ends."""
+    return level_weights_from_floor(active_level_floor(s, k_max), k_max, dt_max,
+                                    half=0.5 if is_sync_boundary(s, k_max) else 1.0, dtype=dtype)
+
+
+def boundary_weight_table(k_max: int, dt_max: float, *, dtype=np.float64) -> np.ndarray:
+    """Row s = boundary_level_weights(s, ...), s = 0 .. 2**k_max."""
+    return np.stack([boundary_level_weights(s, k_max, dt_max, dtype=dtype) for s in range(n_sub(k_max) + 1)])
 
 
 def mutual_near_field_forces(state: MutualFMMState, positions, masses):

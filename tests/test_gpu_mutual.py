@@ -63,3 +63,27 @@ def test_symmetric_gears_keep_momentum():
         out[sym] = mutual.momentum_residual(m[:, None] * ps.run()[:, :3].double())
     assert out[True] < ROUND_OFF
     assert out[False] > out[True]  # per-direction orders break the pairwise balance
+
+
+def test_block_step_weights():
+    """The rung-weighted form: unit weights give the full acceleration, the
+    per-level accelerations add up to it, and any weights keep momentum."""
+    n = 131_072
+    pos, mass = workloads.plummer(n, 12)
+    rng = np.random.default_rng(3)
+    rung = rng.integers(0, 4, size=n).astype(np.int32)
+    mt, _ = mutual.build_mutual_topology(pos, mass, theta=0.55, order=6, leaf_size=32)
+    st = mutual.build_mutual_state(mt, softening=1e-3)
+    full = mutual.mutual_accelerations(st, pos, mass)
+    scale = np.sqrt((full ** 2).sum(1).mean())
+    ones = mutual.mutual_accelerations(st, pos, mass, rung=rung, level_weights=np.ones(4, np.float32))
+    assert np.abs(ones - full).max() <= 1e-6 * scale
+    levels = [mutual.mutual_level_accelerations(st, pos, mass, rung=rung, level=k, k_max=3) for k in range(4)]
+    assert np.abs(sum(levels) - full).max() <= 1e-5 * scale
+    assert all(np.abs(a).max() > 0 for a in levels)
+    w = mutual.boundary_level_weights(0, 3, 0.01).astype(np.float32)
+    res = mutual.mutual_accelerations(st, pos, mass, rung=rung, level_weights=w, return_parts=True)
+    for f in (res.near_forces, res.far_forces, res.near_forces + res.far_forces):
+        assert mutual.momentum_residual(f) < ROUND_OFF
+    with pytest.raises(ValueError):
+        mutual.mutual_accelerations(st, pos, mass, rung=rung)

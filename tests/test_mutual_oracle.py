@@ -42,3 +42,20 @@ def test_canonical_lists_hold_every_pair_once():
     both = {(min(a, b), max(a, b)) for a, b in zip(tgt.tolist(), t.far_sources.tolist())}
     assert canon == both and len(canon) == mt.far_a.size
     assert mt.self_leaves.size == t.num_leaves and mt.leaf_nodes[0] == t.num_internal
+
+
+def test_block_step_bookkeeping():
+    """Boundary weights of a 2**k_max sub-step base step (force.py:685-883
+    there): ends kick every level with half weight, inner boundaries kick the
+    levels at or above the trailing-zero floor."""
+    k = 3
+    assert mutual.n_sub(k) == 8
+    assert mutual.is_sync_boundary(0, k) and mutual.is_sync_boundary(8, k) and not mutual.is_sync_boundary(4, k)
+    assert [mutual.active_level_floor(s, k) for s in range(9)] == [0, 3, 2, 3, 1, 3, 2, 3, 0]
+    w = mutual.boundary_level_weights(0, k, 1.0)
+    assert np.allclose(w, [0.5, 0.25, 0.125, 0.0625])
+    assert np.allclose(mutual.boundary_level_weights(2, k, 1.0), [0, 0, 0.25, 0.125])
+    table = mutual.boundary_weight_table(k, 2.0)
+    assert table.shape == (9, 4) and np.allclose(table[4], [0, 1.0, 0.5, 0.25])
+    # every level receives dt_max / 2**k per its own sub-step over the base step
+    assert np.allclose(table.sum(0), 2.0)
