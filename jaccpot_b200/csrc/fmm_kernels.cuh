@@ -886,7 +886,7 @@ static __global__ void __launch_bounds__(256) k_leaf_reduce(int num_split, const
 }
 
 // ---------------------------------------------------------------------------
-// Target subset: warp per target.
+// Target subset: warp per target, lane per source leaf.
 // ---------------------------------------------------------------------------
 template <int P>
 __global__ void __launch_bounds__(128) k_eval_targets(const float4* __restrict__ pos4, int num_internal,
@@ -904,10 +904,15 @@ __global__ void __launch_bounds__(128) k_eval_targets(const float4* __restrict__
   const int node = num_internal + leaf;
   const float4 ti = pos4[i];
   float ax = 0.f, ay = 0.f, az = 0.f, aw = 0.f;
+  // lane k takes the k-th source leaf of each group of 32 (the target's own
+  // leaf first) and runs through its particles: the leaves' range lookups
+  // overlap instead of following one another
   const int64_t e0 = near_off[leaf], e1 = near_off[leaf + 1];
-  for (int64_t e = e0 - 1; e < e1; ++e) {
+  for (int64_t eb = e0 - 1; eb < e1; eb += 32) {
+    const int64_t e = eb + lane;
+    if (e >= e1) continue;
     const int2 sr = (e < e0) ? ranges[node] : ranges[num_internal + near_src[e]];
-    for (int j = sr.x + lane; j <= sr.y; j += 32) {
+    for (int j = sr.x; j <= sr.y; ++j) {
       const float4 s = pos4[j];
       const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
       const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
