@@ -1,6 +1,8 @@
 // C-ABI entry points (include/jaccpot_b200.h) and the order-independent kernels.
 #include "fmm_adjoint.cuh"
 
+#include <mutex>
+
 #define JB_ORDERS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 JB_ORDERS(JB_DECLARE_ORDER)
 
@@ -377,6 +379,44 @@ JB_API int jb_m2l_weighted(int p, int num_units, const int* units, const float* 
                           ST(stream), false, 0, far_w);
 }
 
+}  // extern "C"
+
+namespace jb {
+// Side streams of the gear M2L, one set per device, made on first use: the
+// gears' launches touch disjoint rows (a target split over several units,
+// whatever their gears, writes only its own partial rows), so they run side
+// by side instead of one after the other, joined back by events.
+struct GearStreams {
+  cudaStream_t s[8];
+  cudaEvent_t fork, join[8];
+};
+
+static int gear_streams(GearStreams** out) {
+  static std::mutex mu;
+  static GearStreams per_dev[64];
+  static bool made[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (dev < 0 || dev >= 64) return JB_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!made[dev]) {
+    GearStreams& g = per_dev[dev];
+    e = cudaEventCreateWithFlags(&g.fork, cudaEventDisableTiming);
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithFlags(&g.s[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.join[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    made[dev] = true;
+  }
+  *out = &per_dev[dev];
+  return JB_OK;
+}
+}  // namespace jb
+
+extern "C" {
+
 JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orders, const int64_t* gear_unit_offsets,
                         const int* units, const float* mult, const float* centers, const int* far_src,
                         float* locals, float* partials, int num_split, const int* split, void* stream) {
@@ -389,11 +429,35 @@ JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orde
     const int pg = gear_orders[g];
     const int64_t u0 = gear_unit_offsets[g], u1 = gear_unit_offsets[g + 1];
     if (pg < 1 || pg > p_max || u0 < 0 || u1 < u0) return JB_ERR_ARG;
-    if (u1 == u0) continue;
-    if (!units || !mult || !centers || !far_src || !locals) return JB_ERR_ARG;
-    const int rc = dispatch<RunM2L>(pg, (int)(u1 - u0), units + 4 * u0, mult, centers, far_src, locals, partials, 0,
-                                    (const int*)nullptr, ST(stream), false, rs);
+    if (u1 > u0 && (!units || !mult || !centers || !far_src || !locals)) return JB_ERR_ARG;
+  }
+  // the last gear (the highest order, most of the work) on the caller's
+  // stream, the others on side streams forked from it and joined back
+  GearStreams* gs = nullptr;
+  const bool side = num_gears > 1 && num_gears <= 9;
+  if (side) {
+    const int rc = gear_streams(&gs);
     if (rc) return rc;
+    const cudaError_t e = cudaEventRecord(gs->fork, ST(stream));
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  for (int g = 0; g < num_gears; ++g) {
+    const int64_t u0 = gear_unit_offsets[g], u1 = gear_unit_offsets[g + 1];
+    if (u1 == u0) continue;
+    cudaStream_t st = ST(stream);
+    if (side && g < num_gears - 1) {
+      st = gs->s[g];
+      const cudaError_t e = cudaStreamWaitEvent(st, gs->fork, 0);
+      if (e != cudaSuccess) return cuda_status(e);
+    }
+    const int rc = dispatch<RunM2L>(gear_orders[g], (int)(u1 - u0), units + 4 * u0, mult, centers, far_src, locals,
+                                    partials, 0, (const int*)nullptr, st, false, rs);
+    if (rc) return rc;
+    if (side && g < num_gears - 1) {
+      cudaError_t e = cudaEventRecord(gs->join[g], st);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ST(stream), gs->join[g], 0);
+      if (e != cudaSuccess) return cuda_status(e);
+    }
   }
   if (num_split > 0) {
     k_m2l_reduce<<<blocks_1d((int64_t)num_split * rs, 256), 256, 0, ST(stream)>>>(

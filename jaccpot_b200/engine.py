@@ -154,8 +154,8 @@ class Pass:
 
     def __init__(self, dt: DeviceTopology, p: int, *, G: float = 1.0, eps2: float = 0.0,
                  m2l_mode: int = _lib.JB_M2L_FP32, p2p_mode: int = _lib.JB_P2P_FP32,
-                 leaf_range: tuple[int, int] | None = None, m2l_unit_pairs: int = 64,
-                 leaf_unit_sources: int = 4096):
+                 leaf_range: tuple[int, int] | None = None, m2l_unit_pairs: int = 512,
+                 leaf_unit_sources: int = 4096, gear_unit_pairs: int = 128):
         if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
             raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
         if dt.topo.max_leaf_occupancy > 32:
@@ -171,6 +171,9 @@ class Pass:
         self.tc_layout = "units"
         self.tc_products = 1
         self.p2p_mode = int(p2p_mode)
+        # work-unit sizes (pairs per M2L unit, per gear unit; sources per leaf
+        # unit), measured at clustered N=4M, p=8
+        self.gear_unit_pairs = int(gear_unit_pairs)
         self.ws = Workspace.allocate(dt, self.p)
         self.lib = _lib.lib()
         t = dt.topo
@@ -249,9 +252,9 @@ class Pass:
         if max(orders) > self.p or min(orders) < 1:
             raise ValueError(f"gear orders must lie in [1, {self.p}]")
         if _on_gpu(self.dt):
-            gs = gear_m2l_schedule_device(self.dt, gears, orders)
+            gs = gear_m2l_schedule_device(self.dt, gears, orders, max_pairs=self.gear_unit_pairs)
         else:
-            gs = gear_m2l_schedule(self.dt.topo, np.asarray(gears), orders)
+            gs = gear_m2l_schedule(self.dt.topo, np.asarray(gears), orders, max_pairs=self.gear_unit_pairs)
         if getattr(self, "_range_targets", None) is not None:
             gs = _restrict_gears(gs, self._range_targets, self.dt.topo.num_nodes, self.dt.device)
         dev = self.dt.device
