@@ -478,7 +478,7 @@ class Pass:
         if hasattr(self, "_adj_m2l"):
             msc = self._adj_m2l
         else:
-            msc = m2l_schedule_device(dt, max_pairs=64) if _on_gpu(dt) else m2l_schedule(t, max_pairs=64)
+            msc = m2l_schedule_device(dt, max_pairs=512) if _on_gpu(dt) else m2l_schedule(t, max_pairs=512)
             self._adj_m2l = msc
             up = lambda a: _up(a, dt.device)
             A["m2l_units"], A["m2l_split"] = up(msc.units), up(msc.split)
