@@ -7,13 +7,16 @@
 // writer, so results are run-to-run deterministic):
 //   P2M        warp per leaf: COM by warp reduction, U_n^m per lane, transpose
 //              reduction of the (p+1)^2 coefficients through shared memory;
-//   M2M / L2L  thread per (parent) / (parent, child), one launch per level;
-//   M2L        thread per work unit (<= 64 pairs of one target's CSR list),
+//   M2M / L2L  one launch per level: each translation's degrees split over
+//              four warps (k_*_level_split), or thread per (parent, child) on
+//              the wide L2L levels;
+//   M2L        thread per work unit (<= 512 pairs of one target's CSR list),
 //              units sorted by length so warps stay converged; the local
 //              accumulates in registers;
-//   leaf eval  warp per target leaf: L2P (lane = particle, the leaf's local
-//              staged once in shared memory) fused with the P2P near field,
-//              source leaves staged 32 particles at a time in shared memory.
+//   leaf eval  L2P warp per leaf (lane = particle, the leaf's local staged in
+//              shared memory), then P2P warp per work unit (a leaf and a slice
+//              of its neighbour list), sources staged 32 at a time in shared
+//              memory.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
