@@ -174,6 +174,8 @@ class Pass:
         # work-unit sizes (pairs per M2L unit, per gear unit; sources per leaf
         # unit), measured at clustered N=4M, p=8
         self.gear_unit_pairs = int(gear_unit_pairs)
+        self.m2l_unit_pairs = int(m2l_unit_pairs)
+        self.leaf_unit_sources = int(leaf_unit_sources)
         self.ws = Workspace.allocate(dt, self.p)
         self.lib = _lib.lib()
         t = dt.topo

@@ -93,8 +93,8 @@ def test_pass_is_identical_through_either_schedule(topo):
     a = ps.run().clone()
     host = engine.Pass(dt, 6, G=1.0, eps2=1e-6, p2p_mode=_lib.JB_P2P_KAHAN)
     t = dt.topo
-    host.m2l_sched = schedule.m2l_schedule(t)
-    host.leaf_sched = schedule.leaf_schedule(t)
+    host.m2l_sched = schedule.m2l_schedule(t, max_pairs=ps.m2l_unit_pairs)
+    host.leaf_sched = schedule.leaf_schedule(t, max_sources=ps.leaf_unit_sources)
     up = lambda x: torch.from_numpy(x if x.size else np.zeros(4, np.int32)).cuda()
     host.d_m2l_units, host.d_m2l_split = up(host.m2l_sched.units), up(host.m2l_sched.split)
     host.d_leaf_units, host.d_leaf_aux = up(host.leaf_sched.units), up(host.leaf_sched.aux)
