@@ -57,7 +57,7 @@ ERR_BOUND = 1e-4
 
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks + throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks + throttle reasons sampled every 50 ms."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -72,7 +72,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except FileNotFoundError:
@@ -82,6 +82,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([c.strip() for c in line.split(",")])
+
+    def wait_first(self, timeout: float = 5.0) -> None:
+        """Blocks until the sampler has produced a row (nvidia-smi takes a
+        moment to start), so the timed region that follows is covered."""
+        t0 = time.perf_counter()
+        while self.proc is not None and not self.rows and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -181,7 +188,7 @@ def _events_ms(fn, stream, reps=10, warm=3):
     return float(np.median(ts))
 
 
-def measure_prepare(pos, mass, cfg, dev, with_host: bool) -> dict:
+def measure_prepare(pos, mass, cfg, dev, with_host: bool, fmm=None) -> dict:
     """Prepare-time tree + interaction lists for the headline workload: the GPU
     build (jb_tree_build_device; wall time around the call, which syncs: first
     call and the median of three more) and, with_host, the host build of the
@@ -208,6 +215,13 @@ def measure_prepare(pos, mass, cfg, dev, with_host: bool) -> dict:
         lb.jb_dtree_free(h)
     out = {"tree_gpu_ms_first": times[0], "tree_gpu_ms": float(np.median(times[1:])),
            "what": "Morton sort + radix split + FP64 COM/radii + dual walk + CSR lists, on the GPU"}
+    if fmm is not None:  # a second prepare_state: the kernels are loaded, the pools warm
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        st2 = fmm.prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
+        torch.cuda.synchronize(dev)
+        out["prepare_state_warm_s"] = time.perf_counter() - t0
+        del st2
     if with_host:
         dev_topo = tree.build_topology(p, m, leaf_size=cfg["leaf_size"], theta=cfg["theta"], device=dev)
         t0 = time.perf_counter()
@@ -422,10 +436,11 @@ def main() -> None:
         for _ in range(args.warmup):
             step(ps)
         torch.cuda.synchronize()
-    # plain, then chosen (clocks sampled over the chosen form's timed region)
-    ms_plain, stage_plain = timed(passes["plain"], args.steps)
-    ms_split, stage_split = timed(passes["split_bf16"], args.steps)
+    # plain, split-BF16, chosen; clocks sampled over all three timed regions
     with ClockSampler(local) as cs:
+        cs.wait_first()
+        ms_plain, stage_plain = timed(passes["plain"], args.steps)
+        ms_split, stage_split = timed(passes["split_bf16"], args.steps)
         ms_chosen, stage_chosen = timed(passes["chosen"], args.steps)
     clocks = cs.summary()
 
@@ -538,7 +553,7 @@ def main() -> None:
                "sample": f"one float32 pass of the oracle on clustered N={ns} (same generator/order/leaf/theta)"}
 
     extras = measure_extras(dev, stream) if (rank == 0 and world == 1 and not args.no_extras) else None
-    prep = measure_prepare(pos, mass, cfg, dev, with_host=not args.no_extras) if rank == 0 else None
+    prep = measure_prepare(pos, mass, cfg, dev, with_host=not args.no_extras, fmm=fmm) if rank == 0 else None
     launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
     if rank == 0:
         cfg.update({
@@ -560,7 +575,7 @@ def main() -> None:
             "err_vs_fp64_direct": errs,
             "err_targets": int(tg.size),
             "err_bound_met": bool(errs["chosen"]["p99"] <= ERR_BOUND),
-            "prepare_s": prep_s,
+            "prepare_s": prep_s,  # first prepare_state of the process (kernel loading included)
             "prepare": prep,
             "num_nodes": topo.num_nodes,
             "far_pairs": topo.num_far_pairs,
