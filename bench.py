@@ -124,7 +124,7 @@ def _peaks() -> dict:
 # DRAM bytes (read + write) per launch of the dominant kernels at the bench
 # workload, scaled from single-launch ncu captures of a 1M-particle case by
 # the units processed (far pairs / particle pairs); see profiles/.
-TRAFFIC_PER_UNIT = {"k_m2l_units": 12.1, "k_m2l_tc_units": 12.3, "k_leaf_units": 0.0136}
+TRAFFIC_PER_UNIT = {"k_m2l_units": 7.8, "k_m2l_tc_units": 12.3, "k_leaf_units": 0.0136}
 
 
 def _traffic(kernel: str, units: float | None = None):
