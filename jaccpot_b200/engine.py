@@ -154,7 +154,7 @@ class Pass:
 
     def __init__(self, dt: DeviceTopology, p: int, *, G: float = 1.0, eps2: float = 0.0,
                  m2l_mode: int = _lib.JB_M2L_FP32, p2p_mode: int = _lib.JB_P2P_FP32,
-                 leaf_range: tuple[int, int] | None = None, m2l_unit_pairs: int = 512,
+                 leaf_range: tuple[int, int] | None = None, m2l_unit_pairs: int | None = None,
                  leaf_unit_sources: int = 4096, gear_unit_pairs: int = 128):
         if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
             raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
@@ -174,6 +174,8 @@ class Pass:
         # work-unit sizes (pairs per M2L unit, per gear unit; sources per leaf
         # unit), measured at clustered N=4M, p=8
         self.gear_unit_pairs = int(gear_unit_pairs)
+        if m2l_unit_pairs is None:  # the tensor-core form steps a group's units together: shorter units
+            m2l_unit_pairs = 64 if self.m2l_mode == _lib.JB_M2L_SPLIT_BF16 else 512
         self.m2l_unit_pairs = int(m2l_unit_pairs)
         self.leaf_unit_sources = int(leaf_unit_sources)
         self.ws = Workspace.allocate(dt, self.p)
@@ -191,10 +193,10 @@ class Pass:
         # work-unit schedules: built on the GPU from the resident lists when
         # the pass runs there (the host builders give the same arrays)
         if _on_gpu(dt):
-            self.m2l_sched = m2l_schedule_device(dt, max_pairs=m2l_unit_pairs, targets=targets)
+            self.m2l_sched = m2l_schedule_device(dt, max_pairs=self.m2l_unit_pairs, targets=targets)
             self.leaf_sched = leaf_schedule_device(dt, max_sources=leaf_unit_sources, leaf_range=self.leaf_range)
         else:
-            self.m2l_sched = m2l_schedule(t, max_pairs=m2l_unit_pairs, targets=targets)
+            self.m2l_sched = m2l_schedule(t, max_pairs=self.m2l_unit_pairs, targets=targets)
             self.leaf_sched = leaf_schedule(t, max_sources=leaf_unit_sources, leaf_range=self.leaf_range)
         dev = dt.device
         up = lambda a: _up(a, dev)
