@@ -506,7 +506,13 @@ class Pass:
                                           _ptr(grad_mass), s), "jb_scatter_unsorted(grad)")
 
     def launches_per_run(self) -> int:
+        """This library's kernel launches in one run(): P2M, one M2M per level,
+        the M2L (one launch per non-empty gear with gears) and its split
+        reduce, one L2L per level, the leaf L2P + P2P and their split reduce."""
         t = self.dt.topo
-        # p2m + m2m levels + m2l (+ reduce) + l2l levels + leaf eval (+ reduce)
-        return (1 + t.num_levels + 1 + int(self.m2l_sched.split.shape[0] > 0) + t.num_levels + 1
-                + int(self.leaf_sched.split.shape[0] > 0))
+        gs = getattr(self, "gear_sched", None)
+        if gs is not None and self.m2l_mode == _lib.JB_M2L_FP32:
+            m2l = int((np.diff(np.asarray(gs.gear_offsets)) > 0).sum()) + int(gs.split.shape[0] > 0)
+        else:
+            m2l = 1 + int(self.m2l_sched.split.shape[0] > 0)
+        return (1 + t.num_levels + m2l + t.num_levels + 2 + int(self.leaf_sched.split.shape[0] > 0))
