@@ -174,6 +174,12 @@ JB_API void jb_dsched_free(jb_dsched* d);
  * translation.  Same operations either way.  Process-wide setting.          */
 JB_API int jb_set_level_split(int m2m_max_parents, int l2l_max_parents);
 
+/* Near field of jb_leaf_eval: 1 (default) walks the target x source-chunk
+ * work of leaves with more than 16 particles chunk-major over all 32 lanes
+ * of a warp; 0 gives each target one lane (idle lanes for the rest).  The
+ * sums are bit-identical either way.  Process-wide setting.               */
+JB_API int jb_set_leaf_form(int chunk_major);
+
 /* Row stride (floats) of a coefficient array of order p: (p+1)^2 rounded up
  * to a multiple of 4.  Returns 0 for an unsupported order. */
 JB_API int jb_coeff_stride(int p);

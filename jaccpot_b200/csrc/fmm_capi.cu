@@ -10,6 +10,7 @@ namespace jb {
 
 static thread_local char g_err[256] = {0};
 int g_split_max_parents[2] = {1 << 30, 2048};  // measured at clustered N=4M, p=8
+int g_leaf_flat = 1;
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return JB_OK;
@@ -293,6 +294,12 @@ JB_API int jb_set_level_split(int m2m_max_parents, int l2l_max_parents) {
   return JB_OK;
 }
 
+JB_API int jb_set_leaf_form(int chunk_major) {
+  if (chunk_major != 0 && chunk_major != 1) return JB_ERR_ARG;
+  jb::g_leaf_flat = chunk_major;
+  return JB_OK;
+}
+
 JB_API int jb_coeff_stride(int p) { return (p >= 1 && p <= JB_MAX_ORDER) ? cstride(p) : 0; }
 
 JB_API const char* jb_last_cuda_error(void) { return g_err; }
@@ -501,7 +508,8 @@ JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal
   if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL | JB_P2P_FAR_ONLY | JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
   if ((p2p_mode & JB_P2P_FAR_ONLY) && (p2p_mode & JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
   return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, num_units, units, aux, runs, node_ranges, centers,
-                               locals, G, eps2, out_acc4, partials, num_split, split, ST(stream));
+                               locals, G, eps2, out_acc4, partials, num_split, split, ST(stream), nullptr, nullptr,
+                               1, jb::g_leaf_flat != 0);
 }
 
 JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int* node_ranges, const float* centers,

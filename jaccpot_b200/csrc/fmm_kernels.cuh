@@ -35,6 +35,9 @@ int cuda_status(cudaError_t e);
 // [1] kernels, wider ones the thread-per-translation kernels
 // (jb_set_level_split).
 extern int g_split_max_parents[2];
+// Nonzero: leaves of more than 16 particles take the chunk-major near-field
+// form (k_leaf_units_flat) in jb_leaf_eval (jb_set_leaf_form).
+extern int g_leaf_flat;
 inline int launch_status() { return cuda_status(cudaGetLastError()); }
 
 // ---------------------------------------------------------------------------
@@ -831,6 +834,218 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
     leaf_unit<1, KAHAN, POT, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
 }
 
+// ---------------------------------------------------------------------------
+// Near field with every lane busy, for leaves of 17..32 particles.
+//
+// One lane per target leaves 32 - nt lanes idle.  Here a unit's work, nt
+// targets x C source chunks of 32, is walked chunk-major: item f = c * nt + t,
+// 32 items per warp step, lane l of step s takes item 32 s + l (target
+// f mod nt against chunk f / nt).  A step spans at most three consecutive
+// chunks (nt >= 17), so the chunks sit in a ring of four shared-memory slots,
+// padded so that the slots one load instruction reads fall in different
+// banks, and are fetched two chunks ahead.  The per-target sums live in
+// shared memory: lane l < nt owns its item's target and, when lane l + nt
+// holds the same target's next chunk, adds that partial straight after its
+// own.  Every target therefore receives its chunk partials in chunk order
+// through the same (compensated) add as in the lane-per-target form, from
+// the same per-chunk arithmetic: the results are bit-identical to it.
+// ---------------------------------------------------------------------------
+struct alignas(16) FlatStage {
+  float x[4][36], y[4][36], z[4][36], m[4][36];  // source chunk ring (slot stride 144 B)
+  float4 tp[32];                                   // target positions
+  float4 s[32], c[32];                             // per-target sums and their compensations
+};
+
+union WarpStage {
+  NearStage n;
+  FlatStage f;
+};
+
+// Sums of one 32-source chunk for one target, the arithmetic of near_chunk
+// with one lane per target (packed pairs j, j + 1; the two halves added).
+template <bool POT, bool SELF>
+__device__ __forceinline__ float4 chunk_sums(const float* xs, const float* ys, const float* zs, const float* ms,
+                                             float4 ti, int self_j, float eps2) {
+  const ulonglong2* X = reinterpret_cast<const ulonglong2*>(xs);
+  const ulonglong2* Y = reinterpret_cast<const ulonglong2*>(ys);
+  const ulonglong2* Z = reinterpret_cast<const ulonglong2*>(zs);
+  const ulonglong2* M = reinterpret_cast<const ulonglong2*>(ms);
+  const f32x2 TX = f2(ti.x, ti.x), TY = f2(ti.y, ti.y), TZ = f2(ti.z, ti.z), E2 = f2(eps2, eps2);
+  f32x2 AX = f2(0.f, 0.f), AY = AX, AZ = AX, AW = AX;
+  auto step = [&](f32x2 sx, f32x2 sy, f32x2 sz, f32x2 sm, int j0) {
+    const f32x2 dx = f2_sub(TX, sx);
+    const f32x2 dy = f2_sub(TY, sy);
+    const f32x2 dz = f2_sub(TZ, sz);
+    const f32x2 d2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, E2)));
+    float d2a, d2b;
+    f2_split(d2, d2a, d2b);
+    const f32x2 ir = f2(rsqrtf(d2a), rsqrtf(d2b));
+    f32x2 mir = f2_mul(sm, ir);
+    f32x2 w = f2_mul(mir, f2_mul(ir, ir));
+    if (SELF) {
+      float m0, m1, w0, w1;
+      f2_split(mir, m0, m1);
+      f2_split(w, w0, w1);
+      m0 = (j0 == self_j) ? 0.f : m0;
+      w0 = (j0 == self_j) ? 0.f : w0;
+      m1 = (j0 + 1 == self_j) ? 0.f : m1;
+      w1 = (j0 + 1 == self_j) ? 0.f : w1;
+      mir = f2(m0, m1);
+      w = f2(w0, w1);
+    }
+    AX = f2_fma(w, dx, AX);
+    AY = f2_fma(w, dy, AY);
+    AZ = f2_fma(w, dz, AZ);
+    if (POT) AW = f2_add(AW, mir);
+  };
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    const ulonglong2 x = X[v], y = Y[v], z = Z[v], m = M[v];
+    step(x.x, y.x, z.x, m.x, 4 * v);
+    step(x.y, y.y, z.y, m.y, 4 * v + 2);
+  }
+  float x0, x1, y0, y1, z0, z1, w0 = 0.f, w1 = 0.f;
+  f2_split(AX, x0, x1);
+  f2_split(AY, y0, y1);
+  f2_split(AZ, z0, z1);
+  if (POT) f2_split(AW, w0, w1);
+  return make_float4(x0 + x1, y0 + y1, z0 + z1, POT ? w0 + w1 : 0.f);
+}
+
+// Adds one chunk's sums into target t's accumulator in shared memory.
+template <bool KAHAN, bool POT>
+__device__ __forceinline__ void flat_add(FlatStage& S, int t, float4 v) {
+  NearAcc<KAHAN> a;
+  const float4 s = S.s[t];
+  a.s[0] = s.x, a.s[1] = s.y, a.s[2] = s.z, a.s[3] = s.w;
+  if (KAHAN) {
+    const float4 c = S.c[t];
+    a.c[0] = c.x, a.c[1] = c.y, a.c[2] = c.z, a.c[3] = c.w;
+  }
+  a.add(0, v.x);
+  a.add(1, v.y);
+  a.add(2, v.z);
+  if (POT) a.add(3, v.w);
+  S.s[t] = make_float4(a.s[0], a.s[1], a.s[2], a.s[3]);
+  if (KAHAN) S.c[t] = make_float4(a.c[0], a.c[1], a.c[2], a.c[3]);
+}
+
+template <bool KAHAN, bool POT>
+__device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
+                                               const int2* __restrict__ runs, FlatStage& S, int lane, float G_,
+                                               float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
+  const int nt = rg.y - rg.x + 1;  // 17..32
+  const bool tgt = lane < nt;
+  const float4 me = tgt ? pos4[rg.x + lane] : JB_PAD4;
+  S.tp[lane] = me;
+  S.s[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (KAHAN) S.c[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (aux.y & 1) {  // the self block, lane per target, diagonal excluded
+    S.x[0][lane] = me.x;
+    S.y[0][lane] = me.y;
+    S.z[0][lane] = me.z;
+    S.m[0][lane] = me.w;
+    __syncwarp();
+    const float4 ti = tgt ? me : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 v = chunk_sums<POT, true>(S.x[0], S.y[0], S.z[0], S.m[0], ti, lane, eps2);
+    if (tgt) flat_add<KAHAN, POT>(S, lane, v);
+  }
+  const int nsrc = U.w;
+  if (nsrc > 0) {
+    const int C = (nsrc + 31) >> 5;
+    const int total = nt * C;
+    int r = U.y, rbase = 0;
+    int2 run = runs[r];
+    auto fetch = [&](int f) -> float4 {  // source f of the unit (padding past the end)
+      while (f >= rbase + run.y && r + 1 < U.z) {
+        rbase += run.y;
+        ++r;
+        run = runs[r];
+      }
+      return (f < nsrc) ? pos4[run.x + (f - rbase)] : JB_PAD4;
+    };
+    float4 q0 = fetch(lane);                          // the next chunk to stage
+    float4 q1 = (C > 1) ? fetch(32 + lane) : JB_PAD4;  // the one after
+    int staged = 0;
+    int c = (lane >= nt) ? 1 : 0, t = lane - c * nt;  // item f = lane
+    for (int base = 0; base < total; base += 32) {
+      const int chi = min(__shfl_sync(0xffffffffu, c, 31), C - 1);
+      __syncwarp();  // the previous step's reads and adds are done
+      while (staged <= chi) {
+        const int sl = staged & 3;
+        S.x[sl][lane] = q0.x;
+        S.y[sl][lane] = q0.y;
+        S.z[sl][lane] = q0.z;
+        S.m[sl][lane] = q0.w;
+        q0 = q1;
+        ++staged;
+        if (staged + 1 < C) q1 = fetch((staged + 1) * 32 + lane);
+      }
+      __syncwarp();
+      const int sl = c & 3;
+      const float4 v = chunk_sums<POT, false>(S.x[sl], S.y[sl], S.z[sl], S.m[sl], S.tp[t], -1, eps2);
+      float4 v2;
+      v2.x = __shfl_down_sync(0xffffffffu, v.x, nt);
+      v2.y = __shfl_down_sync(0xffffffffu, v.y, nt);
+      v2.z = __shfl_down_sync(0xffffffffu, v.z, nt);
+      v2.w = POT ? __shfl_down_sync(0xffffffffu, v.w, nt) : 0.f;
+      if (tgt && base + lane < total) {
+        flat_add<KAHAN, POT>(S, t, v);
+        if (lane + nt < 32 && base + lane + nt < total) flat_add<KAHAN, POT>(S, t, v2);  // (t, c + 1)
+      }
+      t += 32 - nt;  // item f + 32
+      c += 1;
+      if (t >= nt) {
+        t -= nt;
+        c += 1;
+      }
+    }
+  }
+  __syncwarp();
+  if (tgt) {
+    NearAcc<KAHAN> a;
+    const float4 s = S.s[lane];
+    a.s[0] = s.x, a.s[1] = s.y, a.s[2] = s.z, a.s[3] = s.w;
+    if (KAHAN) {
+      const float4 cc = S.c[lane];
+      a.c[0] = cc.x, a.c[1] = cc.y, a.c[2] = cc.z, a.c[3] = cc.w;
+    }
+    float v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = (POT || i < 3) ? a.value(i) : 0.f;
+    const float4 res = make_float4(-G_ * v[0], -G_ * v[1], -G_ * v[2], -G_ * v[3]);
+    if (aux.x < 0) {
+      const float4 f = out[rg.x + lane];  // the far field k_leaf_l2p wrote
+      out[rg.x + lane] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
+    } else {
+      partial[(size_t)aux.x * 32 + lane] = res;
+    }
+  }
+}
+
+// k_leaf_units with the chunk-major form for leaves of more than 16
+// particles (the lane-group forms below that).  Same results.
+template <bool KAHAN, bool POT>
+static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_leaf_units_flat(
+    const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
+    const int2* __restrict__ aux, const int2* __restrict__ runs, const int2* __restrict__ ranges, float G,
+    float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
+  __shared__ WarpStage sW[kWarpsPerBlock];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarpsPerBlock + warp;
+  if (u >= num_units) return;
+  const int4 U = units[u];
+  const int2 ax = aux[u];
+  const int2 rg = ranges[num_internal + U.x];
+  const int nt = rg.y - rg.x + 1;
+  if (nt <= 8)
+    leaf_unit<4, KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
+  else if (nt <= 16)
+    leaf_unit<2, KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
+  else
+    leaf_unit_flat<KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].f, lane, G, eps2, out, partial);
+}
+
 // Far field (L2P) of every leaf: warp per leaf (its unit with flags & 1),
 // lane per particle, the local expansion staged in shared memory.  Writes
 // out = -G (grad phi, phi); runs before k_leaf_units, which adds the near
@@ -1026,10 +1241,19 @@ struct RunLeafEval {
   template <bool K, bool PT>
   static void go(unsigned nb, cudaStream_t st, const float4* pos4, int num_internal, int num_units, const int4* units,
                  const int2* aux, const int2* runs, const int2* ranges, float G, float eps2, float4* out,
-                 float4* partial, const int* rung, const float* lw, int nlw) {
+                 float4* partial, const int* rung, const float* lw, int nlw, bool flat) {
     if (rung)
       k_leaf_units<K, PT, true><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs,
                                                                     ranges, G, eps2, out, partial, rung, lw, nlw);
+    else if (flat) {
+      // 15 KB of shared memory per block: ask for a carveout that holds the
+      // eight blocks per SM the launch bounds allow.
+      static const cudaError_t carve =
+          cudaFuncSetAttribute(k_leaf_units_flat<K, PT>, cudaFuncAttributePreferredSharedMemoryCarveout, 60);
+      (void)carve;
+      k_leaf_units_flat<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs,
+                                                                   ranges, G, eps2, out, partial);
+    }
     else
       k_leaf_units<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs, ranges,
                                                               G, eps2, out, partial);
@@ -1037,7 +1261,7 @@ struct RunLeafEval {
   static int run(int mode, const float* pos4, int num_internal, int num_units, const int* units, const int* aux,
                  const int* runs, const int* ranges, const float* centers, const float* locals, float G, float eps2,
                  float* out, float* partial, int num_split, const int* split, cudaStream_t st,
-                 const int* rung = nullptr, const float* lw = nullptr, int nlw = 1) {
+                 const int* rung = nullptr, const float* lw = nullptr, int nlw = 1, bool flat = false) {
     if (num_units > 0) {
       const unsigned nb = blocks_for(num_units, kWarpsPerBlock);
       auto a0 = reinterpret_cast<const float4*>(pos4);
@@ -1055,10 +1279,10 @@ struct RunLeafEval {
       if (rc) return rc;
       if (far_only) return JB_OK;
       const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
-      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
-      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
-      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
-      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw);
+      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
+      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
+      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
+      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
       rc = launch_status();
       if (rc) return rc;
     }
