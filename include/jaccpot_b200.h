@@ -176,8 +176,10 @@ JB_API int jb_set_level_split(int m2m_max_parents, int l2l_max_parents);
 
 /* Near field of jb_leaf_eval: 1 (default) walks the target x source-chunk
  * work of leaves with more than 16 particles chunk-major over all 32 lanes
- * of a warp; 0 gives each target one lane (idle lanes for the rest).  The
- * sums are bit-identical either way.  Process-wide setting.               */
+ * of a warp and takes 1/r from the flush-to-zero instruction; 0 gives each
+ * target one lane (idle lanes for the rest).  The sums are bit-identical
+ * either way while every squared distance (+ eps2) is 0 or at least 2^-126.
+ * Process-wide setting.                                                   */
 JB_API int jb_set_leaf_form(int chunk_major);
 
 /* Row stride (floats) of a coefficient array of order p: (p+1)^2 rounded up

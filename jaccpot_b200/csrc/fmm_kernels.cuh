@@ -638,6 +638,18 @@ __device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
   return d;
 }
 
+// 1/sqrt(x) by the approximate special-function instruction with subnormal
+// inputs and results flushed to zero: rsqrtf() adds a range test and two
+// multiplies around the same instruction so that subnormal inputs keep their
+// value; for normal inputs the two agree bit for bit.  A squared distance
+// below 2^-126 (points closer than about 1e-19) reads as 0 here (infinite
+// 1/r, as for coincident points).
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // The 32 sources of one chunk, staged per coordinate in the order the lane
 // groups read them: source j sits at position (j % G) * (32 / G) + j / G, so
 // group h's sources are one contiguous run and four of them load as one
@@ -672,7 +684,7 @@ struct PairWeights {
 // One chunk of 32 staged sources for this lane's target: the lane's 32/G
 // sources (j = q*G + h), two per packed step; the two partial sums are added
 // at the end of the chunk (and into the compensated accumulator when KAHAN).
-template <int G, bool KAHAN, bool POT, bool SELF, bool W = false>
+template <int G, bool KAHAN, bool POT, bool SELF, bool W = false, bool FTZ = false>
 __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h, int self_j, float eps2,
                                            NearAcc<KAHAN>& a, PairWeights pw = PairWeights{nullptr, 0}) {
   constexpr int R = 32 / G;
@@ -689,7 +701,7 @@ __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h
     const f32x2 d2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, E2)));
     float d2a, d2b;
     f2_split(d2, d2a, d2b);
-    const f32x2 ir = f2(rsqrtf(d2a), rsqrtf(d2b));
+    const f32x2 ir = FTZ ? f2(rsqrt_ftz(d2a), rsqrt_ftz(d2b)) : f2(rsqrtf(d2a), rsqrtf(d2b));
     f32x2 mir = f2_mul(sm, ir);
     f32x2 w = f2_mul(mir, f2_mul(ir, ir));
     if (W) {
@@ -735,7 +747,7 @@ __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h
   }
 }
 
-template <int G, bool KAHAN, bool POT, bool W = false>
+template <int G, bool KAHAN, bool POT, bool W = false, bool FTZ = false>
 __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
                                           const int2* __restrict__ runs, NearStage& sP, int lane, float G_,
                                           float eps2, float4* __restrict__ out, float4* __restrict__ partial,
@@ -753,7 +765,7 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
     stage_source<G>(sP, lane, (lane < nt) ? pos4[rg.x + lane] : JB_PAD4);
     if (W) stage_rung<G>(sP, lane, (lane < nt) ? clamp_rung(rung[rg.x + lane]) : 0);
     __syncwarp();
-    near_chunk<G, KAHAN, POT, true, W>(sP, ti, h, tl, eps2, a, pw);
+    near_chunk<G, KAHAN, POT, true, W, FTZ>(sP, ti, h, tl, eps2, a, pw);
     __syncwarp();
   }
   const int nsrc = U.w;
@@ -780,7 +792,7 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
         qn = qi >= 0 ? pos4[qi] : JB_PAD4;
         if (W) qr = qi >= 0 ? clamp_rung(rung[qi]) : 0;
       }
-      near_chunk<G, KAHAN, POT, false, W>(sP, ti, h, -1, eps2, a, pw);
+      near_chunk<G, KAHAN, POT, false, W, FTZ>(sP, ti, h, -1, eps2, a, pw);
       __syncwarp();
     }
   }
@@ -879,7 +891,7 @@ __device__ __forceinline__ float4 chunk_sums(const float* xs, const float* ys, c
     const f32x2 d2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, E2)));
     float d2a, d2b;
     f2_split(d2, d2a, d2b);
-    const f32x2 ir = f2(rsqrtf(d2a), rsqrtf(d2b));
+    const f32x2 ir = f2(rsqrt_ftz(d2a), rsqrt_ftz(d2b));
     f32x2 mir = f2_mul(sm, ir);
     f32x2 w = f2_mul(mir, f2_mul(ir, ir));
     if (SELF) {
@@ -1024,7 +1036,8 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
 }
 
 // k_leaf_units with the chunk-major form for leaves of more than 16
-// particles (the lane-group forms below that).  Same results.
+// particles (the lane-group forms below that) and rsqrt_ftz.  Same results
+// for squared distances in the normal FP32 range.
 template <bool KAHAN, bool POT>
 static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_leaf_units_flat(
     const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
@@ -1039,9 +1052,9 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
   const int2 rg = ranges[num_internal + U.x];
   const int nt = rg.y - rg.x + 1;
   if (nt <= 8)
-    leaf_unit<4, KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
+    leaf_unit<4, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
   else if (nt <= 16)
-    leaf_unit<2, KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
+    leaf_unit<2, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
   else
     leaf_unit_flat<KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].f, lane, G, eps2, out, partial);
 }

@@ -1,7 +1,9 @@
 """The two near-field forms of jb_leaf_eval (jb_set_leaf_form): one lane per
 target, or the chunk-major walk over all 32 lanes for leaves of more than 16
-particles.  Both add the same per-chunk sums in the same order, so the
-accelerations (and potentials) must be equal bit for bit, for whole and
+particles.  Both add the same per-chunk sums in the same order, and 1/r from
+the flush-to-zero instruction equals rsqrtf for the normal squared distances
+these inputs have, so the accelerations (and potentials) must be equal bit
+for bit, for whole and
 split leaves, with and without compensation, with and without a self block
 (target-range passes)."""
 
