@@ -124,7 +124,7 @@ def _peaks() -> dict:
 # DRAM bytes (read + write) per launch of the dominant kernels at the bench
 # workload, scaled from single-launch ncu captures of a 1M-particle case by
 # the units processed (far pairs / particle pairs); see profiles/.
-TRAFFIC_PER_UNIT = {"k_m2l_units": 7.8, "k_m2l_tc_units": 12.3, "k_leaf_units": 0.0136}
+TRAFFIC_PER_UNIT = {"k_m2l_units": 7.8, "k_m2l_tc_units": 12.3, "k_leaf_units_flat": 0.0133}
 
 
 def _traffic(kernel: str, units: float | None = None):
@@ -530,8 +530,9 @@ def main() -> None:
                 "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_m2l_units", topo.num_far_pairs)}
     else:
         ach = p2p_flops / (stage_chosen[3] / 1e3) / 1e12
-        roof = {"kernel": f"k_leaf_units<{cfg['order']},kahan>", "bound": "fp32", "achieved": ach,
-                "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_leaf_units", near_inter)}
+        roof = {"kernel": "k_leaf_units_flat<kahan> (leaf stage: + k_leaf_l2p, k_leaf_reduce)", "bound": "fp32",
+                "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                "traffic": _traffic("k_leaf_units_flat", near_inter)}
     roof["peak_source"] = ("measured bf16 burst (MEASURED_PEAKS.json)" if roof["bound"] == "tensor" else
                            "in-run FP32 FMA probe (MEASURED_PEAKS.json has HBM and bf16 only)")
     roof["stage_ms"] = float(stage_chosen[dom])

@@ -1147,7 +1147,7 @@ __global__ void __launch_bounds__(128) k_eval_targets(const float4* __restrict__
       const float4 s = pos4[j];
       const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
       const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-      const float ir = rsqrtf(d2);
+      const float ir = rsqrt_ftz(d2);
       const bool self = (j == i);
       const float mir = self ? 0.f : s.w * ir;
       const float w = self ? 0.f : mir * ir * ir;
