@@ -266,16 +266,10 @@ __global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units(int num_units, con
       cp_async_commit();
     }
     const int s2 = (e + 2 < e1) ? __ldg(far_src + e + 2) : s1;
-    if (NEG) m2l_kfold<P>(v, cs.x - ct.x, cs.y - ct.y, cs.z - ct.z);
-    else m2l_kfold<P>(v, ct.x - cs.x, ct.y - cs.y, ct.z - cs.z);
-    if (W) {
-      const float wt = __ldg(far_w + e);
-#pragma unroll
-      for (int k = 0; k < C; ++k) acc[k] = fmaf(wt, v[k], acc[k]);
-    } else {
-#pragma unroll
-      for (int k = 0; k < C; ++k) acc[k] += v[k];
-    }
+    const float dx = NEG ? cs.x - ct.x : ct.x - cs.x;
+    const float dy = NEG ? cs.y - ct.y : ct.y - cs.y;
+    const float dz = NEG ? cs.z - ct.z : ct.z - cs.z;
+    m2l_kfold_acc<P, W>(v, acc, dx, dy, dz, W ? __ldg(far_w + e) : 1.f);
     cs = cs1;
     cs1 = centers[s2];
     s1 = s2;
@@ -636,18 +630,6 @@ __device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
   f32x2 d;
   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
   return d;
-}
-
-// 1/sqrt(x) by the approximate special-function instruction with subnormal
-// inputs and results flushed to zero: rsqrtf() adds a range test and two
-// multiplies around the same instruction so that subnormal inputs keep their
-// value; for normal inputs the two agree bit for bit.  A squared distance
-// below 2^-126 (points closer than about 1e-19) reads as 0 here (infinite
-// 1/r, as for coincident points).
-__device__ __forceinline__ float rsqrt_ftz(float x) {
-  float r;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
 }
 
 // The 32 sources of one chunk, staged per coordinate in the order the lane

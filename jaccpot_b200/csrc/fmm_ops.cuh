@@ -147,6 +147,45 @@ __device__ __forceinline__ void rot_mult_to_z(float* v, const Trig<P>& taz, cons
   bu_apply<P, false, false, false>(v);
 }
 
+// 1/sqrt(x) by the approximate special-function instruction with subnormal
+// inputs and results flushed to zero: rsqrtf() adds a range test and two
+// multiplies around the same instruction so that subnormal inputs keep their
+// value; for normal inputs the two agree bit for bit.  A squared distance
+// below 2^-126 (points closer than about 1e-19) reads as 0 here (infinite
+// 1/r, as for coincident points).
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// acc += wt * Dz(+a) v (NEG = false) or wt * Dz(-a) v (NEG = true): dz_rot's
+// rotation with each rotated pair added into acc by two FMAs (no separate
+// add); W = false takes wt = 1 (and W = true with wt = 1 gives the same bits).
+template <int P, bool NEG, bool W = false>
+__device__ __forceinline__ void dz_rot_acc(const float* v, float* acc, float c1, float s1, float wt = 1.f) {
+#pragma unroll
+  for (int l = 0; l <= P; ++l) acc[shi(l, 0)] = W ? fmaf(wt, v[shi(l, 0)], acc[shi(l, 0)]) : acc[shi(l, 0)] + v[shi(l, 0)];
+  const float sa = NEG ? -s1 : s1;
+  float c = c1, s = sa;
+#pragma unroll
+  for (int m = 1; m <= P; ++m) {
+    if (m > 1) {
+      const float cn = c * c1 - s * sa;
+      s = fmaf(s, c1, c * sa);
+      c = cn;
+    }
+    const float cw = W ? c * wt : c, sw = W ? s * wt : s;
+#pragma unroll
+    for (int l = m; l <= P; ++l) {
+      const int ip = shi(l, m), im = shi(l, -m);
+      const float vp = v[ip], vm = v[im];
+      acc[ip] = fmaf(cw, vp, fmaf(-sw, vm, acc[ip]));
+      acc[im] = fmaf(sw, vp, fmaf(cw, vm, acc[im]));
+    }
+  }
+}
+
 // v <- Dz(+a) v (NEG = false) or Dz(-a) v (NEG = true) on every degree, with
 // (cos a, sin a) = (c1, s1); cos/sin(m a) by angle addition, m outermost so
 // that only four trig values are live.
@@ -238,6 +277,46 @@ __device__ __forceinline__ void m2l_kfold(float* v, float dx, float dy, float dz
     dz_rot<P, true>(w, caz, saz);
 #pragma unroll
     for (int k = 0; k < csize(P); ++k) v[k] = w[k];
+  }
+}
+
+// acc += wt * M2L(d) v (v is overwritten; W = false: wt = 1): the chain of
+// m2l_kfold for P <= 8 with the angles' 1/rho and 1/r from the approximate
+// reciprocal square root (instead of correctly rounded square roots and
+// divisions; the rotation cosines and sines move by about one ulp) and the
+// last z-rotation accumulating into acc.  The thread-per-unit M2L kernel uses
+// this form.
+template <int P, bool W = false>
+__device__ __forceinline__ void m2l_kfold_acc(float* v, float* acc, float dx, float dy, float dz, float wt = 1.f) {
+  if constexpr (P <= 8) {
+    const float rho2 = dx * dx + dy * dy;
+    const float r2 = rho2 + dz * dz;
+    float caz = 1.f, saz = 0.f, cax = 1.f, sax = 0.f, rho = 0.f, s = 1.0e30f;
+    if (rho2 > 0.f) {
+      const float ir = rsqrt_ftz(rho2);
+      caz = dy * ir;
+      saz = dx * ir;
+      rho = rho2 * ir;
+    }
+    if (r2 > 0.f) {
+      const float ir = rsqrt_ftz(r2);
+      cax = dz * ir;
+      sax = rho * ir;
+      s = ir;
+    }
+    dz_rot<P, false>(v, caz, saz);
+    BApply<P, false>::apply(v);
+    dz_rot<P, true>(v, cax, sax);
+    scale_degrees<P, 0>(v, s);
+    KFold<P>::apply(v);
+    scale_degrees<P, 1>(v, s);
+    dz_rot<P, false>(v, cax, sax);
+    BApply<P, true>::apply(v);
+    dz_rot_acc<P, true, W>(v, acc, caz, saz, wt);
+  } else {
+    m2l_kfold<P>(v, dx, dy, dz);
+#pragma unroll
+    for (int k = 0; k < csize(P); ++k) acc[k] = W ? fmaf(wt, v[k], acc[k]) : acc[k] + v[k];
   }
 }
 
