@@ -984,8 +984,25 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
       v2.z = __shfl_down_sync(0xffffffffu, v.z, nt);
       v2.w = POT ? __shfl_down_sync(0xffffffffu, v.w, nt) : 0.f;
       if (tgt && base + lane < total) {
-        flat_add<KAHAN, POT>(S, t, v);
-        if (lane + nt < 32 && base + lane + nt < total) flat_add<KAHAN, POT>(S, t, v2);  // (t, c + 1)
+        NearAcc<KAHAN> a;  // one read and one write of the target's sums for both adds
+        const float4 s0 = S.s[t];
+        a.s[0] = s0.x, a.s[1] = s0.y, a.s[2] = s0.z, a.s[3] = s0.w;
+        if (KAHAN) {
+          const float4 c0 = S.c[t];
+          a.c[0] = c0.x, a.c[1] = c0.y, a.c[2] = c0.z, a.c[3] = c0.w;
+        }
+        a.add(0, v.x);
+        a.add(1, v.y);
+        a.add(2, v.z);
+        if (POT) a.add(3, v.w);
+        if (lane + nt < 32 && base + lane + nt < total) {  // lane + nt holds (t, c + 1)
+          a.add(0, v2.x);
+          a.add(1, v2.y);
+          a.add(2, v2.z);
+          if (POT) a.add(3, v2.w);
+        }
+        S.s[t] = make_float4(a.s[0], a.s[1], a.s[2], a.s[3]);
+        if (KAHAN) S.c[t] = make_float4(a.c[0], a.c[1], a.c[2], a.c[3]);
       }
       t += 32 - nt;  // item f + 32
       c += 1;
@@ -1059,14 +1076,17 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
   if (u >= num_units || !(aux[u].y & 1)) return;
   const int node = num_internal + units[u].x;
   const int2 rg = ranges[node];
-  for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
-  __syncwarp();
-  if (rg.x + lane > rg.y) return;
+  const bool act = rg.x + lane <= rg.y;
   if (zero) {  // near field alone: the sums start from zero
-    out[rg.x + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (act) out[rg.x + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
     return;
   }
-  const float4 c = centers[node], ti = pos4[rg.x + lane];
+  // the particle and the centre are fetched alongside the local's staging
+  const float4 c = centers[node];
+  const float4 ti = act ? pos4[rg.x + lane] : c;
+  for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
+  __syncwarp();
+  if (!act) return;
   float U_[C];
   solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
   float phi, g[3];
