@@ -181,7 +181,7 @@ __device__ __forceinline__ void adj_near_pair(float4 tk, float4 wk, float4 s, fl
                                               float* a) {
   const float dx = tk.x - s.x, dy = tk.y - s.y, dz = tk.z - s.z;
   const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-  const float q = skip ? 0.f : rsqrtf(d2);
+  const float q = skip ? 0.f : rsqrt_ftz(d2);
   const float q3 = q * q * q;
   const float q5 = q3 * q * q;
   const float wkd = wk.x * dx + wk.y * dy + wk.z * dz;
