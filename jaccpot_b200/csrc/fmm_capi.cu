@@ -230,17 +230,23 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_adj_near(
     const int nsrc = U.w;
     int r = U.y, rbase = 0;
     int2 run = (U.z > U.y) ? runs[r] : make_int2(0, 0);
-    for (int base = 0; base < nsrc; base += 32) {
-      const int f = base + lane;
+    auto fetch = [&](int f, float4& p, float4& w) {  // source f of the unit (padding past the end)
       while (f >= rbase + run.y && r + 1 < U.z) {
         rbase += run.y;
         ++r;
         run = runs[r];
       }
       const bool ok = f < nsrc;
-      sP[warp][lane] = ok ? pos4[run.x + (f - rbase)] : JB_PAD4;
-      sW[warp][lane] = ok ? w4[run.x + (f - rbase)] : make_float4(0.f, 0.f, 0.f, 0.f);
+      p = ok ? pos4[run.x + (f - rbase)] : JB_PAD4;
+      w = ok ? w4[run.x + (f - rbase)] : make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    float4 qp = JB_PAD4, qw = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (nsrc > 0) fetch(lane, qp, qw);
+    for (int base = 0; base < nsrc; base += 32) {
+      sP[warp][lane] = qp;
+      sW[warp][lane] = qw;
       __syncwarp();
+      if (base + 32 < nsrc) fetch(base + 32 + lane, qp, qw);  // the next chunk, while this one is used
 #pragma unroll 8
       for (int q = 0; q < 32; ++q) adj_near_pair(tk, wk, sP[warp][q], sW[warp][q], eps2, base + q >= nsrc, a);
       __syncwarp();
