@@ -820,12 +820,13 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
   const int2 ax = aux[u];
   const int2 rg = ranges[num_internal + U.x];
   const int nt = rg.y - rg.x + 1;
+  // the weighted form takes 1/r from rsqrt_ftz as the pass's near field does
   if (nt <= 8)
-    leaf_unit<4, KAHAN, POT, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
+    leaf_unit<4, KAHAN, POT, W, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
   else if (nt <= 16)
-    leaf_unit<2, KAHAN, POT, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
+    leaf_unit<2, KAHAN, POT, W, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
   else
-    leaf_unit<1, KAHAN, POT, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
+    leaf_unit<1, KAHAN, POT, W, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
 }
 
 // ---------------------------------------------------------------------------
