@@ -441,6 +441,7 @@ def main() -> None:
         cs.wait_first()
         ms_plain, stage_plain = timed(passes["plain"], args.steps)
         ms_split, stage_split = timed(passes["split_bf16"], args.steps)
+        passes["split_bf16"].check_tc_status()  # a timed-out MMA barrier voids the form's numbers
         ms_chosen, stage_chosen = timed(passes["chosen"], args.steps)
     clocks = cs.summary()
 

@@ -61,6 +61,14 @@ enum {
   JB_P2P_NEAR_ONLY = 8  /* jb_leaf_eval: the near field (P2P) alone, no L2P */
 };
 
+/* Most particles one leaf may hold in the leaf kernels (jb_leaf_eval*,
+ * jb_adj_near).  Bits of the leaf error word (jb_leaf_eval_errors). */
+#define JB_MAX_LEAF_OCCUPANCY 32
+enum {
+  JB_LEAF_ERR_OCCUPANCY = 1, /* a unit's leaf holds more than JB_MAX_LEAF_OCCUPANCY particles: skipped */
+  JB_LEAF_ERR_SLOT = 2       /* a partial-row slot at or beyond the slot count: not written / not read */
+};
+
 /* ------------------------------------------------------------------------ */
 /* Host-side prepare: tree + interaction lists (stand-in for yggdrax).      */
 /* ------------------------------------------------------------------------ */
@@ -203,6 +211,15 @@ JB_API int jb_validate_lists(int num_nodes, int num_internal, const int* left, c
                              const int64_t* near_off, const int* near_src, int64_t num_near,
                              int* bad_count_dev, void* stream);
 
+/* Leaf-occupancy precondition of the leaf kernels: writes to *bad_count_dev
+ * (int32, device) the number of leaves whose inclusive node range is empty,
+ * reversed or holds more than max_occupancy particles (max_occupancy in
+ * [1, JB_MAX_LEAF_OCCUPANCY]).  No reference counterpart: yggdrax's leaf
+ * blocks are padded to the tree's max leaf size by construction
+ * (nearfield/_schedules.py:271). */
+JB_API int jb_validate_leaves(int num_nodes, int num_internal, const int* node_ranges, int max_occupancy,
+                              int* bad_count_dev, void* stream);
+
 /* Upward sweep, leaf stage: COM centre (yggdrax compute_tree_mass_moments,
  * upward/real_tree_expansions.py:439) and P2M (:89-213, p2m_real_direct,
  * operators/real_p2m_l2p.py:51) for every leaf.  Writes centers[leaf] and
@@ -296,7 +313,11 @@ JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* 
  * slot < 0: writes out_acc4 for the leaf's particles; slot >= 0: writes 32
  * float4 at partials[32*slot] (scratch), then split int4[num_split] = (leaf,
  * first slot, slot count, 0) is summed into out_acc4.  out_acc4[i] = (ax, ay,
- * az, potential) in sorted order; p2p_mode is a JB_P2P_* flag set. */
+ * az, potential) in sorted order; p2p_mode is a JB_P2P_* flag set.
+ * Preconditions: every leaf a unit names holds at most JB_MAX_LEAF_OCCUPANCY
+ * particles (check once with jb_validate_leaves; a unit breaking it writes
+ * nothing and sets JB_LEAF_ERR_OCCUPANCY), and partials holds 32 float4 per
+ * slot for every slot in aux / split. */
 /* jb_leaf_eval with every particle pair scaled by
  * level_weights[max(rung_i, rung_j)] (rung: int32 per SORTED particle,
  * clamped to [0, num_level_weights); num_level_weights <= 32; device
@@ -313,20 +334,31 @@ JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal
                         const float* locals, float G, float eps2, float* out_acc4, float* partials, int num_split,
                         const int* split, void* stream);
 
+/* Reads the leaf error word of the current device (JB_LEAF_ERR_* bits set by
+ * jb_leaf_eval, jb_leaf_eval_weighted and jb_leaf_eval_noalloc launches so
+ * far) into *flags after the work queued on `stream` has finished, and clears
+ * it when `clear` is nonzero.  Synchronises the stream.  No reference
+ * counterpart (the reference raises at trace time instead). */
+JB_API int jb_leaf_eval_errors(int* flags, int clear, void* stream);
+
 /* jb_leaf_eval for callers that cannot allocate device memory: no reference
  * counterpart (the reference's XLA runtime owns all buffers).  A jax.ffi /
  * XLA custom-call handler only receives the buffers XLA planned for it and
  * must not cudaMalloc in the middle of XLA's asynchronous schedule, and code
  * running under CUDA stream capture may not cudaMalloc at all; both can still
  * pass inputs and outputs.  Same arguments as jb_leaf_eval except that
- * `partials` is replaced by num_slots (1 + the largest slot in aux / split,
- * the schedule's slot count): the scratch is a static device array of
- * JB_LEAF_EVAL_NOALLOC_MAX_SLOTS x 32 float4 (16 MiB) that every GPU loading
- * the library holds until exit.  num_slots above the maximum returns
- * JB_ERR_WORKSPACE.  Allocates nothing.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU (different streams, no ordering between them) race. */
+ * `partials` is replaced by num_slots, which must be at least 1 + the largest
+ * slot in aux and split (the schedule's slot count): the scratch is a static
+ * device array of JB_LEAF_EVAL_NOALLOC_MAX_SLOTS x 32 float4 (16 MiB) that
+ * every GPU loading the library holds until exit.  num_slots above the
+ * maximum returns JB_ERR_WORKSPACE; a slot at or beyond num_slots is neither
+ * written nor read and sets JB_LEAF_ERR_SLOT (jb_leaf_eval_errors).  Leaves
+ * as jb_leaf_eval (at most JB_MAX_LEAF_OCCUPANCY particles).  Allocates
+ * nothing.  The first call on a device (and the first after the device's
+ * context was reset) looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (different
+ * streams, no ordering between them) race. */
 #define JB_LEAF_EVAL_NOALLOC_MAX_SLOTS 32768
 JB_API int jb_leaf_eval_noalloc(int p, int p2p_mode, const float* pos4, int num_internal, int num_units,
                                 const int* units, const int* aux, const int* runs, const int* node_ranges,

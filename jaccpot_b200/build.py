@@ -45,9 +45,8 @@ def _cxx() -> str:
 
 
 def _deps(src: Path) -> list[Path]:
-    return [src, CSRC / "fmm_ops.cuh", CSRC / "fmm_kernels.cuh", CSRC / "generated" / "bu_tables.h",
-            CSRC / "generated" / "kfold_tables.h", CSRC / "generated" / "tc_plans.h", CSRC / "generated" / "bu_code.h",
-            INCLUDE / "jaccpot_b200.h", CSRC / "tree_build.h", CSRC / "tcgen05_m2l.cuh"]
+    return [src, *sorted(CSRC.glob("*.cuh")), *sorted((CSRC / "generated").glob("*.h")),
+            INCLUDE / "jaccpot_b200.h", CSRC / "tree_build.h"]
 
 
 def _stale(obj: Path, deps: list[Path]) -> bool:

@@ -1,4 +1,5 @@
 // C-ABI entry points (include/jaccpot_b200.h) and the order-independent kernels.
+#include "device_symbol.cuh"
 #include "fmm_adjoint.cuh"
 
 #include <mutex>
@@ -16,6 +17,20 @@ int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return JB_OK;
   snprintf(g_err, sizeof(g_err), "%s", cudaGetErrorString(e));
   return JB_ERR_CUDA;
+}
+
+// Leaf error word (JB_LEAF_ERR_* bits) of each device, set by the leaf
+// kernels when a precondition is broken, read by jb_leaf_eval_errors.
+static __device__ int g_leaf_err;
+static SymbolCache g_leaf_err_cache;
+
+int leaf_error_word(int** out) {
+  void* p = nullptr;
+  const cudaError_t e = cached_symbol_address(
+      g_leaf_err_cache, [](void** q) { return cudaGetSymbolAddress(q, g_leaf_err); }, &p);
+  if (e != cudaSuccess) return cuda_status(e);
+  *out = static_cast<int*>(p);
+  return JB_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -66,6 +81,19 @@ __global__ void k_validate(int num_nodes, int num_internal, const int* left, con
   for (int64_t i = tid; i <= num_leaves; i += stride) {
     if (near_off[i] < 0 || near_off[i] > num_near) ++b;
     if (i > 0 && near_off[i] < near_off[i - 1]) ++b;
+  }
+  if (b) atomicAdd(bad, b);
+}
+
+__global__ void k_validate_leaves(int num_nodes, int num_internal, const int2* __restrict__ ranges, int max_occ,
+                                  int* bad) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int b = 0;
+  for (int64_t i = num_internal + tid; i < num_nodes; i += stride) {
+    const int2 r = ranges[i];
+    const int64_t cnt = (int64_t)r.y - r.x + 1;
+    if (r.x < 0 || cnt < 1 || cnt > max_occ) ++b;
   }
   if (b) atomicAdd(bad, b);
 }
@@ -207,6 +235,7 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_adj_near(
   const int2 ax = aux[u];
   const int2 rg = ranges[num_internal + U.x];
   const int nt = rg.y - rg.x + 1;
+  if (nt > kMaxLeaf) return;  // a split leaf's partial row holds kMaxLeaf targets (jb_validate_leaves)
   float a[4] = {0.f, 0.f, 0.f, 0.f};
   // targets beyond 32 particles take further passes
   for (int t0 = 0; t0 < nt; t0 += 32) {
@@ -254,7 +283,7 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_adj_near(
     if (active) {
       const float4 res = make_float4(G * a[0], G * a[1], G * a[2], G * a[3]);
       if (ax.x < 0) out[rg.x + tl] = res;
-      else partial[(size_t)ax.x * 32 + tl] = res;
+      else partial[(size_t)ax.x * kMaxLeaf + tl] = res;
     }
   }
 }
@@ -339,6 +368,29 @@ JB_API int jb_validate_lists(int num_nodes, int num_internal, const int* left, c
   k_validate<<<148 * 4, 256, 0, ST(stream)>>>(num_nodes, num_internal, left, right, far_off, far_src, num_far, near_off,
                                               near_src, num_near, bad_count_dev);
   return launch_status();
+}
+
+JB_API int jb_validate_leaves(int num_nodes, int num_internal, const int* node_ranges, int max_occupancy,
+                              int* bad_count_dev, void* stream) {
+  if (num_nodes < 1 || num_internal < 0 || num_internal >= num_nodes || !node_ranges || !bad_count_dev ||
+      max_occupancy < 1 || max_occupancy > kMaxLeaf)
+    return JB_ERR_ARG;
+  const cudaError_t e = cudaMemsetAsync(bad_count_dev, 0, sizeof(int), ST(stream));
+  if (e != cudaSuccess) return cuda_status(e);
+  k_validate_leaves<<<148 * 4, 256, 0, ST(stream)>>>(num_nodes, num_internal, reinterpret_cast<const int2*>(node_ranges),
+                                                     max_occupancy, bad_count_dev);
+  return launch_status();
+}
+
+JB_API int jb_leaf_eval_errors(int* flags, int clear, void* stream) {
+  if (!flags) return JB_ERR_ARG;
+  int* w = nullptr;
+  int rc = leaf_error_word(&w);
+  if (rc != JB_OK) return rc;
+  cudaError_t e = cudaMemcpyAsync(flags, w, sizeof(int), cudaMemcpyDeviceToHost, ST(stream));
+  if (e == cudaSuccess && clear) e = cudaMemsetAsync(w, 0, sizeof(int), ST(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ST(stream));
+  return cuda_status(e);
 }
 
 JB_API int jb_direct_f64(int64_t n, const float* pos4, int64_t num_targets, const int* targets_sorted, double G,
@@ -498,9 +550,12 @@ JB_API int jb_leaf_eval_weighted(int p, int p2p_mode, const float* pos4, const i
     return JB_ERR_ARG;
   if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL | JB_P2P_FAR_ONLY | JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
   if ((p2p_mode & JB_P2P_FAR_ONLY) && (p2p_mode & JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
+  int* err = nullptr;
+  const int rc = leaf_error_word(&err);
+  if (rc != JB_OK) return rc;
   return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, num_units, units, aux, runs, node_ranges, centers,
                                locals, G, eps2, out_acc4, partials, num_split, split, ST(stream), rung,
-                               level_weights, num_level_weights);
+                               level_weights, num_level_weights, false, 0x7fffffff, err);
 }
 
 JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal, int num_units, const int* units,
@@ -513,9 +568,12 @@ JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal
     return JB_ERR_ARG;
   if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL | JB_P2P_FAR_ONLY | JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
   if ((p2p_mode & JB_P2P_FAR_ONLY) && (p2p_mode & JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
+  int* err = nullptr;
+  const int rc = leaf_error_word(&err);
+  if (rc != JB_OK) return rc;
   return dispatch<RunLeafEval>(p, p2p_mode, pos4, num_internal, num_units, units, aux, runs, node_ranges, centers,
                                locals, G, eps2, out_acc4, partials, num_split, split, ST(stream), nullptr, nullptr,
-                               1, jb::g_leaf_flat != 0);
+                               1, jb::g_leaf_flat != 0, 0x7fffffff, err);
 }
 
 JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int* node_ranges, const float* centers,
@@ -551,7 +609,7 @@ JB_API int jb_adj_near(const float* pos4, const float* w4, int num_internal, int
   if (num_split > 0) {
     k_leaf_reduce<false><<<blocks_1d((int64_t)num_split * 32, 256), 256, 0, ST(stream)>>>(
         num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(node_ranges),
-        reinterpret_cast<const float4*>(partials), reinterpret_cast<float4*>(out_xm4));
+        reinterpret_cast<const float4*>(partials), reinterpret_cast<float4*>(out_xm4), 0x7fffffff, nullptr);
     return launch_status();
   }
   return JB_OK;

@@ -40,6 +40,17 @@ extern int g_split_max_parents[2];
 extern int g_leaf_flat;
 inline int launch_status() { return cuda_status(cudaGetLastError()); }
 
+// Most particles a leaf may hold: the near-field kernels give each target of
+// a leaf one lane (or a lane group) of a warp and each split leaf one
+// partial row of kMaxLeaf float4.  A unit whose leaf holds more writes
+// nothing and sets JB_LEAF_ERR_OCCUPANCY in the error word; a partial-row
+// slot at or beyond the caller's slot count is skipped and sets
+// JB_LEAF_ERR_SLOT (jb_leaf_eval_errors reads the word).
+constexpr int kMaxLeaf = 32;
+__device__ __forceinline__ void leaf_error(int* err, int bit) {
+  if (err) atomicOr(err, bit);
+}
+
 // ---------------------------------------------------------------------------
 // P2M (+ leaf COM).
 // ---------------------------------------------------------------------------
@@ -729,12 +740,12 @@ __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h
   }
 }
 
-template <int G, bool KAHAN, bool POT, bool W = false, bool FTZ = false>
+template <int G, bool KAHAN, bool POT, bool W, bool FTZ>
 __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
                                           const int2* __restrict__ runs, NearStage& sP, int lane, float G_,
                                           float eps2, float4* __restrict__ out, float4* __restrict__ partial,
-                                          const int* __restrict__ rung = nullptr, const float* tbl = nullptr,
-                                          int nlw = 1) {
+                                          int max_slots, int* err, const int* __restrict__ rung = nullptr,
+                                          const float* tbl = nullptr, int nlw = 1) {
   const int tl = lane / G, h = lane % G;
   const int nt = rg.y - rg.x + 1;
   const bool active = tl < nt;
@@ -790,8 +801,10 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
     if (aux.x < 0) {
       const float4 f = out[rg.x + tl];  // the far field k_leaf_l2p wrote
       out[rg.x + tl] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
+    } else if (aux.x < max_slots) {
+      partial[(size_t)aux.x * kMaxLeaf + tl] = res;
     } else {
-      partial[(size_t)aux.x * 32 + tl] = res;
+      leaf_error(err, JB_LEAF_ERR_SLOT);
     }
   }
 }
@@ -801,12 +814,13 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
 //
 // W: the block-step weighted form of the mutual lane -- every pair scaled by
 // lw[max(rung_i, rung_j)] (rung: per sorted particle, lw: nlw <= 32 weights).
-template <bool KAHAN, bool POT, bool W = false>
+// FTZ: 1/r from rsqrt_ftz (the pass's forms all use it; false gives rsqrtf).
+template <bool KAHAN, bool POT, bool W = false, bool FTZ = true>
 static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_leaf_units(
     const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
     const int2* __restrict__ aux, const int2* __restrict__ runs, const int2* __restrict__ ranges, float G,
-    float eps2, float4* __restrict__ out, float4* __restrict__ partial, const int* __restrict__ rung = nullptr,
-    const float* __restrict__ lw = nullptr, int nlw = 1) {
+    float eps2, float4* __restrict__ out, float4* __restrict__ partial, int max_slots, int* err,
+    const int* __restrict__ rung = nullptr, const float* __restrict__ lw = nullptr, int nlw = 1) {
   __shared__ NearStage sP[kWarpsPerBlock];
   __shared__ float tbl[32];
   if (W) {
@@ -820,13 +834,19 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
   const int2 ax = aux[u];
   const int2 rg = ranges[num_internal + U.x];
   const int nt = rg.y - rg.x + 1;
-  // the weighted form takes 1/r from rsqrt_ftz as the pass's near field does
+  if (nt > kMaxLeaf) {
+    if (lane == 0) leaf_error(err, JB_LEAF_ERR_OCCUPANCY);
+    return;
+  }
   if (nt <= 8)
-    leaf_unit<4, KAHAN, POT, W, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
+    leaf_unit<4, KAHAN, POT, W, FTZ>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
+                                     rung, tbl, nlw);
   else if (nt <= 16)
-    leaf_unit<2, KAHAN, POT, W, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
+    leaf_unit<2, KAHAN, POT, W, FTZ>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
+                                     rung, tbl, nlw);
   else
-    leaf_unit<1, KAHAN, POT, W, W>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, rung, tbl, nlw);
+    leaf_unit<1, KAHAN, POT, W, FTZ>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
+                                     rung, tbl, nlw);
 }
 
 // ---------------------------------------------------------------------------
@@ -928,7 +948,8 @@ __device__ __forceinline__ void flat_add(FlatStage& S, int t, float4 v) {
 template <bool KAHAN, bool POT>
 __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
                                                const int2* __restrict__ runs, FlatStage& S, int lane, float G_,
-                                               float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
+                                               float eps2, float4* __restrict__ out, float4* __restrict__ partial,
+                                               int max_slots, int* err) {
   const int nt = rg.y - rg.x + 1;  // 17..32
   const bool tgt = lane < nt;
   const float4 me = tgt ? pos4[rg.x + lane] : JB_PAD4;
@@ -1029,8 +1050,10 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
     if (aux.x < 0) {
       const float4 f = out[rg.x + lane];  // the far field k_leaf_l2p wrote
       out[rg.x + lane] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
+    } else if (aux.x < max_slots) {
+      partial[(size_t)aux.x * kMaxLeaf + lane] = res;
     } else {
-      partial[(size_t)aux.x * 32 + lane] = res;
+      leaf_error(err, JB_LEAF_ERR_SLOT);
     }
   }
 }
@@ -1042,7 +1065,7 @@ template <bool KAHAN, bool POT>
 static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_leaf_units_flat(
     const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
     const int2* __restrict__ aux, const int2* __restrict__ runs, const int2* __restrict__ ranges, float G,
-    float eps2, float4* __restrict__ out, float4* __restrict__ partial) {
+    float eps2, float4* __restrict__ out, float4* __restrict__ partial, int max_slots, int* err) {
   __shared__ WarpStage sW[kWarpsPerBlock];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int u = blockIdx.x * kWarpsPerBlock + warp;
@@ -1051,12 +1074,18 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
   const int2 ax = aux[u];
   const int2 rg = ranges[num_internal + U.x];
   const int nt = rg.y - rg.x + 1;
+  if (nt > kMaxLeaf) {
+    if (lane == 0) leaf_error(err, JB_LEAF_ERR_OCCUPANCY);
+    return;
+  }
   if (nt <= 8)
-    leaf_unit<4, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
+    leaf_unit<4, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial, max_slots,
+                                          err);
   else if (nt <= 16)
-    leaf_unit<2, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial);
+    leaf_unit<2, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial, max_slots,
+                                          err);
   else
-    leaf_unit_flat<KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].f, lane, G, eps2, out, partial);
+    leaf_unit_flat<KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].f, lane, G, eps2, out, partial, max_slots, err);
 }
 
 // Far field (L2P) of every leaf: warp per leaf (its unit with flags & 1),
@@ -1077,6 +1106,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
   if (u >= num_units || !(aux[u].y & 1)) return;
   const int node = num_internal + units[u].x;
   const int2 rg = ranges[node];
+  if (rg.y - rg.x + 1 > kMaxLeaf) return;  // refused by the near-field kernel, which flags it
   const bool act = rg.x + lane <= rg.y;
   if (zero) {  // near field alone: the sums start from zero
     if (act) out[rg.x + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1101,16 +1131,21 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
 template <bool ACCUM>
 static __global__ void __launch_bounds__(256) k_leaf_reduce(int num_split, const int4* __restrict__ split, int num_internal,
                                                      const int2* __restrict__ ranges, const float4* __restrict__ partial,
-                                                     float4* __restrict__ out) {
+                                                     float4* __restrict__ out, int max_slots, int* err) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (int)(t >> 5), l = (int)(t & 31);
   if (i >= num_split) return;
   const int4 sp = split[i];
   const int2 rg = ranges[num_internal + sp.x];
+  if (rg.y - rg.x + 1 > kMaxLeaf) return;  // flagged by the near-field kernel
+  if (sp.y < 0 || sp.z < 0 || (int64_t)sp.y + sp.z > max_slots) {
+    if (l == 0) leaf_error(err, JB_LEAF_ERR_SLOT);
+    return;
+  }
   if (rg.x + l > rg.y) return;
   float4 a = ACCUM ? out[rg.x + l] : make_float4(0.f, 0.f, 0.f, 0.f);
   for (int q = 0; q < sp.z; ++q) {
-    const float4 v = partial[(size_t)(sp.y + q) * 32 + l];
+    const float4 v = partial[(size_t)(sp.y + q) * kMaxLeaf + l];
     a.x += v.x;
     a.y += v.y;
     a.z += v.z;
@@ -1257,10 +1292,11 @@ struct RunLeafEval {
   template <bool K, bool PT>
   static void go(unsigned nb, cudaStream_t st, const float4* pos4, int num_internal, int num_units, const int4* units,
                  const int2* aux, const int2* runs, const int2* ranges, float G, float eps2, float4* out,
-                 float4* partial, const int* rung, const float* lw, int nlw, bool flat) {
+                 float4* partial, const int* rung, const float* lw, int nlw, bool flat, int max_slots, int* err) {
     if (rung)
       k_leaf_units<K, PT, true><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs,
-                                                                    ranges, G, eps2, out, partial, rung, lw, nlw);
+                                                                    ranges, G, eps2, out, partial, max_slots, err,
+                                                                    rung, lw, nlw);
     else if (flat) {
       // 15 KB of shared memory per block: ask for a carveout that holds the
       // eight blocks per SM the launch bounds allow.
@@ -1268,16 +1304,17 @@ struct RunLeafEval {
           cudaFuncSetAttribute(k_leaf_units_flat<K, PT>, cudaFuncAttributePreferredSharedMemoryCarveout, 60);
       (void)carve;
       k_leaf_units_flat<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs,
-                                                                   ranges, G, eps2, out, partial);
+                                                                   ranges, G, eps2, out, partial, max_slots, err);
     }
     else
       k_leaf_units<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs, ranges,
-                                                              G, eps2, out, partial);
+                                                              G, eps2, out, partial, max_slots, err);
   }
   static int run(int mode, const float* pos4, int num_internal, int num_units, const int* units, const int* aux,
                  const int* runs, const int* ranges, const float* centers, const float* locals, float G, float eps2,
                  float* out, float* partial, int num_split, const int* split, cudaStream_t st,
-                 const int* rung = nullptr, const float* lw = nullptr, int nlw = 1, bool flat = false) {
+                 const int* rung = nullptr, const float* lw = nullptr, int nlw = 1, bool flat = false,
+                 int max_slots = 0x7fffffff, int* err = nullptr) {
     if (num_units > 0) {
       const unsigned nb = blocks_for(num_units, kWarpsPerBlock);
       auto a0 = reinterpret_cast<const float4*>(pos4);
@@ -1295,17 +1332,17 @@ struct RunLeafEval {
       if (rc) return rc;
       if (far_only) return JB_OK;
       const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
-      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
-      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
-      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
-      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat);
+      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
+      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
+      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
+      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
       rc = launch_status();
       if (rc) return rc;
     }
     if (num_split > 0) {
       k_leaf_reduce<true><<<blocks_for((int64_t)num_split * 32, 256), 256, 0, st>>>(
           num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(ranges),
-          reinterpret_cast<const float4*>(partial), reinterpret_cast<float4*>(out));
+          reinterpret_cast<const float4*>(partial), reinterpret_cast<float4*>(out), max_slots, err);
       return launch_status();
     }
     return JB_OK;

@@ -10,10 +10,9 @@
 // them this file holds that scratch in a fixed-size device array that every
 // GPU loading the library keeps until the process exits.
 //
-// The kernels are the ones jb_leaf_eval launches; only the scratch pointer
-// differs.
-#include <mutex>
-
+// The kernels are the ones jb_leaf_eval launches (the same near-field form,
+// so the results are equal bit for bit); only the scratch pointer differs.
+#include "device_symbol.cuh"
 #include "fmm_adjoint.cuh"
 
 #define JB_ORDERS_NA(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
@@ -22,30 +21,17 @@ JB_ORDERS_NA(JB_DECLARE_ORDER)
 namespace {
 
 // 32768 slots x 32 particles x float4 = 16 MiB per device.
-constexpr int64_t kSlotElems = 32;
-static __device__ __align__(256) float4 g_leaf_scratch[(int64_t)JB_LEAF_EVAL_NOALLOC_MAX_SLOTS * kSlotElems];
+static __device__ __align__(256) float4 g_leaf_scratch[(int64_t)JB_LEAF_EVAL_NOALLOC_MAX_SLOTS * jb::kMaxLeaf];
 
-constexpr int kMaxDevices = 128;
-std::mutex g_scratch_mu;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
+jb::SymbolCache g_scratch_cache;
 
-// Device address of g_leaf_scratch on the current device.  In host code the
-// array's name is only a host-side handle, so the address is looked up once
-// per device (with that device current) and cached.
+// Device address of g_leaf_scratch on the current device: in host code the
+// array's name is only a host-side handle, so the address is looked up with
+// that device current, once per device and context, and cached.
 int scratch_address(void** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return jb::cuda_status(e);
-  if (dev < 0 || dev >= kMaxDevices) return JB_ERR_ARG;
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (g_scratch_addr[dev] == nullptr) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_leaf_scratch);
-    if (e != cudaSuccess) return jb::cuda_status(e);
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
-  return JB_OK;
+  const cudaError_t e = jb::cached_symbol_address(
+      g_scratch_cache, [](void** p) { return cudaGetSymbolAddress(p, g_leaf_scratch); }, out);
+  return e == cudaSuccess ? JB_OK : jb::cuda_status(e);
 }
 
 template <template <int> class F, typename... A>
@@ -76,11 +62,17 @@ extern "C" JB_API int jb_leaf_eval_noalloc(int p, int p2p_mode, const float* pos
   if (p < 1 || p > JB_MAX_ORDER) return JB_ERR_ORDER;
   if (num_slots > JB_LEAF_EVAL_NOALLOC_MAX_SLOTS) return JB_ERR_WORKSPACE;
   // Every scratch row that the reduce reads is written earlier in the same
-  // call, so nothing needs clearing between calls.
+  // call, so nothing needs clearing between calls; slots at or beyond
+  // num_slots are neither written nor read (JB_LEAF_ERR_SLOT).
   void* scratch = nullptr;
-  const int rc = scratch_address(&scratch);
+  int rc = scratch_address(&scratch);
+  if (rc != JB_OK) return rc;
+  int* err = nullptr;
+  rc = jb::leaf_error_word(&err);
   if (rc != JB_OK) return rc;
   return dispatch_order<jb::RunLeafEval>(p, p2p_mode, pos4, num_internal, num_units, units, aux, runs, node_ranges,
                                          centers, locals, G, eps2, out_acc4, static_cast<float*>(scratch),
-                                         num_split, split, reinterpret_cast<cudaStream_t>(stream));
+                                         num_split, split, reinterpret_cast<cudaStream_t>(stream),
+                                         (const int*)nullptr, (const float*)nullptr, 1, jb::g_leaf_flat != 0,
+                                         num_slots, err);
 }

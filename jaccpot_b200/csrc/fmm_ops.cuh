@@ -147,12 +147,12 @@ __device__ __forceinline__ void rot_mult_to_z(float* v, const Trig<P>& taz, cons
   bu_apply<P, false, false, false>(v);
 }
 
-// 1/sqrt(x) by the approximate special-function instruction with subnormal
-// inputs and results flushed to zero: rsqrtf() adds a range test and two
-// multiplies around the same instruction so that subnormal inputs keep their
-// value; for normal inputs the two agree bit for bit.  A squared distance
-// below 2^-126 (points closer than about 1e-19) reads as 0 here (infinite
-// 1/r, as for coincident points).
+// 1/sqrt(x) by the PTX instruction rsqrt.approx.ftz.f32 (the approximate
+// reciprocal square root with subnormal inputs and results flushed to zero).
+// For squared distances in the normal FP32 range its results equal rsqrtf()'s
+// bit for bit (tests/test_gpu_leaf_form.py compares the two forms).  A squared
+// distance below 2^-126 (points closer than about 1e-19) reads as 0 here
+// (infinite 1/r, as for coincident points).
 __device__ __forceinline__ float rsqrt_ftz(float x) {
   float r;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));

@@ -18,8 +18,10 @@
 // runs of equal target (the far list is sorted by target) are summed by
 // column; targets whose whole list lies in one tile write their local row,
 // the others write scratch rows that k_m2l_reduce sums in slot order.  Every
-// wait on the MMA barrier is bounded: on timeout the kernel records a status
-// word, drains its outstanding commit (bounded), frees TMEM and returns.
+// wait on the MMA barrier is bounded: on timeout the kernel records status 1,
+// drains its outstanding commit (bounded), frees TMEM and returns; status 2
+// means the drain timed out as well (the TMEM was released while an MMA may
+// still write it: the context is not to be used further).
 #include <cuda_bf16.h>
 
 #include "fmm_kernels.cuh"
@@ -360,9 +362,11 @@ __global__ void __launch_bounds__(kThreads) k_m2l_tc(int num_tiles, int64_t num_
   }
 
   if (aborted) {
-    if (tid == 0) atomicExch(status, 1);
-    // drain the outstanding commit before TMEM is released (bounded as well)
-    if (pending) (void)mbar_wait(mbar, phase);
+    if (tid == 0) atomicMax(status, 1);
+    // drain the outstanding commit before TMEM is released (bounded as well);
+    // status 2: the drain timed out too, so the MMA may still be writing the
+    // TMEM freed below and the context must be treated as unusable
+    if (pending && !mbar_wait(mbar, phase) && tid == 0) atomicMax(status, 2);
     fence_before();
   }
   __syncthreads();
@@ -556,8 +560,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_m2l_tc_units(int num_units, con
     }
   }
   if (aborted) {
-    if (tid == 0) atomicExch(status, 1);
-    if (pending) (void)mbar_wait(mbar, phase);
+    if (tid == 0) atomicMax(status, 1);
+    if (pending && !mbar_wait(mbar, phase) && tid == 0) atomicMax(status, 2);  // as in k_m2l_tc
   }
   fence_before();
   __syncthreads();

@@ -36,6 +36,8 @@ struct jb_dsched {
 
 namespace {
 
+constexpr int kMaxLeafOcc = JB_MAX_LEAF_OCCUPANCY;
+
 inline int bits_for(int64_t v) {  // bits to hold values in [0, v)
   int b = 1;
   while (b < 62 && ((int64_t)1 << b) < v) ++b;
@@ -346,6 +348,14 @@ __global__ void k_leaf_split(int NL, int lo, const int* __restrict__ n_per, cons
   if (j < NL && n_per[j] > 1) split[spos[j]] = make_int4(lo + j, slot_base[j], n_per[j], 0);
 }
 
+// Largest leaf occupancy in [lo, hi) (atomicMax into *occ, zeroed first).
+__global__ void k_leaf_max_occ(const int* __restrict__ ranges, int num_internal, int lo, int hi, int* __restrict__ occ) {
+  const int j = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= hi) return;
+  const int n = num_internal + j;
+  atomicMax(occ, ranges[2 * n + 1] - ranges[2 * n] + 1);
+}
+
 void build_leaf(jb_dsched& d, int num_internal, const int* ranges, const int64_t* near_off, const int* near_src, int lo,
                 int hi, int max_sources, cudaStream_t st) {
   Scratch s;
@@ -353,6 +363,13 @@ void build_leaf(jb_dsched& d, int num_internal, const int* ranges, const int64_t
   int* d_tot = tot32(s);
   int64_t* d_tot64 = s.total.as<int64_t>();
   const int NL = hi - lo;
+  // the leaf kernels hold at most kMaxLeafOcc targets per leaf: refuse more
+  if (NL > 0) {
+    ck(cudaMemsetAsync(d_tot, 0, sizeof(int), st));
+    k_leaf_max_occ<<<nblocks(NL, 256), 256, 0, st>>>(ranges, num_internal, lo, hi, d_tot);
+    ck_launch();
+    if (read_word(d_tot, st) > kMaxLeafOcc) throw Fail{JB_ERR_ARG};
+  }
   int64_t ends[2] = {0, 0};
   ck(cudaMemcpyAsync(&ends[0], near_off + lo, 8, cudaMemcpyDeviceToHost, st));
   ck(cudaMemcpyAsync(&ends[1], near_off + hi, 8, cudaMemcpyDeviceToHost, st));

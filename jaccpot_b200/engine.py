@@ -47,6 +47,8 @@ class DeviceTopology:
         self.right = up(topo.right_child if topo.num_internal else np.zeros(1, np.int32), torch.int32)
         self.far_off = up(topo.far_offsets, torch.int64)
         self.far_src = up(topo.far_sources if topo.num_far_pairs else np.zeros(1, np.int32), torch.int32)
+        # per-far-pair gear tags of an error-controlled walk (None: one order)
+        self.far_gear = None
         self.near_off = up(topo.near_offsets, torch.int64)
         self.near_src = up(topo.near_leaves if topo.num_near_pairs else np.zeros(1, np.int32), torch.int32)
         self.leaf_of = up(topo.leaf_of_particle, torch.int32)
@@ -81,6 +83,13 @@ class DeviceTopology:
         nbad = int(bad.item())
         if nbad:
             raise _lib.JBError(f"topology has {nbad} out-of-range list entries")
+        _lib.check(_lib.lib().jb_validate_leaves(t.num_nodes, t.num_internal, _ptr(self.node_ranges),
+                                                 _lib.JB_MAX_LEAF_OCCUPANCY, _ptr(bad), _stream_handle(None)),
+                   "jb_validate_leaves")
+        nbad = int(bad.item())
+        if nbad:
+            raise _lib.JBError(f"{nbad} leaves hold more than {_lib.JB_MAX_LEAF_OCCUPANCY} particles "
+                               "(or none): the leaf kernels take leaf_size <= 32")
 
 
 @dataclass
@@ -327,6 +336,7 @@ class Pass:
         if self.tc_layout == "units":
             if getattr(self, "_tc_status", None) is None:
                 self._tc_status = torch.zeros(1, device=self.dt.device, dtype=torch.int32)
+            self._tc_status.zero_()  # the word reports this launch only
             ws, sc = self.ws, self.m2l_sched
             _lib.check(self.lib.jb_m2l_split_units(self.p, int(sc.units.shape[0]), _ptr(self.d_m2l_units),
                                                    _ptr(ws.mult), _ptr(ws.centers), _ptr(self.dt.far_src),
@@ -351,6 +361,7 @@ class Pass:
             }
         T, t, ws = self._tc, self.dt.topo, self.ws
         sc = T["sched"]
+        T["status"].zero_()
         _lib.check(self.lib.jb_m2l_split(self.p, self.tc_products, sc.num_tiles, t.num_far_pairs, _ptr(T["pair_tgt"]),
                                          _ptr(self.dt.far_src), _ptr(T["seg_off"]), _ptr(T["segs"]), _ptr(ws.mult),
                                          _ptr(ws.centers), _ptr(ws.locals), _ptr(T["partials"]),
@@ -358,11 +369,27 @@ class Pass:
                    "jb_m2l_split")
 
     def tc_status(self) -> int:
-        """Status word of the tensor-core M2L (0 = ok, 1 = a barrier wait timed out)."""
+        """Status word of the last tensor-core M2L (0 = ok, 1 = a barrier wait
+        timed out and the locals are incomplete, 2 = the drain after it timed
+        out too: the CUDA context is not to be used further).  Reading it
+        synchronises the device."""
         T = getattr(self, "_tc", None)
         st = 0 if T is None else int(T["status"].item())
         U = getattr(self, "_tc_status", None)
-        return st | (0 if U is None else int(U.item()))
+        return max(st, 0 if U is None else int(U.item()))
+
+    def check_tc_status(self) -> None:
+        """Raises JBError when the last tensor-core M2L reported a timeout
+        (see tc_status); a no-op for the FP32 M2L."""
+        if self.m2l_mode != _lib.JB_M2L_SPLIT_BF16:
+            return
+        st = self.tc_status()
+        if st == 1:
+            raise _lib.JBError("tensor-core M2L: an MMA barrier wait timed out; the locals of this pass are "
+                               "incomplete")
+        if st >= 2:
+            raise _lib.JBError("tensor-core M2L: an MMA barrier wait and its drain timed out; the CUDA context "
+                               "must not be used further")
 
     def l2l(self, stream=None) -> None:
         t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)

@@ -153,6 +153,7 @@ class FastMultipoleMethod:
             _gears.apply_gears(ps, model)
         ps.upward()
         ps.downward()
+        ps.check_tc_status()
         st = FMMPreparedState(topology=topo, device_topology=dt, pass_=ps, max_order=int(max_order), theta=th,
                               leaf_size=int(leaf_size), num_particles=int(topo.num_particles),
                               input_dtype=positions.dtype if hasattr(positions, "dtype") else np.float64)

@@ -8,7 +8,8 @@ They were produced with preset="accurate", theta 0.5, softening 1e-2, G 1
 (leaf 8 for the forward cases, leaf 4 for the gradient cases) on inputs drawn
 from jax.random.PRNGKey(0xC0FFEE), which tests/golden/jax_prng.py regenerates.
 
-Usage: python tests/golden/make_fixtures.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_fixtures.py REFERENCE_ROOT
+(REFERENCE_ROOT: the jaccpot checkout holding tests/characterization/.)
 Writes tests/golden/reference_goldens.npz (uniform real-basis cases only).
 """
 
@@ -24,7 +25,7 @@ MODES = ["bkt_uni_real_n256_p4"]
 GRAD = ["uni_real_n128_p2", "uni_real_n128_p4", "uni_real_n256_p4"]
 
 
-def main(ref_root: str = "/root/reference") -> Path:
+def main(ref_root: str) -> Path:
     base = Path(ref_root) / "tests" / "characterization"
     out = {}
     for c in FORWARD:
@@ -43,4 +44,6 @@ def main(ref_root: str = "/root/reference") -> Path:
 
 
 if __name__ == "__main__":
-    print(main(*sys.argv[1:]))
+    if len(sys.argv) != 2:
+        raise SystemExit(__doc__)
+    print(main(sys.argv[1]))

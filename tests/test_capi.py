@@ -52,3 +52,32 @@ def test_argument_errors_without_a_device():
     assert lib.jb_direct_f64(0, None, 0, None, 1.0, 0.0, None, None) == 1
     info = _lib.TreeInfo()
     assert lib.jb_tree_info(None, ctypes.byref(info)) == 1
+
+
+def test_leaf_checks_refuse_bad_arguments_without_a_device():
+    lib = _lib.lib()
+    # max_occupancy outside [1, JB_MAX_LEAF_OCCUPANCY], null arrays
+    assert lib.jb_validate_leaves(3, 1, 1, 33, 1, None) == 1
+    assert lib.jb_validate_leaves(3, 1, 1, 0, 1, None) == 1
+    assert lib.jb_validate_leaves(3, 1, None, 32, 1, None) == 1
+    assert lib.jb_leaf_eval_errors(None, 0, None) == 1
+
+
+def test_tensor_core_status_raises_on_the_host():
+    """The split-BF16 M2L's status word: 1 (a barrier wait timed out) and 2
+    (its drain timed out too) raise; 0 and the FP32 M2L do not."""
+    torch = pytest.importorskip("torch")
+    from jaccpot_b200 import engine
+
+    ps = engine.Pass.__new__(engine.Pass)  # host logic only: no device pass is built
+    ps.m2l_mode = _lib.JB_M2L_SPLIT_BF16
+    ps._tc = None
+    for word, msg in ((1, "incomplete"), (2, "must not be used")):
+        ps._tc_status = torch.tensor([word], dtype=torch.int32)
+        with pytest.raises(_lib.JBError, match=msg):
+            ps.check_tc_status()
+    ps._tc_status = torch.tensor([0], dtype=torch.int32)
+    ps.check_tc_status()
+    ps.m2l_mode = _lib.JB_M2L_FP32
+    ps._tc_status = torch.tensor([1], dtype=torch.int32)
+    ps.check_tc_status()  # the FP32 M2L has no status word
