@@ -5,10 +5,20 @@ Workload: 64-clump Plummer mixture, N = 4,194,304, real basis, order p = 8,
 leaf size 32 (the split-precision configuration the headline metric is quoted
 on).  A step is one evaluation pass over the prepared topology: Morton gather
 of the resident inputs, P2M -> M2M -> M2L -> L2L -> L2P + P2P, un-permute into
-input order.  The host tree build / traversal (prepare) is done once, outside
-the timed region, as in the reference's prepare_state / evaluate split.
+input order.  Prepare (tree, lists, schedules) is done once, outside the
+timed region, as in the reference's prepare_state / evaluate split.
 
-`value` is particles/s of the timed form with inputs resident in HBM; `e2e`
+Forms, each held to p99 relative force error <= 1e-4 against an FP64 direct
+sum (its accuracy parameter chosen in the run on one target sample, errors
+reported on another):
+  chosen  -- the error-controlled walk (the reference's Dehnen eq. 15/16a
+             acceptance, adaptive_error_model="dehnen_paper") with per-pair
+             gears (2, 4, 6, 8), FP32 M2L, Kahan-compensated P2P;
+  plain   -- the theta walk at the maximum order, FP32 M2L and P2P;
+  split_bf16, learned_gears -- reported beside (plain's lists with the
+             tensor-core M2L, or with the MLP-selected gears).
+
+`value` is particles/s of the chosen form with inputs resident in HBM; `e2e`
 is the same metric through the public API (FastMultipoleMethod.
 differentiable_accelerations on the prepared state) from pinned host buffers,
 H2D + pass + D2H inside the timed region.  L2 is flushed (256 MiB write)
@@ -53,6 +63,23 @@ WORKLOAD = {
 }
 ERR_TARGETS = 32768
 ERR_BOUND = 1e-4
+# Each form's accuracy parameter is chosen in the run: the largest value on
+# its grid whose p99 on a selection sample of ERR_TARGETS targets (and on its
+# first 4,096) stays within SELECT_BOUND; errors are then reported on a
+# disjoint sample of the same size.
+SELECT_BOUND = 0.9 * ERR_BOUND
+THETA_GRID = (0.6, 0.59, 0.58, 0.57, 0.56, 0.55, 0.53, 0.5)
+EPS_GRID = (5e-5, 4e-5, 3.5e-5, 3e-5, 2.5e-5, 2e-5, 1.5e-5, 1e-5)
+GEARS = (2, 4, 6, 8)
+
+
+def m2l_flops_per_pair(p: int) -> float:
+    """Algorithmic flops of one rotate+scale M2L at order p: 2 x (two
+    rotation blocks sum (2l+1)^2 + the z-translation terms)."""
+    rot = sum((2 * ell + 1) ** 2 for ell in range(p + 1))
+    zt = sum((2 if m else 1) * sum(1 for a in range(m, p + 1) for b in range(m, p + 1) if a + b <= p)
+             for m in range(p + 1))
+    return 2.0 * (2 * rot + zt)
 
 
 # ---------------------------------------------------------------------------
@@ -340,59 +367,131 @@ def main() -> None:
     cfg = dict(WORKLOAD)
     cfg["N"] = n
     pos, mass = workloads.GENERATORS[cfg["generator"]](n, cfg["seed"])
-    fmm = FastMultipoleMethod(theta=cfg["theta"], G=1.0, softening=0.0, device=dev)
-    t0 = time.perf_counter()
-    state = fmm.prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
-    torch.cuda.synchronize()
-    prep_s = time.perf_counter() - t0
-    topo = state.topology
-    dt = state.device_topology
-
-    # leaf range of this rank (Morton order); ranks > 1 evaluate a slice
-    L = topo.num_leaves
-    leaf_lo, leaf_hi = (L * rank) // world, (L * (rank + 1)) // world
-
-    # plain: FP32 M2L + FP32 P2P at the maximum order.  chosen: the learned
-    # per-pair gears + FP32 M2L + Kahan-compensated P2P.  split_bf16 (reported):
-    # the tensor-core split-BF16 M2L + Kahan P2P at the maximum order.
-    forms = {
-        "plain": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_FP32),
-        "split_bf16": dict(m2l_mode=_lib.JB_M2L_SPLIT_BF16, p2p_mode=_lib.JB_P2P_KAHAN),
-        "chosen": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_KAHAN),
-    }
-    passes = {k: engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, leaf_range=(leaf_lo, leaf_hi), **v)
-              for k, v in forms.items()}
     d_pos = torch.from_numpy(pos).to(dev)
     d_mass = torch.from_numpy(mass).to(dev)
     if world > 1:  # sources replicated from rank 0 (one broadcast), targets sharded
         from jaccpot_b200 import sharding
         sharding.replicate_sources(d_pos, d_mass)
-    # learned gears for the chosen form: chosen once per topology from a plain
-    # pass's force scale (prepare-time, like the reference's gear buckets)
+    stream = torch.cuda.current_stream()
+
+    # FP64 direct-sum references on two disjoint target samples: one chooses
+    # each form's accuracy parameter, the other reports the errors
+    rng = np.random.default_rng(12345)
+    both = rng.choice(n, size=min(2 * ERR_TARGETS, n), replace=False)
+    tg_sel, tg = both[:both.size // 2], both[both.size // 2:]
+    base_topo = tree.build_topology(pos, mass, leaf_size=cfg["leaf_size"], theta=0.6, device=dev)
+    base_pass = engine.Pass(engine.DeviceTopology(base_topo, dev), 1)
+    base_pass.load_particles(d_pos, d_mass)
+
+    def direct_ref(targets):
+        ts = torch.from_numpy(base_topo.inverse_permutation[targets].astype(np.int32)).to(dev)
+        ref = torch.empty((targets.size, 4), device=dev, dtype=torch.float64)
+        _lib.check(_lib.lib().jb_direct_f64(n, base_pass.ws.pos4.data_ptr(), targets.size, ts.data_ptr(), 1.0, 0.0,
+                                            ref.data_ptr(), stream.cuda_stream), "jb_direct_f64")
+        return ref[:, :3].cpu().numpy()
+
+    ref_sel, ref_rep = direct_ref(tg_sel), direct_ref(tg)
+    del base_pass
+
+    def errors_of(acc4_sorted, topo, targets, ref):
+        ts = torch.from_numpy(topo.inverse_permutation[targets].astype(np.int64)).to(dev)
+        got = acc4_sorted[ts, :3].double().cpu().numpy()
+        e = workloads.relative_errors(got, ref)
+        return {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
+                "p99_first_4096": float(np.percentile(e[:4096], 99))}
+
+    def meets(err) -> bool:
+        return err["p99"] <= SELECT_BOUND and err["p99_first_4096"] <= SELECT_BOUND
+
+    # plain: FP32 rotate+scale M2L + FP32 P2P at the maximum order over the
+    # theta walk; theta = the largest of THETA_GRID that meets the bound on the
+    # selection sample (whole-tree passes, identical on every rank)
+    sel = {"bound": SELECT_BOUND, "targets": int(tg_sel.size), "plain": [], "chosen": []}
+    plain_theta = THETA_GRID[-1]
+    for th in THETA_GRID:
+        topo_t = tree.build_topology(pos, mass, leaf_size=cfg["leaf_size"], theta=th, device=dev)
+        ps_t = engine.Pass(engine.DeviceTopology(topo_t, dev), cfg["order"], G=1.0, eps2=0.0)
+        ps_t.load_particles(d_pos, d_mass)
+        e = errors_of(ps_t.run(), topo_t, tg_sel, ref_sel)
+        sel["plain"].append({"theta": th, "p99": e["p99"], "p99_first_4096": e["p99_first_4096"]})
+        del ps_t
+        if meets(e):
+            plain_theta = th
+            break
+    cfg["theta"] = plain_theta
+
+    # chosen: the error-controlled walk (Dehnen eq. 15/16a acceptance, per-pair
+    # gears GEARS) + FP32 M2L + Kahan-compensated P2P, through the public API
+    # (adaptive_error_model="dehnen_paper"); eps = the largest of EPS_GRID that
+    # meets the bound on the selection sample
+    def chosen_solver(eps):
+        return FastMultipoleMethod(theta=0.6, G=1.0, softening=0.0, adaptive_order=True, p_gears=GEARS,
+                                   adaptive_error_model="dehnen_paper", adaptive_eps=eps,
+                                   mac_force_scale_mode="paper", device=dev, nearfield_compensated=True)
+
+    chosen_eps = EPS_GRID[-1]
+    for eps in EPS_GRID:
+        st_e = chosen_solver(eps).prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
+        e = errors_of(st_e.pass_.evaluate(), st_e.topology, tg_sel, ref_sel)
+        sel["chosen"].append({"eps": eps, "p99": e["p99"], "p99_first_4096": e["p99_first_4096"]})
+        del st_e
+        if meets(e):
+            chosen_eps = eps
+            break
+
+    fmm = chosen_solver(chosen_eps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    state = fmm.prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
+    torch.cuda.synchronize()
+    prep_s = time.perf_counter() - t0
+    atopo = state.topology
+    topo = tree.build_topology(pos, mass, leaf_size=cfg["leaf_size"], theta=plain_theta, device=dev)
+    dt = engine.DeviceTopology(topo, dev)
+
+    # leaf range of this rank (Morton order); ranks > 1 evaluate a slice
+    L = topo.num_leaves
+    leaf_lo, leaf_hi = (L * rank) // world, (L * (rank + 1)) // world
+    forms = {
+        "plain": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_FP32),
+        "split_bf16": dict(m2l_mode=_lib.JB_M2L_SPLIT_BF16, p2p_mode=_lib.JB_P2P_KAHAN),
+        "learned_gears": dict(m2l_mode=_lib.JB_M2L_FP32, p2p_mode=_lib.JB_P2P_KAHAN),
+    }
+    passes = {k: engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, leaf_range=(leaf_lo, leaf_hi), **v)
+              for k, v in forms.items()}
+    if world > 1:  # the chosen pass over this rank's Morton range of the adaptive tree
+        La = atopo.num_leaves
+        passes["chosen"] = engine.Pass(state.device_topology, cfg["order"], G=1.0, eps2=0.0,
+                                       p2p_mode=_lib.JB_P2P_KAHAN,
+                                       leaf_range=((La * rank) // world, (La * (rank + 1)) // world))
+        passes["chosen"].set_gears(torch.from_numpy(atopo.far_gears).to(dev), GEARS)
+    else:
+        passes["chosen"] = state.pass_
+    # the learned selector (MLP gears on the theta walk), reported beside:
+    # chosen once per topology from a plain pass's force scale
     from jaccpot_b200 import gears as gear_mod
     gear_info = None
     if gear_mod.DEFAULT_MODEL.exists():
         model = gear_mod.GearModel.load()
-        passes["chosen"].load_particles(d_pos, d_mass)
+        passes["learned_gears"].load_particles(d_pos, d_mass)
         torch.cuda.synchronize()
         g0 = time.perf_counter()
         if world > 1:
-            # the selector reads the force scale of every node, so it runs on a
-            # whole-tree pass; the rank's pass keeps the units of its targets
-            full = engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, **forms["chosen"])
+            full = engine.Pass(dt, cfg["order"], G=1.0, eps2=0.0, **forms["learned_gears"])
             full.load_particles(d_pos, d_mass)
             gsel = gear_mod.apply_gears(full, model)
-            passes["chosen"].set_gears(gsel, model.orders)
+            passes["learned_gears"].set_gears(gsel, model.orders)
             del full
         else:
-            gsel = gear_mod.apply_gears(passes["chosen"], model)
+            gsel = gear_mod.apply_gears(passes["learned_gears"], model)
         torch.cuda.synchronize()
         gear_info = {"select_s": time.perf_counter() - g0, "budget": model.budget,
                      "fraction": (np.bincount(gsel, minlength=len(model.orders)) / max(1, gsel.size)).tolist(),
                      "orders": list(model.orders)}
+    else:
+        del passes["learned_gears"]
     acc_out = torch.empty((n, 3), device=dev, dtype=torch.float32)
     flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
-    stream = torch.cuda.current_stream()
 
     def step(ps: engine.Pass, ev=None):
         if ev is not None:
@@ -414,7 +513,7 @@ def main() -> None:
         if ev is not None:
             ev[5].record(stream)
 
-    def timed(ps: engine.Pass, steps: int, sampler=None):
+    def timed(ps: engine.Pass, steps: int):
         per_step, stage = [], np.zeros(5)
         if world > 1:
             dist.barrier()
@@ -431,18 +530,18 @@ def main() -> None:
             dist.barrier()
         return float(np.mean(per_step)), stage / steps
 
-    results = {}
     for name, ps in passes.items():
         for _ in range(args.warmup):
             step(ps)
         torch.cuda.synchronize()
-    # plain, split-BF16, chosen; clocks sampled over all three timed regions
+    # every form timed in turn; clocks sampled over all timed regions
+    timings = {}
     with ClockSampler(local) as cs:
         cs.wait_first()
-        ms_plain, stage_plain = timed(passes["plain"], args.steps)
-        ms_split, stage_split = timed(passes["split_bf16"], args.steps)
-        passes["split_bf16"].check_tc_status()  # a timed-out MMA barrier voids the form's numbers
-        ms_chosen, stage_chosen = timed(passes["chosen"], args.steps)
+        for name, ps in passes.items():
+            timings[name] = timed(ps, args.steps)
+            if name == "split_bf16":
+                ps.check_tc_status()  # a timed-out MMA barrier voids the form's numbers
     clocks = cs.summary()
 
     def reduce_max(x: float) -> float:
@@ -452,40 +551,33 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    ms_plain = reduce_max(ms_plain)
-    ms_chosen = reduce_max(ms_chosen)
-    ms_split = reduce_max(ms_split)
+    ms = {k: reduce_max(v[0]) for k, v in timings.items()}
+    ms_plain, ms_chosen = ms["plain"], ms["chosen"]
+    stage_chosen, stage_plain = timings["chosen"][1], timings["plain"][1]
 
-    # accuracy of both forms against an FP64 direct sum on sampled targets
-    rng = np.random.default_rng(12345)
-    tg = rng.choice(n, size=min(ERR_TARGETS, n), replace=False)
-    ts = torch.from_numpy(topo.inverse_permutation[tg].astype(np.int32)).to(dev)
-    ref = torch.empty((tg.size, 4), device=dev, dtype=torch.float64)
-    ps0 = passes["chosen"]
-    _lib.check(_lib.lib().jb_direct_f64(n, ps0.ws.pos4.data_ptr(), tg.size, ts.data_ptr(), 1.0, 0.0,
-                                        ref.data_ptr(), stream.cuda_stream), "jb_direct_f64")
+    # accuracy of every form against the FP64 direct sum on the report sample
     errs = {}
-    ts_long = ts.long()
     for name, ps in passes.items():
         step(ps)
         torch.cuda.synchronize()
+        tp = atopo if name == "chosen" else topo
         if world > 1:  # every rank's sorted slice, reassembled (one all_gather)
             from jaccpot_b200 import sharding
-            b, e = sharding.particle_range(topo, leaf_lo, leaf_hi)
-            full_acc = sharding.gather_sorted(ps.ws.acc4[b:e].contiguous(), topo)
+            lo_, hi_ = ps.leaf_range
+            b, e = sharding.particle_range(tp, lo_, hi_)
+            full_acc = sharding.gather_sorted(ps.ws.acc4[b:e].contiguous(), tp)
         else:
             full_acc = ps.ws.acc4
-        got = full_acc[ts_long, :3].double().cpu().numpy()
-        e = workloads.relative_errors(got, ref[:, :3].cpu().numpy())
-        errs[name] = {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
-                      "p99_first_4096": float(np.percentile(e[:4096], 99))}
+        errs[name] = errors_of(full_acc, tp, tg, ref_rep)
     split_err = errs.pop("split_bf16")
+    learned_err = errs.pop("learned_gears", None)
 
     # e2e through the public API from pinned host buffers
     h_pos = torch.from_numpy(pos).pin_memory()
     h_mass = torch.from_numpy(mass).pin_memory()
     h_out = torch.empty((n, 3), dtype=torch.float32).pin_memory()
-    state.pass_ = passes["chosen"]
+    if world > 1:
+        state.pass_ = passes["chosen"]
     for _ in range(args.warmup):
         fmm.differentiable_accelerations(state, h_pos, h_mass, out=h_out)
     torch.cuda.synchronize()
@@ -502,9 +594,11 @@ def main() -> None:
 
     # roofline of the dominant kernel (largest stage time of the chosen form)
     peaks = _peaks()
-    near_inter = topo.near_pair_interactions()
+    near_inter = atopo.near_pair_interactions()
     p2p_flops = 20.0 * near_inter
-    m2l_flops = {4: 718.0, 6: 1964.0, 8: 4166.0}.get(cfg["order"], 4166.0) * topo.num_far_pairs
+    gear_pairs = np.bincount(atopo.far_gears, minlength=len(GEARS)) if atopo.num_far_pairs else np.zeros(len(GEARS))
+    m2l_flops = float(sum(int(c) * m2l_flops_per_pair(o) for c, o in zip(gear_pairs, GEARS)))
+    m2l_flops_plain = m2l_flops_per_pair(cfg["order"]) * topo.num_far_pairs
     # measured FP32 FMA peak (in-run probe, 148 SMs x 8 blocks x 256 thr)
     sink = torch.empty(256, device=dev)
     pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -524,11 +618,12 @@ def main() -> None:
         ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
         roof = {"kernel": f"k_m2l_tc_units<{cfg['order']}>", "bound": "tensor", "achieved": ach,
                 "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": ach / peaks["bf16_tflops"],
-                "traffic": _traffic("k_m2l_tc_units", topo.num_far_pairs), "fp32_pipe_frac": ach / fp32_peak}
+                "traffic": _traffic("k_m2l_tc_units", atopo.num_far_pairs), "fp32_pipe_frac": ach / fp32_peak}
     elif stage_names[dom] == "m2l":
         ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
-        roof = {"kernel": f"k_m2l_units<{cfg['order']}>", "bound": "fp32", "achieved": ach, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": _traffic("k_m2l_units", topo.num_far_pairs)}
+        roof = {"kernel": "k_m2l_units<2,4,6,8> (one launch per gear)", "bound": "fp32", "achieved": ach,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                "traffic": _traffic("k_m2l_units", atopo.num_far_pairs)}
     else:
         ach = p2p_flops / (stage_chosen[3] / 1e3) / 1e12
         roof = {"kernel": "k_leaf_units_flat<kahan> (leaf stage: + k_leaf_l2p, k_leaf_reduce)", "bound": "fp32",
@@ -539,6 +634,7 @@ def main() -> None:
     roof["stage_ms"] = float(stage_chosen[dom])
     roof["algorithmic"] = "P2P 20 flop/pair x near pairs; M2L 2*(2*sum(2l+1)^2 + z-terms) flop/pair"
 
+    ms_split, stage_split = ms["split_bf16"], timings["split_bf16"][1]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         import oracle
@@ -559,17 +655,27 @@ def main() -> None:
     launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
     if rank == 0:
         cfg.update({
-            "form": ("chosen = learned per-pair gears (2,4,6,8) + FP32 rotate+scale M2L + Kahan-compensated P2P"
-                     if gear_info else "chosen = FP32 rotate+scale M2L + Kahan-compensated P2P")
-                    + "; plain = FP32 M2L + FP32 P2P at the maximum order; split_bf16 = tcgen05 split-BF16 M2L "
-                    "(K product on the tensor cores) + Kahan P2P at the maximum order",
-            "gears": gear_info,
+            "form": (f"chosen = error-controlled walk (Dehnen eq. 15/16a acceptance, eps={chosen_eps:g}, "
+                     f"per-pair gears {GEARS}) + FP32 rotate+scale M2L + Kahan-compensated P2P; plain = theta walk "
+                     f"(theta={plain_theta:g}) + FP32 M2L + FP32 P2P at the maximum order p={cfg['order']}; "
+                     "split_bf16 = plain's lists with the tcgen05 split-BF16 M2L + Kahan P2P; learned_gears = "
+                     "plain's lists with the MLP-selected gears + Kahan P2P"),
+            "selection": sel,
+            "chosen_vs_plain": ms_plain / ms_chosen,
+            "chosen": {"eps": chosen_eps, "gears": list(GEARS), "theta_max": 1.0, "theta_prepass": 0.6,
+                       "far_pairs": atopo.num_far_pairs, "far_pairs_per_gear": [int(c) for c in gear_pairs],
+                       "near_leaf_pairs": atopo.num_near_pairs, "near_interactions": near_inter,
+                       "m2l_algorithmic_flop": m2l_flops},
+            "learned_gears": None if learned_err is None else {
+                "ms_per_step": ms["learned_gears"], "particles_per_s": n / (ms["learned_gears"] / 1e3),
+                "stage_ms": dict(zip(stage_names, [float(x) for x in timings["learned_gears"][1]])),
+                "err_vs_fp64_direct": learned_err, "selector": gear_info},
             "split_bf16": {
                 "ms_per_step": ms_split, "particles_per_s": n / (ms_split / 1e3),
                 "stage_ms": dict(zip(stage_names, [float(x) for x in stage_split])),
                 "err_vs_fp64_direct": split_err, "err_bound_met": bool(split_err["p99"] <= ERR_BOUND),
-                "m2l_tensor_frac": m2l_flops / (stage_split[1] / 1e3) / 1e12 / peaks["bf16_tflops"],
-                "m2l_fp32_pipe_frac": m2l_flops / (stage_split[1] / 1e3) / 1e12 / fp32_peak},
+                "m2l_tensor_frac": m2l_flops_plain / (stage_split[1] / 1e3) / 1e12 / peaks["bf16_tflops"],
+                "m2l_fp32_pipe_frac": m2l_flops_plain / (stage_split[1] / 1e3) / 1e12 / fp32_peak},
             "plain_particles_per_s": n / (ms_plain / 1e3),
             "plain_ms_per_step": ms_plain,
             "stage_ms_chosen": dict(zip(stage_names, [float(x) for x in stage_chosen])),
@@ -580,9 +686,9 @@ def main() -> None:
             "prepare_s": prep_s,  # first prepare_state of the process (kernel loading included)
             "prepare": prep,
             "num_nodes": topo.num_nodes,
-            "far_pairs": topo.num_far_pairs,
-            "near_leaf_pairs": topo.num_near_pairs,
-            "near_interactions": near_inter,
+            "plain_far_pairs": topo.num_far_pairs,
+            "plain_near_leaf_pairs": topo.num_near_pairs,
+            "plain_near_interactions": topo.near_pair_interactions(),
             "l2": "flushed (256 MiB write) between timed steps",
             "parallelism": f"target-leaf ranges over {world} rank(s)",
             "timing": "CUDA events per step on the launching stream; max over ranks",

@@ -95,7 +95,8 @@ enum {
   JB_TREE_NEAR_OFFSETS = 10,    /* int64[num_leaves+1] */
   JB_TREE_NEAR_SOURCES = 11,    /* int32[num_near_pairs] (leaf indices) */
   JB_TREE_CENTERS_F64 = 12,     /* double[3*num_nodes], COM */
-  JB_TREE_RADII_F64 = 13        /* double[num_nodes], bounding radius about COM */
+  JB_TREE_RADII_F64 = 13,       /* double[num_nodes], bounding radius about COM */
+  JB_TREE_FAR_GEARS = 14        /* int32[num_far_pairs]: gear of each far pair (jb_dtree_adaptive_walk only) */
 };
 
 /* Morton sort + radix tree with leaves of <= leaf_size particles + dual
@@ -130,6 +131,37 @@ JB_API const void* jb_dtree_field(const jb_dtree* t, int field);
 /* Synchronous device-to-host copy of a field (sizes as for jb_tree_copy). */
 JB_API int jb_dtree_copy(const jb_dtree* t, int field, void* dst);
 JB_API void jb_dtree_free(jb_dtree* t);
+
+/* Replaces the far and near lists of a device tree by those of the
+ * error-controlled walk: the reference's Dehnen eq. (15)/(16a) acceptance
+ * (adaptive_error_model="dehnen_paper", runtime/_adaptive_policy.py:267-376,
+ * :2216-2376) taken target-centric.  An ordered node pair (t <- s) is far
+ * when (rho_s + rho_t) < theta_max d and the force-error estimate
+ *   dF_p = 8 max(rho_s, rho_t) / (rho_s + rho_t) * G
+ *          * sum_{l<=p} C(p,l) P_l(s) rho_t^(p-l) / d^(p+2)
+ * of the highest gear is below max(eps * force_scale[t], 1e-24); it is then
+ * tagged with the lowest passing gear (JB_TREE_FAR_GEARS).  Otherwise two
+ * leaves are a near pair (t's list only) and anything else splits the node of
+ * larger radius.  Lists come out target-major CSR like the theta walk's, but
+ * need not be symmetric.  Inputs (device): power = Dehnen's per-degree source
+ * power P_l (num_nodes x num_degrees, double; jb_node_dehnen_power),
+ * force_scale = per-node force scale (float; jb_node_force_scale); host:
+ * gear_orders ascending, num_gears <= 8, each < num_degrees.  Synchronises. */
+/* Inputs of jb_dtree_adaptive_walk.  jb_node_dehnen_power: Dehnen's
+ * per-degree source power P_l = sqrt(sum_m (l-|m|)! (l+|m|)! w_m M_l^m^2), w_m =
+ * 2 for m != 0 in the real packing, l = 0..p, double, num_nodes x (p+1)
+ * (runtime/_adaptive_policy.py:161-214 dehnen_multipole_power_by_degree).
+ * jb_node_force_scale: the smallest |a| over each node's particles (sorted
+ * acc4 of a prepass), leaves first, then internal nodes level by level,
+ * deepest first -- the "min" reduction the reference uses with
+ * dehnen_paper (_adaptive_policy.py:402-470). */
+JB_API int jb_node_dehnen_power(int p, int num_nodes, const float* mult, int row_stride, double* out, void* stream);
+JB_API int jb_node_force_scale(int num_nodes, int num_internal, const int* left, const int* right,
+                               const int* level_offsets_host, int num_levels, const int* node_ranges,
+                               const float* acc4, float* scale, void* stream);
+JB_API int jb_dtree_adaptive_walk(jb_dtree* t, int num_degrees, const double* power, const float* force_scale,
+                                  double G, double eps, double theta_max, int num_gears, const int* gear_orders,
+                                  void* stream);
 
 /* Work-unit schedules built on the GPU (csrc/schedule_gpu.cu) from device
  * lists, entry for entry the arrays of the host builders in schedule.py

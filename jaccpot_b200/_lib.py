@@ -49,6 +49,7 @@ TREE_FIELDS = {
     "near_leaves": (11, "int32"),
     "centers_f64": (12, "float64"),
     "radii_f64": (13, "float64"),
+    "far_gears": (14, "int32"),
 }
 
 
@@ -87,6 +88,9 @@ _SIGNATURES = {
     "jb_dtree_field": [_P, _I],
     "jb_dtree_copy": [_P, _I, _P],
     "jb_dtree_free": [_P],
+    "jb_dtree_adaptive_walk": [_P, _I, _P, _P, _D, _D, _D, _I, _P, _P],
+    "jb_node_dehnen_power": [_I, _I, _P, _I, _P, _P],
+    "jb_node_force_scale": [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P],
     "jb_set_level_split": [_I, _I],
     "jb_set_leaf_form": [_I],
     "jb_far_reverse_index": [_I, _P, _P, _P, _P],

@@ -87,6 +87,27 @@ __global__ void k_force_min_level(int first, int last, const int* __restrict__ l
   scale[i] = fminf(scale[left[i]], scale[right[i]]);
 }
 
+// Dehnen's per-degree power P_l = sqrt(sum_m w_lm M_l^m^2), w_lm = (l-|m|)!
+// (l+|m|)! doubled for m != 0 in the real no-sqrt2 packing
+// (_adaptive_policy.py:161-214 dehnen_multipole_power_by_degree), in FP64 for
+// l = 0..p (a point mass m at distance r has P_l = m r^l).
+__global__ void k_dehnen_power(int p, int num_nodes, const float* __restrict__ mult, int rs,
+                               double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= num_nodes) return;
+  const float* M = mult + (size_t)i * rs;
+  for (int l = 0; l <= p; ++l) {
+    double acc = 0.0;
+    for (int m = -l; m <= l; ++m) {
+      const int am = m < 0 ? -m : m;
+      const double w = factd2(l - am) * factd2(l + am) * (m != 0 ? 2.0 : 1.0);
+      const double c = (double)M[l * l + l + m];
+      acc += w * c * c;
+    }
+    out[(size_t)i * (p + 1) + l] = sqrt(acc);
+  }
+}
+
 // The 12 features of far pair (t <- s).
 __device__ __forceinline__ void pair_features(int t, int s, const float4* __restrict__ centers,
                                               const float* __restrict__ radii, const float* __restrict__ node_feat,
@@ -445,6 +466,37 @@ JB_API int jb_gear_node_features(int p, int num_nodes, int num_internal, const i
                                                    reinterpret_cast<const int2*>(node_ranges),
                                                    reinterpret_cast<const float4*>(acc4), scale);
   rc = launch_status();
+  if (rc) return rc;
+  for (int lev = num_levels - 1; lev >= 0; --lev) {
+    const int a = level_offsets_host[lev], b = level_offsets_host[lev + 1];
+    if (b <= a) continue;
+    k_force_min_level<<<gblocks(b - a, 128), 128, 0, st>>>(a, b, left, right, scale);
+    rc = launch_status();
+    if (rc) return rc;
+  }
+  return JB_OK;
+}
+
+JB_API int jb_node_dehnen_power(int p, int num_nodes, const float* mult, int row_stride, double* out, void* stream) {
+  if (p < 0 || p > JB_MAX_ORDER || num_nodes < 0 || row_stride < (p + 1) * (p + 1) ||
+      (num_nodes > 0 && (!mult || !out)))
+    return JB_ERR_ARG;
+  if (num_nodes == 0) return JB_OK;
+  k_dehnen_power<<<gblocks(num_nodes, 128), 128, 0, GST(stream)>>>(p, num_nodes, mult, row_stride, out);
+  return launch_status();
+}
+
+JB_API int jb_node_force_scale(int num_nodes, int num_internal, const int* left, const int* right,
+                               const int* level_offsets_host, int num_levels, const int* node_ranges,
+                               const float* acc4, float* scale, void* stream) {
+  if (num_nodes < 1 || num_internal < 0 || num_internal >= num_nodes || !node_ranges || !acc4 || !scale ||
+      (num_internal > 0 && (!left || !right || !level_offsets_host || num_levels < 1)))
+    return JB_ERR_ARG;
+  cudaStream_t st = GST(stream);
+  const int L = num_nodes - num_internal;
+  k_leaf_force_min<<<gblocks(L, 128), 128, 0, st>>>(num_nodes, num_internal, reinterpret_cast<const int2*>(node_ranges),
+                                                   reinterpret_cast<const float4*>(acc4), scale);
+  int rc = launch_status();
   if (rc) return rc;
   for (int lev = num_levels - 1; lev >= 0; --lev) {
     const int a = level_offsets_host[lev], b = level_offsets_host[lev + 1];

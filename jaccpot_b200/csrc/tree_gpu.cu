@@ -299,6 +299,9 @@ __global__ void k_internal_com(int first, int last, const int* __restrict__ left
 // 4. Dual walk, breadth-first over node pairs.
 // ---------------------------------------------------------------------------
 enum : int { kNone = 0, kSelf = 1, kFar = 2, kNear = 3, kSplitA = 4, kSplitB = 5 };
+constexpr int kMaxGears = 8;
+constexpr int kMaxGearOrder = 24;
+constexpr int kGearShift = 56;  // far keys of the adaptive walk carry the gear in bits 56..63
 
 struct WalkCtx {
   const int* left;
@@ -307,6 +310,14 @@ struct WalkCtx {
   const double* radius;
   int num_internal;
   double theta2;
+  // error-controlled, target-centric walk (jb_dtree_adaptive_walk); unused
+  // by the symmetric theta walk
+  const double* power;  // Dehnen per-degree source power P_l, num_nodes x npow
+  const float* fscale;  // force scale of each target node (smallest |a| under it)
+  int npow;             // degrees 0..npow-1 of power
+  int num_gears;
+  int gear_order[kMaxGears];
+  double G, eps, theta_max;
 };
 
 __device__ __forceinline__ int walk_decide(const WalkCtx& w, int a, int b) {
@@ -361,6 +372,113 @@ __global__ void k_walk_emit(const int2* __restrict__ fr, int F, WalkCtx w, const
   }
 }
 
+// Error-controlled acceptance of the far pair (target t <- source s), the
+// reference's Dehnen eq. (15)/(16a) policy (runtime/_adaptive_policy.py:
+// 267-376 dehnen_paper_pair_error_by_order, :2285-2338 the directional test):
+//   E_p   = sum_{l=0}^{p} C(p, l) P_l(s) rho_t^(p-l)        (eq. 15, binomial sum)
+//   dF_p  = 8 max(rho_s, rho_t) / (rho_s + rho_t) * G E_p / d^(p+2)
+// (the source mass of E_p / (M_s d^p) and of G M_s / d^2 cancels), accepted
+// when (rho_s + rho_t) < theta_max d and the highest gear passes
+// dF < max(eps * fscale[t], 1e-24); the gear is the lowest passing one.
+// Returns the gear index, or -1.  Every step is a separately rounded FP64
+// operation (this file is compiled with -fmad=false), in the order the
+// oracle's restatement (oracle/adaptive_walk.py) uses.
+__device__ int error_gear(const WalkCtx& w, int t, int s, double d, double rt, double rs) {
+  double rtp[kMaxGearOrder + 1], dp[kMaxGearOrder + 3];
+  const int pmax = w.gear_order[w.num_gears - 1];
+  rtp[0] = 1.0;
+  for (int k = 1; k <= pmax; ++k) rtp[k] = rtp[k - 1] * rt;
+  dp[0] = 1.0;
+  for (int k = 1; k <= pmax + 2; ++k) dp[k] = dp[k - 1] * d;
+  const double den = fmax(rs + rt, 1e-24);
+  const double imp = (8.0 * fmax(rs, rt)) / den;
+  const double thr = fmax(w.eps * (double)w.fscale[t], 1e-24);
+  const double* P = w.power + (int64_t)s * w.npow;
+  int first = -1;
+  bool pass = false;
+  for (int g = 0; g < w.num_gears; ++g) {
+    const int p = w.gear_order[g];
+    double e = 0.0, c = 1.0;  // c = C(p, l)
+    for (int l = 0; l <= p && l < w.npow; ++l) {
+      if (l > 0) c = (c * (double)(p - l + 1)) / (double)l;
+      e = e + (c * P[l]) * rtp[p - l];
+    }
+    const double ferr = ((w.G * imp) * e) / dp[p + 2];
+    pass = ferr < thr;
+    if (pass && first < 0) first = g;
+  }
+  return pass ? first : -1;  // the highest gear must pass
+}
+
+__device__ __forceinline__ int adaptive_decide(const WalkCtx& w, int t, int s, int* gear) {
+  const bool lt = t >= w.num_internal, ls = s >= w.num_internal;
+  if (t == s) return lt ? kNone : kSelf;
+  double d2 = 0;
+  for (int k = 0; k < 3; ++k) {
+    const double dd = w.com[3 * (int64_t)t + k] - w.com[3 * (int64_t)s + k];
+    d2 += dd * dd;
+  }
+  const double rt = w.radius[t], rs = w.radius[s];
+  if (d2 > 0) {
+    const double d = sqrt(d2);
+    if (rs + rt < w.theta_max * d) {
+      const int g = error_gear(w, t, s, d, rt, rs);
+      if (g >= 0) {
+        *gear = g;
+        return kFar;
+      }
+    }
+  }
+  if (lt && ls) return kNear;
+  return (!lt && (ls || rt >= rs)) ? kSplitA : kSplitB;
+}
+
+__global__ void k_awalk_count(const int2* __restrict__ fr, int F, WalkCtx w, I3* __restrict__ cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F) return;
+  int g = 0;
+  const int d = adaptive_decide(w, fr[i].x, fr[i].y, &g);
+  cnt[i] = I3{d == kSelf ? 4 : (d >= kSplitA ? 2 : 0), d == kFar ? 1 : 0, d == kNear ? 1 : 0};
+}
+
+__global__ void k_awalk_emit(const int2* __restrict__ fr, int F, WalkCtx w, const I3* __restrict__ off,
+                             int2* __restrict__ next, uint64_t* __restrict__ far_keys, int far_shift,
+                             uint64_t* __restrict__ near_keys, int near_shift) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F) return;
+  const I3 o3 = off[i];
+  const int t = fr[i].x, s = fr[i].y;
+  int g = 0;
+  const int d = adaptive_decide(w, t, s, &g);
+  if (d == kSelf) {
+    const int l = w.left[t], r = w.right[t];
+    int2* o = next + o3.a;
+    o[0] = make_int2(l, l);
+    o[1] = make_int2(r, r);
+    o[2] = make_int2(l, r);
+    o[3] = make_int2(r, l);
+  } else if (d == kSplitA) {
+    next[o3.a] = make_int2(w.left[t], s);
+    next[o3.a + 1] = make_int2(w.right[t], s);
+  } else if (d == kSplitB) {
+    next[o3.a] = make_int2(t, w.left[s]);
+    next[o3.a + 1] = make_int2(t, w.right[s]);
+  } else if (d == kFar) {
+    far_keys[o3.b] = ((uint64_t)g << kGearShift) | ((uint64_t)t << far_shift) | (uint64_t)s;
+  } else if (d == kNear) {
+    near_keys[o3.c] = ((uint64_t)(t - w.num_internal) << near_shift) | (uint64_t)(s - w.num_internal);
+  }
+}
+
+// Moves the gear bits of sorted far keys into gears[] (CSR order).
+__global__ void k_take_gears(uint64_t* __restrict__ keys, int64_t n, int* __restrict__ gears) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t k = keys[i];
+  gears[i] = (int)(k >> kGearShift);
+  keys[i] = k & ((1ULL << kGearShift) - 1);
+}
+
 // ---------------------------------------------------------------------------
 // 5. CSR from sorted (row << shift | col) keys.
 // ---------------------------------------------------------------------------
@@ -399,9 +517,109 @@ inline int bits_for(int64_t v) {  // bits to hold values in [0, v)
 struct jb_dtree {
   jb_tree_info_t info{};
   DBuf perm, ranges, left, right, parent, level, level_off, leaf_of, far_off, far_src, near_off, near_src, com, radius;
+  DBuf far_gear;  // gear index per far pair (CSR order) after jb_dtree_adaptive_walk
+  int walk_kind = 0;  // 0: symmetric theta walk, 1: error-controlled target-centric walk
 };
 
 namespace {
+
+// Steps 4 and 5: the dual walk from (root, root) and the CSR lists built from
+// what it emits, into t.far_off/far_src/near_off/near_src (and t.far_gear for
+// the adaptive walk).  Sets t.info.num_far_pairs / num_near_pairs.
+int64_t walk_lists(jb_dtree& t, const WalkCtx& w, bool adaptive, int NN, int L, Scratch& s, int* d_total32,
+                   cudaStream_t st) {
+  const int far_shift = bits_for(NN), near_shift = bits_for(std::max(L, 1));
+  DBuf w0, w1, cnt3, off3, far_keys, near_keys;
+  int64_t n_far = 0, n_near = 0;
+  if (NN > 1) {
+    const int64_t cap = std::max<int64_t>(1 << 16, 4 * (int64_t)NN);
+    ck(w0.alloc(cap * sizeof(int2)));
+    ck(w1.alloc(cap * sizeof(int2)));
+    ck(cnt3.alloc(cap * sizeof(I3)));
+    ck(off3.alloc(cap * sizeof(I3)));
+    ck(far_keys.alloc((size_t)std::max<int64_t>(1 << 16, 256 * (int64_t)NN) * 8));
+    ck(near_keys.alloc((size_t)std::max<int64_t>(1 << 16, 256 * (int64_t)L) * 8));
+    I3* d_tot3 = reinterpret_cast<I3*>(d_total32);
+    const int2 root = make_int2(0, 0);
+    ck(cudaMemcpyAsync(w0.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    DBuf* wc = &w0;
+    DBuf* wn = &w1;
+    int64_t Fw = 1;
+    while (Fw > 0) {
+      if ((size_t)Fw * sizeof(I3) > cnt3.bytes) {
+        ck(cnt3.alloc((size_t)Fw * 2 * sizeof(I3)));
+        ck(off3.alloc((size_t)Fw * 2 * sizeof(I3)));
+      }
+      if (adaptive)
+        k_awalk_count<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, cnt3.as<I3>());
+      else
+        k_walk_count<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, cnt3.as<I3>());
+      ck_launch();
+      exclusive_scan<I3>(cnt3.as<I3>(), off3.as<I3>(), Fw, d_tot3, s, st);
+      const I3 tot = read_word(d_tot3, st);
+      // grow the next frontier and the key buffers as needed (stream-ordered)
+      ck(wn->grow((size_t)tot.a * 2 * sizeof(int2), 0, st));
+      const size_t need_far = (size_t)(n_far + tot.b) * 8, need_near = (size_t)(n_near + tot.c) * 8;
+      if (need_far > far_keys.bytes) ck(far_keys.grow(std::max(need_far, 2 * far_keys.bytes), (size_t)n_far * 8, st));
+      if (need_near > near_keys.bytes)
+        ck(near_keys.grow(std::max(need_near, 2 * near_keys.bytes), (size_t)n_near * 8, st));
+      if (adaptive)
+        k_awalk_emit<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, off3.as<I3>(), wn->as<int2>(),
+                                                       far_keys.as<uint64_t>() + n_far, far_shift,
+                                                       near_keys.as<uint64_t>() + n_near, near_shift);
+      else
+        k_walk_emit<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, off3.as<I3>(), wn->as<int2>(),
+                                                      far_keys.as<uint64_t>() + n_far, far_shift,
+                                                      near_keys.as<uint64_t>() + n_near, near_shift);
+      ck_launch();
+      n_far += tot.b;
+      n_near += tot.c;
+      Fw = tot.a;
+      std::swap(wc, wn);
+    }
+  }
+  w0.release();
+  w1.release();
+  cnt3.release();
+  off3.release();
+
+  auto to_csr = [&](DBuf& keys, int64_t m, int shift, int rows, DBuf& off, DBuf& col, DBuf* gears) {
+    ck(off.alloc((size_t)(rows + 1) * 8));
+    ck(col.alloc((size_t)std::max<int64_t>(m, 1) * 4));
+    if (gears) ck(gears->alloc((size_t)std::max<int64_t>(m, 1) * 4));
+    if (m == 0) {
+      ck(cudaMemsetAsync(off.p, 0, (size_t)(rows + 1) * 8, st));
+      return;
+    }
+    DBuf tmp;
+    ck(tmp.alloc((size_t)m * 8));
+    radix_sort(keys.as<uint64_t>(), nullptr, tmp.as<uint64_t>(), nullptr, m, 2 * shift, s, st);
+    if (gears) {
+      k_take_gears<<<nblocks(m, 256), 256, 0, st>>>(keys.as<uint64_t>(), m, gears->as<int>());
+      ck_launch();
+    }
+    k_csr<<<nblocks(std::max<int64_t>(m, rows + 1), 256), 256, 0, st>>>(keys.as<uint64_t>(), m, shift, rows,
+                                                                       col.as<int>(), off.as<int64_t>());
+    ck_launch();
+  };
+  if (NN > 1) {
+    to_csr(far_keys, n_far, far_shift, NN, t.far_off, t.far_src, adaptive ? &t.far_gear : nullptr);
+    far_keys.release();
+    to_csr(near_keys, n_near, near_shift, L, t.near_off, t.near_src, nullptr);
+    near_keys.release();
+  } else {
+    ck(t.far_off.alloc((size_t)(NN + 1) * 8));
+    ck(cudaMemsetAsync(t.far_off.p, 0, (size_t)(NN + 1) * 8, st));
+    ck(t.near_off.alloc((size_t)(L + 1) * 8));
+    ck(cudaMemsetAsync(t.near_off.p, 0, (size_t)(L + 1) * 8, st));
+    ck(t.far_src.alloc(4));
+    ck(t.near_src.alloc(4));
+    if (adaptive) ck(t.far_gear.alloc(4));
+  }
+  t.info.num_far_pairs = n_far;
+  t.info.num_near_pairs = n_near;
+  return 0;
+}
 
 void build(jb_dtree& t, int64_t n, const double* pos, const double* mass, int leaf_size, double theta, cudaStream_t st) {
   tl_stream = st;
@@ -532,82 +750,16 @@ void build(jb_dtree& t, int64_t n, const double* pos, const double* mass, int le
   k1.release();
   v1.release();
 
-  // 4. Dual walk (only when the root is split, as the host).
-  const int far_shift = bits_for(NN), near_shift = bits_for(std::max(L, 1));
-  DBuf w0, w1, cnt3, off3, far_keys, near_keys;
-  int64_t n_far = 0, n_near = 0;
-  if (NN > 1) {
-    const WalkCtx w{t.left.as<int>(), t.right.as<int>(), t.com.as<double>(), t.radius.as<double>(), NI, theta * theta};
-    const int64_t cap = std::max<int64_t>(1 << 16, 4 * (int64_t)NN);
-    ck(w0.alloc(cap * sizeof(int2)));
-    ck(w1.alloc(cap * sizeof(int2)));
-    ck(cnt3.alloc(cap * sizeof(I3)));
-    ck(off3.alloc(cap * sizeof(I3)));
-    ck(far_keys.alloc((size_t)std::max<int64_t>(1 << 16, 256 * (int64_t)NN) * 8));
-    ck(near_keys.alloc((size_t)std::max<int64_t>(1 << 16, 256 * (int64_t)L) * 8));
-    I3* d_tot3 = reinterpret_cast<I3*>(d_total32);
-    const int2 root = make_int2(0, 0);
-    ck(cudaMemcpyAsync(w0.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
-    DBuf* wc = &w0;
-    DBuf* wn = &w1;
-    int64_t Fw = 1;
-    while (Fw > 0) {
-      if ((size_t)Fw * sizeof(I3) > cnt3.bytes) {
-        ck(cnt3.alloc((size_t)Fw * 2 * sizeof(I3)));
-        ck(off3.alloc((size_t)Fw * 2 * sizeof(I3)));
-      }
-      k_walk_count<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, cnt3.as<I3>());
-      ck_launch();
-      exclusive_scan<I3>(cnt3.as<I3>(), off3.as<I3>(), Fw, d_tot3, s, st);
-      const I3 tot = read_word(d_tot3, st);
-      // grow the next frontier and the key buffers as needed (stream-ordered)
-      ck(wn->grow((size_t)tot.a * 2 * sizeof(int2), 0, st));
-      const size_t need_far = (size_t)(n_far + tot.b) * 8, need_near = (size_t)(n_near + tot.c) * 8;
-      if (need_far > far_keys.bytes) ck(far_keys.grow(std::max(need_far, 2 * far_keys.bytes), (size_t)n_far * 8, st));
-      if (need_near > near_keys.bytes)
-        ck(near_keys.grow(std::max(need_near, 2 * near_keys.bytes), (size_t)n_near * 8, st));
-      k_walk_emit<<<nblocks(Fw, 256), 256, 0, st>>>(wc->as<int2>(), (int)Fw, w, off3.as<I3>(), wn->as<int2>(),
-                                                    far_keys.as<uint64_t>() + n_far, far_shift,
-                                                    near_keys.as<uint64_t>() + n_near, near_shift);
-      ck_launch();
-      n_far += tot.b;
-      n_near += tot.c;
-      Fw = tot.a;
-      std::swap(wc, wn);
-    }
-  }
-  w0.release();
-  w1.release();
-  cnt3.release();
-  off3.release();
-
-  // 5. CSR lists.
-  auto to_csr = [&](DBuf& keys, int64_t m, int shift, int rows, DBuf& off, DBuf& col) {
-    ck(off.alloc((size_t)(rows + 1) * 8));
-    ck(col.alloc((size_t)std::max<int64_t>(m, 1) * 4));
-    if (m == 0) {
-      ck(cudaMemsetAsync(off.p, 0, (size_t)(rows + 1) * 8, st));
-      return;
-    }
-    DBuf tmp;
-    ck(tmp.alloc((size_t)m * 8));
-    radix_sort(keys.as<uint64_t>(), nullptr, tmp.as<uint64_t>(), nullptr, m, 2 * shift, s, st);
-    k_csr<<<nblocks(std::max<int64_t>(m, rows + 1), 256), 256, 0, st>>>(keys.as<uint64_t>(), m, shift, rows,
-                                                                       col.as<int>(), off.as<int64_t>());
-    ck_launch();
-  };
-  if (NN > 1) {
-    to_csr(far_keys, n_far, far_shift, NN, t.far_off, t.far_src);
-    far_keys.release();
-    to_csr(near_keys, n_near, near_shift, L, t.near_off, t.near_src);
-    near_keys.release();
-  } else {
-    ck(t.far_off.alloc((size_t)(NN + 1) * 8));
-    ck(cudaMemsetAsync(t.far_off.p, 0, (size_t)(NN + 1) * 8, st));
-    ck(t.near_off.alloc((size_t)(L + 1) * 8));
-    ck(cudaMemsetAsync(t.near_off.p, 0, (size_t)(L + 1) * 8, st));
-    ck(t.far_src.alloc(4));
-    ck(t.near_src.alloc(4));
+  // 4./5. Dual walk (only when the root is split, as the host) and CSR lists.
+  {
+    WalkCtx w{};
+    w.left = t.left.as<int>();
+    w.right = t.right.as<int>();
+    w.com = t.com.as<double>();
+    w.radius = t.radius.as<double>();
+    w.num_internal = NI;
+    w.theta2 = theta * theta;
+    walk_lists(t, w, false, NN, L, s, d_total32, st);
   }
   ck(cudaStreamSynchronize(st));
 
@@ -616,8 +768,6 @@ void build(jb_dtree& t, int64_t n, const double* pos, const double* mass, int le
   t.info.num_internal = NI;
   t.info.num_leaves = L;
   t.info.num_levels = num_levels;
-  t.info.num_far_pairs = n_far;
-  t.info.num_near_pairs = n_near;
   t.info.max_leaf_occupancy = max_occ;
 }
 
@@ -637,6 +787,7 @@ const DBuf* field_buf(const jb_dtree* t, int field) {
     case JB_TREE_NEAR_SOURCES: return &t->near_src;
     case JB_TREE_CENTERS_F64: return &t->com;
     case JB_TREE_RADII_F64: return &t->radius;
+    case JB_TREE_FAR_GEARS: return t->walk_kind == 1 ? &t->far_gear : nullptr;
     default: return nullptr;
   }
 }
@@ -658,6 +809,7 @@ size_t field_bytes(const jb_dtree* t, int field) {
     case JB_TREE_NEAR_SOURCES: return (size_t)i.num_near_pairs * 4;
     case JB_TREE_CENTERS_F64: return (size_t)i.num_nodes * 24;
     case JB_TREE_RADII_F64: return (size_t)i.num_nodes * 8;
+    case JB_TREE_FAR_GEARS: return t->walk_kind == 1 ? (size_t)i.num_far_pairs * 4 : 0;
     default: return 0;
   }
 }
@@ -684,6 +836,52 @@ JB_API int jb_tree_build_device(int64_t n, const double* pos, const double* mass
     return JB_ERR_ALLOC;
   }
   *out = t;
+  return JB_OK;
+}
+
+JB_API int jb_dtree_adaptive_walk(jb_dtree* t, int num_degrees, const double* power, const float* force_scale,
+                                  double G, double eps, double theta_max, int num_gears, const int* gear_orders,
+                                  void* stream) {
+  if (!t || !power || !force_scale || num_degrees < 1 || num_gears < 1 || num_gears > kMaxGears || !gear_orders ||
+      !(eps > 0) || !(theta_max > 0) || theta_max > 1.0 || !(G > 0))
+    return JB_ERR_ARG;
+  for (int g = 0; g < num_gears; ++g) {
+    const int p = gear_orders[g];
+    if (p < 0 || p > kMaxGearOrder || p >= num_degrees || (g > 0 && p <= gear_orders[g - 1])) return JB_ERR_ARG;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  try {
+    tl_stream = st;
+    Scratch s;
+    ck(s.total.alloc(64));
+    int* d_total32 = reinterpret_cast<int*>(s.total.as<int64_t>() + 4);
+    WalkCtx w{};
+    w.left = t->left.as<int>();
+    w.right = t->right.as<int>();
+    w.com = t->com.as<double>();
+    w.radius = t->radius.as<double>();
+    w.num_internal = t->info.num_internal;
+    w.power = power;
+    w.fscale = force_scale;
+    w.npow = num_degrees;
+    w.num_gears = num_gears;
+    for (int g = 0; g < num_gears; ++g) w.gear_order[g] = gear_orders[g];
+    w.G = G;
+    w.eps = eps;
+    w.theta_max = theta_max;
+    t->far_off.release();
+    t->far_src.release();
+    t->near_off.release();
+    t->near_src.release();
+    t->far_gear.release();
+    walk_lists(*t, w, true, t->info.num_nodes, t->info.num_leaves, s, d_total32, st);
+    t->walk_kind = 1;
+    ck(cudaStreamSynchronize(st));
+  } catch (const Fail& f) {
+    return f.rc;
+  } catch (const std::bad_alloc&) {
+    return JB_ERR_ALLOC;
+  }
   return JB_OK;
 }
 

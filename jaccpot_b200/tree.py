@@ -43,6 +43,9 @@ class Topology:
     centers_f64: np.ndarray  # float64[num_nodes, 3] (host COM used by the MAC)
     radii_f64: np.ndarray  # float64[num_nodes]
     m2l_targets: np.ndarray = field(default=None)  # int32, nodes with >= 1 far pair, longest list first
+    # error-controlled walk only: gear index of every far pair and the gears' orders
+    far_gears: np.ndarray = field(default=None)  # int32[num_far]
+    gear_orders: tuple = field(default=None)
 
     @property
     def num_far_pairs(self) -> int:
@@ -106,20 +109,23 @@ def _field_sizes(n: int, info) -> dict:
         "near_leaves": info.num_near_pairs,
         "centers_f64": 3 * info.num_nodes,
         "radii_f64": info.num_nodes,
+        "far_gears": info.num_far_pairs,
     }
 
 
-def _copy_fields(copy_fn, handle, n: int, info) -> dict:
+def _copy_fields(copy_fn, handle, n: int, info, with_gears: bool = False) -> dict:
     sizes = _field_sizes(n, info)
     arrs = {}
     for name, (fid, dt) in _lib.TREE_FIELDS.items():
+        if name == "far_gears" and not with_gears:
+            continue
         a = np.empty(max(sizes[name], 1), dtype=dt)
         _lib.check(copy_fn(handle, fid, a.ctypes.data), f"tree field copy ({name})")
         arrs[name] = a[: sizes[name]]
     return arrs
 
 
-def _topology(n: int, info, arrs: dict, leaf_size: int, theta: float) -> Topology:
+def _topology(n: int, info, arrs: dict, leaf_size: int, theta: float, gear_orders=None) -> Topology:
     perm = arrs["permutation"]
     inv = np.empty_like(perm)
     inv[perm] = np.arange(n, dtype=np.int64)
@@ -151,6 +157,8 @@ def _topology(n: int, info, arrs: dict, leaf_size: int, theta: float) -> Topolog
         centers_f64=arrs["centers_f64"].reshape(-1, 3),
         radii_f64=arrs["radii_f64"],
         m2l_targets=tg[order].astype(np.int32),
+        far_gears=arrs.get("far_gears"),
+        gear_orders=None if gear_orders is None else tuple(int(o) for o in gear_orders),
     )
 
 
@@ -220,14 +228,36 @@ class DeviceTree:
         self.info = _lib.TreeInfo()
         _lib.check(self._lb.jb_dtree_info(self._h, ctypes.byref(self.info)), "jb_dtree_info")
         self.sizes = _field_sizes(self.n, self.info)
+        self.gear_orders = None  # set by adaptive_walk
+
+    def adaptive_walk(self, power, force_scale, *, G: float, eps: float, theta_max: float = 1.0,
+                      gear_orders=(8,)) -> None:
+        """Replaces the lists by those of the error-controlled walk
+        (jb_dtree_adaptive_walk: Dehnen eq. (15)/(16a) acceptance, target-
+        centric, per-pair gears).  power: float64 (num_nodes, P+1) Dehnen
+        source powers; force_scale: float32 (num_nodes,) -- both on this
+        tree's device, in its node order."""
+        torch = self._torch
+        orders = np.ascontiguousarray(np.asarray(gear_orders, dtype=np.int32))
+        pw = power.to(device=self.device, dtype=torch.float64).contiguous()
+        fs = force_scale.to(device=self.device, dtype=torch.float32).contiguous()
+        if pw.dim() != 2 or pw.shape[0] != self.info.num_nodes or fs.shape != (self.info.num_nodes,):
+            raise ValueError("power must be (num_nodes, P+1) and force_scale (num_nodes,)")
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(self._lb.jb_dtree_adaptive_walk(self._h, int(pw.shape[1]), pw.data_ptr(), fs.data_ptr(),
+                                                   float(G), float(eps), float(theta_max), int(orders.size),
+                                                   orders.ctypes.data, stream), "jb_dtree_adaptive_walk")
+        _lib.check(self._lb.jb_dtree_info(self._h, ctypes.byref(self.info)), "jb_dtree_info")
+        self.sizes = _field_sizes(self.n, self.info)
+        self.gear_orders = tuple(int(o) for o in orders)
 
     def field(self, name: str):
         fid, dt = _lib.TREE_FIELDS[name]
         return device_view(self._lb.jb_dtree_field(self._h, fid), (self.sizes[name],), dt, self.device)
 
     def topology(self) -> Topology:
-        arrs = _copy_fields(self._lb.jb_dtree_copy, self._h, self.n, self.info)
-        return _topology(self.n, self.info, arrs, self.leaf_size, self.theta)
+        arrs = _copy_fields(self._lb.jb_dtree_copy, self._h, self.n, self.info, with_gears=self.gear_orders is not None)
+        return _topology(self.n, self.info, arrs, self.leaf_size, self.theta, self.gear_orders)
 
     def free(self) -> None:
         if self._h:
