@@ -853,22 +853,26 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
 // Near field with every lane busy, for leaves of 17..32 particles.
 //
 // One lane per target leaves 32 - nt lanes idle.  Here a unit's work, nt
-// targets x C source chunks of 32, is walked chunk-major: item f = c * nt + t,
-// 32 items per warp step, lane l of step s takes item 32 s + l (target
-// f mod nt against chunk f / nt).  A step spans at most three consecutive
-// chunks (nt >= 17), so the chunks sit in a ring of four shared-memory slots,
-// padded so that the slots one load instruction reads fall in different
-// banks, and are fetched two chunks ahead.  The per-target sums live in
-// shared memory: lane l < nt owns its item's target and, when lane l + nt
-// holds the same target's next chunk, adds that partial straight after its
-// own.  Every target therefore receives its chunk partials in chunk order
-// through the same (compensated) add as in the lane-per-target form, from
-// the same per-chunk arithmetic: the results are bit-identical to it.
+// targets x C source chunks of kFlatChunk (64), is walked chunk-major: item
+// f = c * nt + t, 32 items per warp step, lane l of step s takes item 32 s + l
+// (target f mod nt against chunk f / nt).  A step spans at most three
+// consecutive chunks (nt >= 17), so the chunks sit in a ring of four
+// shared-memory slots, padded so that the slots one load instruction reads
+// fall in different banks.  Each chunk is copied into its slot by cp.async
+// (four 4-byte copies per source: the ring is one array per coordinate, so
+// that a 16-byte load yields two packed source pairs), one chunk ahead of the
+// chunks the step reads, so no register holds a source in flight.  The
+// per-target sums live in shared memory: lane l < nt owns its item's target
+// and, when lane l + nt holds the same target's next chunk, adds that partial
+// straight after its own, so every target receives its chunk partials in
+// chunk order through one (compensated) add per 64 sources.
 // ---------------------------------------------------------------------------
+constexpr int kFlatChunk = 64;                // sources per chunk (item)
+constexpr int kFlatSlot = kFlatChunk + 4;     // slot stride (floats): the three slots one load reads use distinct banks
 struct alignas(16) FlatStage {
-  float x[4][36], y[4][36], z[4][36], m[4][36];  // source chunk ring (slot stride 144 B)
-  float4 tp[32];                                   // target positions
-  float4 s[32], c[32];                             // per-target sums and their compensations
+  float x[4][kFlatSlot], y[4][kFlatSlot], z[4][kFlatSlot], m[4][kFlatSlot];  // source chunk ring
+  float4 tp[32];                                                            // target positions
+  float4 s[32], c[32];                                                      // per-target sums and compensations
 };
 
 union WarpStage {
@@ -876,9 +880,16 @@ union WarpStage {
   FlatStage f;
 };
 
-// Sums of one 32-source chunk for one target, the arithmetic of near_chunk
-// with one lane per target (packed pairs j, j + 1; the two halves added).
-template <bool POT, bool SELF>
+__device__ __forceinline__ void cp_async4(float* smem_dst, const float* gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Sums of one chunk of NS sources for one target, the arithmetic of
+// near_chunk with one lane per target (packed pairs j, j + 1; the two halves
+// added at the end).
+template <bool POT, bool SELF, int NS = 32>
 __device__ __forceinline__ float4 chunk_sums(const float* xs, const float* ys, const float* zs, const float* ms,
                                              float4 ti, int self_j, float eps2) {
   const ulonglong2* X = reinterpret_cast<const ulonglong2*>(xs);
@@ -914,7 +925,7 @@ __device__ __forceinline__ float4 chunk_sums(const float* xs, const float* ys, c
     if (POT) AW = f2_add(AW, mir);
   };
 #pragma unroll
-  for (int v = 0; v < 8; ++v) {
+  for (int v = 0; v < NS / 4; ++v) {
     const ulonglong2 x = X[v], y = Y[v], z = Z[v], m = M[v];
     step(x.x, y.x, z.x, m.x, 4 * v);
     step(x.y, y.y, z.y, m.y, 4 * v + 2);
@@ -950,6 +961,7 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
                                                const int2* __restrict__ runs, FlatStage& S, int lane, float G_,
                                                float eps2, float4* __restrict__ out, float4* __restrict__ partial,
                                                int max_slots, int* err) {
+  constexpr int CH = kFlatChunk;
   const int nt = rg.y - rg.x + 1;  // 17..32
   const bool tgt = lane < nt;
   const float4 me = tgt ? pos4[rg.x + lane] : JB_PAD4;
@@ -968,38 +980,55 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
   }
   const int nsrc = U.w;
   if (nsrc > 0) {
-    const int C = (nsrc + 31) >> 5;
+    const int C = (nsrc + CH - 1) / CH;
     const int total = nt * C;
     int r = U.y, rbase = 0;
     int2 run = runs[r];
-    auto fetch = [&](int f) -> float4 {  // source f of the unit (padding past the end)
+    // copies source f of the unit (padding past the end) into position q of
+    // ring slot sl; a lane's f only grow, so its run cursor only advances
+    auto stage_src = [&](int f, int sl, int q) {
       while (f >= rbase + run.y && r + 1 < U.z) {
         rbase += run.y;
         ++r;
         run = runs[r];
       }
-      return (f < nsrc) ? pos4[run.x + (f - rbase)] : JB_PAD4;
+      if (f < nsrc) {
+        const float* src = reinterpret_cast<const float*>(pos4 + run.x + (f - rbase));
+        cp_async4(&S.x[sl][q], src);
+        cp_async4(&S.y[sl][q], src + 1);
+        cp_async4(&S.z[sl][q], src + 2);
+        cp_async4(&S.m[sl][q], src + 3);
+      } else {
+        S.x[sl][q] = 1e18f;
+        S.y[sl][q] = 1e18f;
+        S.z[sl][q] = 1e18f;
+        S.m[sl][q] = 0.f;
+      }
     };
-    float4 q0 = fetch(lane);                          // the next chunk to stage
-    float4 q1 = (C > 1) ? fetch(32 + lane) : JB_PAD4;  // the one after
+    auto stage_chunk = [&](int k) {  // one cp.async group per chunk
+      const int sl = k & 3;
+      stage_src(k * CH + lane, sl, lane);
+      stage_src(k * CH + 32 + lane, sl, 32 + lane);
+      cp_async_commit();
+    };
     int staged = 0;
     int c = (lane >= nt) ? 1 : 0, t = lane - c * nt;  // item f = lane
+    __syncwarp();  // the self block's reads of slot 0 are done
     for (int base = 0; base < total; base += 32) {
       const int chi = min(__shfl_sync(0xffffffffu, c, 31), C - 1);
       __syncwarp();  // the previous step's reads and adds are done
-      while (staged <= chi) {
-        const int sl = staged & 3;
-        S.x[sl][lane] = q0.x;
-        S.y[sl][lane] = q0.y;
-        S.z[sl][lane] = q0.z;
-        S.m[sl][lane] = q0.w;
-        q0 = q1;
-        ++staged;
-        if (staged + 1 < C) q1 = fetch((staged + 1) * 32 + lane);
-      }
+      // chunks up to chi are needed now; chi + 1 is copied ahead.  The slot
+      // of chunk k held chunk k - 4 <= chi - 3, older than any chunk a step
+      // spanning at most three chunks reads.
+      const int want = min(chi + 1, C - 1);
+      while (staged <= want) stage_chunk(staged++);
+      if (staged - 1 > chi)
+        cp_async_wait_one();  // all but the chunk copied ahead
+      else
+        cp_async_wait_all();
       __syncwarp();
       const int sl = c & 3;
-      const float4 v = chunk_sums<POT, false>(S.x[sl], S.y[sl], S.z[sl], S.m[sl], S.tp[t], -1, eps2);
+      const float4 v = chunk_sums<POT, false, CH>(S.x[sl], S.y[sl], S.z[sl], S.m[sl], S.tp[t], -1, eps2);
       float4 v2;
       v2.x = __shfl_down_sync(0xffffffffu, v.x, nt);
       v2.y = __shfl_down_sync(0xffffffffu, v.y, nt);
@@ -1033,6 +1062,7 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
         c += 1;
       }
     }
+    cp_async_wait_all();  // nothing left in flight (the ring is reused by the next unit)
   }
   __syncwarp();
   if (tgt) {
@@ -1298,10 +1328,10 @@ struct RunLeafEval {
                                                                     ranges, G, eps2, out, partial, max_slots, err,
                                                                     rung, lw, nlw);
     else if (flat) {
-      // 15 KB of shared memory per block: ask for a carveout that holds the
-      // eight blocks per SM the launch bounds allow.
-      static const cudaError_t carve =
-          cudaFuncSetAttribute(k_leaf_units_flat<K, PT>, cudaFuncAttributePreferredSharedMemoryCarveout, 60);
+      // 23.5 KB of shared memory per block: ask for the carveout that holds
+      // the eight blocks per SM the launch bounds allow.
+      static const cudaError_t carve = cudaFuncSetAttribute(
+          k_leaf_units_flat<K, PT>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
       (void)carve;
       k_leaf_units_flat<K, PT><<<nb, 32 * kWarpsPerBlock, 0, st>>>(pos4, num_internal, num_units, units, aux, runs,
                                                                    ranges, G, eps2, out, partial, max_slots, err);

@@ -31,9 +31,8 @@ _lib = None
 
 def build(force: bool = False) -> Path:
     """Compile the oracle library with ``make`` (g++ -O3 -fopenmp)."""
-    if force or not _LIB_PATH.exists() or (
-        _LIB_PATH.stat().st_mtime < (_HERE / "fmm_oracle.cpp").stat().st_mtime
-    ):
+    srcs = [_HERE / "fmm_oracle.cpp", _HERE / "tree_oracle.cpp"]
+    if force or not _LIB_PATH.exists() or any(_LIB_PATH.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-s", "-C", str(_HERE)], check=True)
     return _LIB_PATH
 
@@ -224,6 +223,22 @@ class Pass:
             _p(self.leaf_of), ctypes.c_int64(nt), _p(ts), dt(G), dt(eps2), _p(acc), _p(pot))
         return acc, pot
 
+    def evaluate_range(self, p, pos, mass, centers, loc, leaf_lo, leaf_hi, G, eps2):
+        """evaluate() for the leaves [leaf_lo, leaf_hi) only; the other rows of
+        the returned (N, 3) array are zero."""
+        pos = _c(pos, self.dtype)
+        mass = _c(mass, self.dtype)
+        centers = _c(centers, self.dtype)
+        loc = _c(loc, self.dtype)
+        acc = np.zeros((pos.shape[0], 3), dtype=self.dtype)
+        dt = ctypes.c_double if self.dtype == np.float64 else ctypes.c_float
+        getattr(lib(), f"oracle_evaluate_range_{self.sfx}")(
+            ctypes.c_int(p), _p(pos), _p(mass), ctypes.c_int(self.t.num_nodes),
+            ctypes.c_int(self.t.num_internal), _p(self.ranges), _p(centers), _p(loc),
+            _p(self.near_off), _p(self.near_leaf), dt(G), dt(eps2), ctypes.c_int(leaf_lo),
+            ctypes.c_int(leaf_hi), _p(acc), None)
+        return acc
+
     def run(self, p, pos_sorted, mass_sorted, G=1.0, eps2=0.0):
         """Whole pass on sorted particles; returns a dict of every stage."""
         centers = self.com(pos_sorted, mass_sorted)
@@ -232,6 +247,50 @@ class Pass:
         loc = self.l2l_cascade(p, centers, loc)
         acc, pot = self.evaluate(p, pos_sorted, mass_sorted, centers, loc, G, eps2)
         return {"centers": centers, "multipoles": mult, "locals": loc, "acc": acc, "pot": pot}
+
+
+_TREE_FIELDS = (("permutation", np.int64, "n"), ("node_ranges", np.int32, "2nodes"),
+                ("left_child", np.int32, "internal"), ("right_child", np.int32, "internal"),
+                ("parent", np.int32, "nodes"), ("node_level", np.int32, "nodes"),
+                ("level_offsets", np.int32, "levels+1"), ("leaf_of_particle", np.int32, "n"),
+                ("far_offsets", np.int64, "nodes+1"), ("far_sources", np.int32, "far"),
+                ("near_offsets", np.int64, "leaves+1"), ("near_leaves", np.int32, "near"),
+                ("centers_f64", np.float64, "3nodes"), ("radii_f64", np.float64, "nodes"))
+
+
+def tree_build(pos, mass, leaf_size, theta):
+    """The oracle's own tree + lists (oracle/tree_oracle.cpp, a transcription
+    of oracle/tree.py): a namespace with the Topology fields that Pass reads."""
+    from types import SimpleNamespace
+
+    pos = _c(pos, np.float64).reshape(-1, 3)
+    mass = _c(mass, np.float64).reshape(-1)
+    n = pos.shape[0]
+    sizes = np.zeros(6, np.int64)
+    f = lib().oracle_tree_build
+    f.restype = ctypes.c_void_p
+    h = f(ctypes.c_int64(n), _p(pos), _p(mass), ctypes.c_int(int(leaf_size)), ctypes.c_double(float(theta)),
+          _p(sizes))
+    if not h:
+        raise ValueError("oracle_tree_build: bad arguments")
+    nodes, internal, leaves, levels, far, near = (int(v) for v in sizes)
+    dims = {"n": n, "2nodes": 2 * nodes, "internal": internal, "nodes": nodes, "levels+1": levels + 1,
+            "nodes+1": nodes + 1, "far": far, "leaves+1": leaves + 1, "near": near, "3nodes": 3 * nodes}
+    out = SimpleNamespace(num_particles=n, num_nodes=nodes, num_internal=internal, num_leaves=leaves,
+                          num_levels=levels, leaf_size=int(leaf_size), theta=float(theta))
+    try:
+        for fid, (name, dt, dim) in enumerate(_TREE_FIELDS):
+            a = np.empty(max(dims[dim], 1), dtype=dt)
+            if lib().oracle_tree_copy(ctypes.c_void_p(h), ctypes.c_int(fid), _p(a)) != 0:
+                raise RuntimeError(f"oracle_tree_copy({name})")
+            setattr(out, name, a[:dims[dim]])
+    finally:
+        lib().oracle_tree_free(ctypes.c_void_p(h))
+    out.node_ranges = out.node_ranges.reshape(-1, 2)
+    out.centers_f64 = out.centers_f64.reshape(-1, 3)
+    out.inverse_permutation = np.empty_like(out.permutation)
+    out.inverse_permutation[out.permutation] = np.arange(n, dtype=np.int64)
+    return out
 
 
 def direct_sum(pos, mass, targets=None, G=1.0, eps2=0.0):

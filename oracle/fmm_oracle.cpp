@@ -525,11 +525,12 @@ static void p2p_leaf_pair(const T* pos, const T* mass, int t0, int t1, int s0, i
 template <typename T>
 static void evaluate(int p, const T* pos, const T* mass, int num_nodes, int num_internal,
                      const int* ranges, const T* centers, const T* loc, const int64_t* near_off,
-                     const int* near_leaf, T G, T eps2, T* acc_out, T* pot_out) {
+                     const int* near_leaf, T G, T eps2, T* acc_out, T* pot_out, int leaf_lo = 0, int leaf_hi = -1) {
   const int C = sh_size(p);
   const int L = num_nodes - num_internal;
+  if (leaf_hi < 0) leaf_hi = L;
 #pragma omp parallel for schedule(dynamic, 8)
-  for (int lf = 0; lf < L; ++lf) {
+  for (int lf = leaf_lo; lf < leaf_hi; ++lf) {
     const int node = num_internal + lf;
     const int t0 = ranges[2 * node], t1 = ranges[2 * node + 1];
     const int nt = t1 - t0 + 1;
@@ -632,6 +633,14 @@ static void evaluate_targets(int p, const T* pos, const T* mass, int num_interna
                                         const int* near_leaf, T G, T eps2, T* acc, T* pot) {     \
     orc::ensure_tables(p); orc::evaluate(p, pos, mass, num_nodes, num_internal, ranges, centers, loc, near_off,         \
                   near_leaf, G, eps2, acc, pot);                                                 \
+  }                                                                                              \
+  ORC_EXPORT void oracle_evaluate_range_##SFX(int p, const T* pos, const T* mass, int num_nodes,  \
+                                              int num_internal, const int* ranges,               \
+                                              const T* centers, const T* loc,                    \
+                                              const int64_t* near_off, const int* near_leaf, T G, \
+                                              T eps2, int leaf_lo, int leaf_hi, T* acc, T* pot) { \
+    orc::ensure_tables(p); orc::evaluate(p, pos, mass, num_nodes, num_internal, ranges, centers, loc, near_off,         \
+                  near_leaf, G, eps2, acc, pot, leaf_lo, leaf_hi);                               \
   }                                                                                              \
   ORC_EXPORT void oracle_evaluate_targets_##SFX(                                                 \
       int p, const T* pos, const T* mass, int num_internal, const int* ranges,                   \

@@ -63,3 +63,35 @@ def test_host_builder_matches_the_oracle_bit_for_bit(case):
     t = tree.build_topology(pos, mass, leaf_size=leaf, theta=theta)
     compare(topo_fields(t), want, str(case))
     assert t.num_levels == want["num_levels"]
+
+
+@pytest.mark.parametrize("kind,n,leaf,theta", [("clustered", 3000, 8, 0.6), ("uniform", 2000, 16, 0.5),
+                                               ("plummer", 4000, 32, 0.7), ("uniform", 1, 8, 0.6)])
+def test_compiled_oracle_tree_equals_the_scalar_restatement(kind, n, leaf, theta):
+    """oracle/tree_oracle.cpp (the oracle's fast tree, used by the benchmark's
+    CPU legs) transcribes oracle/tree.py: the same arrays bit for bit."""
+    import oracle
+    from jaccpot_b200 import workloads
+    from oracle import tree as otree
+
+    pos, mass = workloads.GENERATORS[kind](n, 3)
+    a = oracle.tree_build(pos, mass, leaf, theta)
+    b = otree.build(pos, mass, leaf, theta)
+    for k, v in b.items():
+        if k == "num_levels":
+            assert a.num_levels == v
+        else:
+            assert np.array_equal(getattr(a, k), v), k
+
+
+def test_compiled_oracle_tree_equals_the_product_host_builder():
+    import oracle
+    from jaccpot_b200 import tree, workloads
+
+    pos, mass = workloads.clustered(100_000, 9)
+    a = oracle.tree_build(pos, mass, 32, 0.55)
+    h = tree.build_topology(pos, mass, leaf_size=32, theta=0.55)
+    for k in ("permutation", "node_ranges", "left_child", "right_child", "parent", "node_level", "level_offsets",
+              "leaf_of_particle", "far_offsets", "far_sources", "near_offsets", "near_leaves", "centers_f64",
+              "radii_f64"):
+        assert np.array_equal(getattr(a, k), getattr(h, k)), k
