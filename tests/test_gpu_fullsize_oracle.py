@@ -1,0 +1,146 @@
+"""The benchmark configurations at their full sizes against the FP64 oracle
+(the C++/OpenMP restatement, on the same topology): every acceleration of
+the Plummer 1M p=6 pass and its 65,536-target subset; a 4,096-target sample
+of the clustered 4M p=8 pass in the plain form and in the error-controlled
+form (same lists, every far pair at its gear); and the config-5 adjoint at
+N = 1,048,576 through a directional derivative -- the FP64 central
+difference of L = sum w . a along a random direction against <grad L, v>
+from the hand-written VJP."""
+
+from __future__ import annotations
+
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover - CPU container
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import oracle  # noqa: E402
+from jaccpot_b200 import FastMultipoleMethod, _lib, engine, workloads  # noqa: E402
+
+ACC_P99 = 1e-5  # FP32 kernels vs the FP64 oracle on the same lists (north star's FP32-mode bound)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _threads():
+    import os
+
+    oracle.build()
+    oracle.set_threads(os.cpu_count() or 1)
+
+
+def test_plummer_1m_p6_every_acceleration_and_the_target_subset():
+    n = 1048576
+    pos, mass = workloads.plummer(n, 0)
+    fmm = FastMultipoleMethod(preset="large_n_gpu", theta=0.6, G=1.0, softening=0.0)
+    st = fmm.prepare_state(pos, mass, leaf_size=32, max_order=6)
+    got = fmm.evaluate_prepared_state(st)
+    topo = st.topology
+    perm = topo.permutation
+    P = oracle.Pass(topo, np.float64)
+    res = P.run(6, pos[perm].astype(np.float64), mass[perm].astype(np.float64))
+    want = np.empty_like(res["acc"])
+    want[perm] = res["acc"]
+    err = workloads.relative_errors(got, want)
+    assert np.percentile(err, 99) <= ACC_P99, np.percentile(err, [50, 99, 100])
+    tg = np.random.default_rng(2).choice(n, 65536, replace=False).astype(np.int32)
+    sub = fmm.evaluate_prepared_state(st, target_indices=tg)
+    ts = topo.inverse_permutation[tg].astype(np.int32)
+    acc_t, _ = P.evaluate_targets(6, pos[perm].astype(np.float64), mass[perm].astype(np.float64),
+                                  res["centers"], res["locals"], ts, 1.0, 0.0)
+    err = workloads.relative_errors(sub, acc_t)
+    assert np.percentile(err, 99) <= ACC_P99, np.percentile(err, [50, 99, 100])
+
+
+def _oracle_targets(topo, pos_s, mass_s, p, ts, gears=None, orders=None):
+    """FP64 oracle accelerations at sorted targets `ts`: the whole upward
+    sweep, M2L over the far list (far pair e at order orders[gears[e]] when
+    gears are given), L2L, then L2P + P2P at the targets."""
+    P = oracle.Pass(topo, np.float64)
+    centers = P.com(pos_s, mass_s)
+    mult = P.upward(p, pos_s, mass_s, centers)
+    if gears is None:
+        loc = P.m2l_accumulate(p, mult, centers)
+    else:
+        loc = np.zeros_like(mult)
+        tgt = topo.far_pair_targets()
+        for gi, q in enumerate(orders):
+            m = gears == gi
+            if not m.any():
+                continue
+            off = np.zeros(topo.num_nodes + 1, np.int64)
+            np.add.at(off, tgt[m].astype(np.int64) + 1, 1)
+            sub = SimpleNamespace(**{k: getattr(topo, k) for k in (
+                "num_nodes", "num_internal", "num_levels", "node_ranges", "left_child", "right_child",
+                "level_offsets", "near_offsets", "near_leaves", "leaf_of_particle")})
+            sub.far_offsets, sub.far_sources = np.cumsum(off), topo.far_sources[m]
+            C = (q + 1) ** 2
+            loc[:, :C] += oracle.Pass(sub, np.float64).m2l_accumulate(q, np.ascontiguousarray(mult[:, :C]),
+                                                                       centers)
+    loc = P.l2l_cascade(p, centers, loc)
+    acc, _ = P.evaluate_targets(p, pos_s, mass_s, centers, loc, ts, 1.0, 0.0)
+    return acc
+
+
+@pytest.mark.parametrize("form", ["plain", "error_controlled"])
+def test_clustered_4m_p8_targets_against_the_oracle(form):
+    n = 4194304
+    pos, mass = workloads.clustered(n, 0)
+    if form == "plain":
+        fmm = FastMultipoleMethod(theta=0.55, G=1.0, softening=0.0)
+    else:
+        fmm = FastMultipoleMethod(theta=0.6, G=1.0, softening=0.0, adaptive_order=True, p_gears=(2, 4, 6, 8),
+                                  adaptive_error_model="dehnen_paper", adaptive_eps=3e-5,
+                                  mac_force_scale_mode="paper", nearfield_compensated=True)
+    st = fmm.prepare_state(pos, mass, leaf_size=32, max_order=8)
+    topo = st.topology
+    tg = np.random.default_rng(4).choice(n, 4096, replace=False)
+    ts = topo.inverse_permutation[tg].astype(np.int32)
+    got = st.pass_.evaluate()[torch.from_numpy(ts.astype(np.int64)).cuda(), :3].double().cpu().numpy()
+    perm = topo.permutation
+    want = _oracle_targets(topo, pos[perm].astype(np.float64), mass[perm].astype(np.float64), 8, ts,
+                           gears=topo.far_gears, orders=topo.gear_orders)
+    err = workloads.relative_errors(got, want)
+    assert np.percentile(err, 99) <= ACC_P99, np.percentile(err, [50, 99, 100])
+
+
+def test_adjoint_directional_derivative_at_plummer_1m_p6():
+    """d/dh L(x + h v, m + h u) at h = 0 by FP64 central differences of the
+    oracle's forward pass on the same (fixed) topology, against
+    <grad_x L, v> + <grad_m L, u> from the GPU's VJP."""
+    n = 1048576
+    pos, mass = workloads.plummer(n, 0)
+    fmm = FastMultipoleMethod(preset="large_n_gpu", theta=0.6, G=1.0, softening=0.0)
+    st = fmm.prepare_state(pos, mass, leaf_size=32, max_order=6)
+    ps, topo = st.pass_, st.topology
+    rng = np.random.default_rng(5)
+    w = rng.normal(size=(n, 3)).astype(np.float32)
+    v = rng.normal(size=(n, 3))
+    u = rng.normal(size=n)
+    d_pos, d_mass = torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda()
+    ps.load_particles(d_pos, d_mass)
+    gx, gm = torch.empty_like(d_pos), torch.empty_like(d_mass)
+    ps.vjp(torch.from_numpy(w).cuda(), gx, gm, recompute=True)
+    perm = topo.permutation
+    P = oracle.Pass(topo, np.float64)
+    hx = 1e-3 * 1e-2  # 1e-3 of the inner inter-particle spacing (~0.01 at r < 1)
+    hm = 1e-3 * float(mass[0])
+
+    def L(h):
+        x = pos.astype(np.float64) + h * hx * v
+        m = mass.astype(np.float64) + h * hm * u
+        acc = P.run(6, x[perm], m[perm])["acc"]
+        return float((acc * w[perm].astype(np.float64)).sum())
+
+    fd = (L(1.0) - L(-1.0)) / 2.0  # change of L over the step (hx v, hm u)
+    gxn, gmn = gx.double().cpu().numpy(), gm.double().cpu().numpy()
+    lin = float((gxn * (hx * v)).sum() + (gmn * (hm * u)).sum())
+    assert np.isfinite(lin) and np.isfinite(fd)
+    rel = abs(fd - lin) / abs(fd)
+    assert rel <= 1e-3, (fd, lin, rel)
