@@ -657,6 +657,15 @@ def main() -> None:
     pe1.record(stream)
     torch.cuda.synchronize()
     fp32_peak = 2.0 * 148 * 8 * 256 * iters * 8 / (pe0.elapsed_time(pe1) / 1e3) / 1e12
+    # the pair rate the FP32 + MUFU pipes allow for the near field's exact
+    # instruction mix, on register-resident data (probe mode 3: 24 pairs per
+    # thread and iteration)
+    _lib.lib().jb_probe_throughput(148 * 8, 16, 3, sink.data_ptr(), stream.cuda_stream)
+    pe0.record(stream)
+    _lib.lib().jb_probe_throughput(148 * 8, 512, 3, sink.data_ptr(), stream.cuda_stream)
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    mix_pairs_per_s = 148 * 8 * 256 * 512 * 24 / (pe0.elapsed_time(pe1) / 1e3)
     stage_names = ["upward", "m2l", "l2l", "leaf_eval", "unsort"]
     dom = int(np.argmax(stage_chosen))
     split_m2l = False
@@ -674,9 +683,12 @@ def main() -> None:
                 "traffic": _traffic("k_m2l_units", atopo.num_far_pairs)}
     else:
         ach = p2p_flops / (stage_chosen[3] / 1e3) / 1e12
+        pairs_per_s = near_inter / (stage_chosen[3] / 1e3)
         roof = {"kernel": "k_leaf_units_flat<kahan> (leaf stage: + k_leaf_l2p, k_leaf_reduce)", "bound": "fp32",
                 "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
-                "traffic": _traffic("k_leaf_units_flat", near_inter)}
+                "traffic": _traffic("k_leaf_units_flat", near_inter),
+                "pairs_per_s": pairs_per_s, "mix_peak_pairs_per_s": mix_pairs_per_s,
+                "frac_of_mix_peak": pairs_per_s / mix_pairs_per_s}
     roof["peak_source"] = ("measured bf16 burst (MEASURED_PEAKS.json)" if roof["bound"] == "tensor" else
                            "in-run FP32 FMA probe (MEASURED_PEAKS.json has HBM and bf16 only)")
     roof["stage_ms"] = float(stage_chosen[dom])

@@ -510,7 +510,10 @@ JB_API int jb_direct_f64(int64_t n, const float* pos4, int64_t num_targets, cons
                          double eps2, double* out4, void* stream);
 
 /* Pipe-throughput probe: blocks x 256 threads x iters x 8 dependent-chain
- * FMAs (use_mufu = 0) or rsqrt (use_mufu = 1).  Time it with events. */
+ * FMAs (use_mufu = 0), rsqrt (1) or packed f32x2 FMAs (2); or (3) the near
+ * field's particle-pair arithmetic on register-resident data, 24 pairs per
+ * thread and iteration (the pair rate the FP32 + MUFU pipes allow for that
+ * instruction mix).  Time it with events. */
 JB_API int jb_probe_throughput(int blocks, int iters, int use_mufu, float* sink, void* stream);
 
 #ifdef __cplusplus

@@ -175,8 +175,83 @@ __global__ void __launch_bounds__(256) k_direct_f64(int64_t n, const float4* __r
   }
 }
 
-// Throughput probe: FP32 FMA chains (8 independent per thread) or MUFU rsqrt.
+// Throughput probe.  mode 0: FP32 FMA chains (8 independent per thread);
+// 1: MUFU rsqrt chains; 2: packed f32x2 FMA chains (8 per thread); 3: the
+// near field's particle-pair arithmetic on register-resident sources (the
+// packed step of chunk_sums: 2 pairs per step, 3 targets' accumulators) --
+// the pair rate the FP32 and MUFU pipes allow for that instruction mix.
 __global__ void k_probe(int iters, int use_mufu, float* out) {
+  if (use_mufu == 2) {
+    f32x2 a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = f2(1.0f + 1e-3f * (threadIdx.x + k), 1.0f - 1e-3f * k);
+    const f32x2 b = f2(0.999f, 0.999f), c = f2(1e-4f, 1e-4f);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = f2_fma(a[k], b, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      float lo, hi;
+      f2_split(a[k], lo, hi);
+      s += lo + hi;
+    }
+    if (s == 12345.678f) out[threadIdx.x] = s;
+    return;
+  }
+  if (use_mufu == 3) {
+    f32x2 sx[4], sy[4], sz[4], sm[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      sx[k] = f2(0.1f * k + 1e-3f * threadIdx.x, 0.2f * k);
+      sy[k] = f2(0.3f * k, 0.1f + 0.05f * k);
+      sz[k] = f2(-0.2f * k, 0.4f);
+      sm[k] = f2(1e-3f, 2e-3f);
+    }
+    const f32x2 E2 = f2(1e-4f, 1e-4f);
+    f32x2 TX[3], TY[3], TZ[3], AX[3], AY[3], AZ[3];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      TX[t] = f2(1.f + t, 1.f + t);
+      TY[t] = f2(2.f, 2.f);
+      TZ[t] = f2(0.5f * t, 0.5f * t);
+      AX[t] = AY[t] = AZ[t] = f2(0.f, 0.f);
+    }
+    const f32x2 step = f2(1e-6f, -1e-6f);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {  // the targets move, so nothing is loop-invariant
+        TX[t] = f2_add(TX[t], step);
+        TY[t] = f2_add(TY[t], step);
+        TZ[t] = f2_add(TZ[t], step);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+          const f32x2 dx = f2_sub(TX[t], sx[k]), dy = f2_sub(TY[t], sy[k]), dz = f2_sub(TZ[t], sz[k]);
+          const f32x2 d2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, E2)));
+          float d2a, d2b;
+          f2_split(d2, d2a, d2b);
+          const f32x2 ir = f2(rsqrt_ftz(d2a), rsqrt_ftz(d2b));
+          const f32x2 w = f2_mul(f2_mul(sm[k], ir), f2_mul(ir, ir));
+          AX[t] = f2_fma(w, dx, AX[t]);
+          AY[t] = f2_fma(w, dy, AY[t]);
+          AZ[t] = f2_fma(w, dz, AZ[t]);
+        }
+      }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      float lo, hi;
+      f2_split(f2_add(f2_add(AX[t], AY[t]), AZ[t]), lo, hi);
+      s += lo + hi;
+    }
+    if (s == 12345.678f) out[threadIdx.x] = s;
+    return;
+  }
   float a[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) a[k] = 1.0f + 1e-3f * (threadIdx.x + k);

@@ -857,8 +857,8 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
 // f = c * nt + t, 32 items per warp step, lane l of step s takes item 32 s + l
 // (target f mod nt against chunk f / nt).  A step spans at most three
 // consecutive chunks (nt >= 17), so the chunks sit in a ring of four
-// shared-memory slots, laid out (ring_pos) so that what one load instruction
-// reads from them is a single shared-memory wavefront.  Each chunk is copied into its slot by cp.async
+// shared-memory slots, padded so that the slots one load instruction reads
+// fall in different banks.  Each chunk is copied into its slot by cp.async
 // (four 4-byte copies per source: the ring is one array per coordinate, so
 // that a 16-byte load yields two packed source pairs), one chunk ahead of the
 // chunks the step reads, so no register holds a source in flight.  The
@@ -867,19 +867,12 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
 // straight after its own, so every target receives its chunk partials in
 // chunk order through one (compensated) add per 64 sources.
 // ---------------------------------------------------------------------------
-constexpr int kFlatChunk = 64;  // sources per chunk (item)
-// The ring, one array per coordinate: source q of slot sl at
-//   ring_pos(sl, q) = 16 (q / 4) + 4 ((sl + q / 8) mod 4) + q mod 4,
-// so quad q / 4 of all four slots shares one 64-byte span.  The up to three
-// slots a step reads then cost a 16-byte load one shared-memory wavefront
-// (one 128-byte segment) instead of one per slot, and the rotation by q / 8
-// spreads one slot's 32 staged floats over all 32 banks.
-constexpr int kRingFloats = 4 * kFlatChunk;
-__host__ __device__ constexpr int ring_pos(int sl, int q) { return 16 * (q >> 2) + 4 * ((sl + (q >> 3)) & 3) + (q & 3); }
+constexpr int kFlatChunk = 64;                // sources per chunk (item)
+constexpr int kFlatSlot = kFlatChunk + 4;     // slot stride (floats): the three slots one load reads use distinct banks
 struct alignas(16) FlatStage {
-  float x[kRingFloats], y[kRingFloats], z[kRingFloats], m[kRingFloats];  // source chunk ring
-  float4 tp[32];                                                        // target positions
-  float4 s[32], c[32];                                                  // per-target sums and compensations
+  float x[4][kFlatSlot], y[4][kFlatSlot], z[4][kFlatSlot], m[4][kFlatSlot];  // source chunk ring
+  float4 tp[32];                                                            // target positions
+  float4 s[32], c[32];                                                      // per-target sums and compensations
 };
 
 union WarpStage {
@@ -945,56 +938,6 @@ __device__ __forceinline__ float4 chunk_sums(const float* xs, const float* ys, c
   return make_float4(x0 + x1, y0 + y1, z0 + z1, POT ? w0 + w1 : 0.f);
 }
 
-// chunk_sums over slot sl of the ring (NS sources: the swizzled layout of
-// ring_pos); the same arithmetic in the same order.
-template <bool POT, bool SELF, int NS>
-__device__ __forceinline__ float4 ring_sums(const FlatStage& S, int sl, float4 ti, int self_j, float eps2) {
-  const f32x2 TX = f2(ti.x, ti.x), TY = f2(ti.y, ti.y), TZ = f2(ti.z, ti.z), E2 = f2(eps2, eps2);
-  f32x2 AX = f2(0.f, 0.f), AY = AX, AZ = AX, AW = AX;
-  auto step = [&](f32x2 sx, f32x2 sy, f32x2 sz, f32x2 sm, int j0) {
-    const f32x2 dx = f2_sub(TX, sx);
-    const f32x2 dy = f2_sub(TY, sy);
-    const f32x2 dz = f2_sub(TZ, sz);
-    const f32x2 d2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, E2)));
-    float d2a, d2b;
-    f2_split(d2, d2a, d2b);
-    const f32x2 ir = f2(rsqrt_ftz(d2a), rsqrt_ftz(d2b));
-    f32x2 mir = f2_mul(sm, ir);
-    f32x2 w = f2_mul(mir, f2_mul(ir, ir));
-    if (SELF) {
-      float m0, m1, w0, w1;
-      f2_split(mir, m0, m1);
-      f2_split(w, w0, w1);
-      m0 = (j0 == self_j) ? 0.f : m0;
-      w0 = (j0 == self_j) ? 0.f : w0;
-      m1 = (j0 + 1 == self_j) ? 0.f : m1;
-      w1 = (j0 + 1 == self_j) ? 0.f : w1;
-      mir = f2(m0, m1);
-      w = f2(w0, w1);
-    }
-    AX = f2_fma(w, dx, AX);
-    AY = f2_fma(w, dy, AY);
-    AZ = f2_fma(w, dz, AZ);
-    if (POT) AW = f2_add(AW, mir);
-  };
-#pragma unroll
-  for (int v = 0; v < NS / 4; ++v) {
-    const int o = 16 * v + 4 * ((sl + (v >> 1)) & 3);
-    const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(S.x + o);
-    const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(S.y + o);
-    const ulonglong2 z = *reinterpret_cast<const ulonglong2*>(S.z + o);
-    const ulonglong2 m = *reinterpret_cast<const ulonglong2*>(S.m + o);
-    step(x.x, y.x, z.x, m.x, 4 * v);
-    step(x.y, y.y, z.y, m.y, 4 * v + 2);
-  }
-  float x0, x1, y0, y1, z0, z1, w0 = 0.f, w1 = 0.f;
-  f2_split(AX, x0, x1);
-  f2_split(AY, y0, y1);
-  f2_split(AZ, z0, z1);
-  if (POT) f2_split(AW, w0, w1);
-  return make_float4(x0 + x1, y0 + y1, z0 + z1, POT ? w0 + w1 : 0.f);
-}
-
 // Adds one chunk's sums into target t's accumulator in shared memory.
 template <bool KAHAN, bool POT>
 __device__ __forceinline__ void flat_add(FlatStage& S, int t, float4 v) {
@@ -1026,14 +969,13 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
   S.s[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (KAHAN) S.c[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (aux.y & 1) {  // the self block, lane per target, diagonal excluded
-    const int q = ring_pos(0, lane);
-    S.x[q] = me.x;
-    S.y[q] = me.y;
-    S.z[q] = me.z;
-    S.m[q] = me.w;
+    S.x[0][lane] = me.x;
+    S.y[0][lane] = me.y;
+    S.z[0][lane] = me.z;
+    S.m[0][lane] = me.w;
     __syncwarp();
     const float4 ti = tgt ? me : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 v = ring_sums<POT, true, 32>(S, 0, ti, lane, eps2);
+    const float4 v = chunk_sums<POT, true>(S.x[0], S.y[0], S.z[0], S.m[0], ti, lane, eps2);
     if (tgt) flat_add<KAHAN, POT>(S, lane, v);
   }
   const int nsrc = U.w;
@@ -1050,18 +992,17 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
         ++r;
         run = runs[r];
       }
-      const int o = ring_pos(sl, q);
       if (f < nsrc) {
         const float* src = reinterpret_cast<const float*>(pos4 + run.x + (f - rbase));
-        cp_async4(S.x + o, src);
-        cp_async4(S.y + o, src + 1);
-        cp_async4(S.z + o, src + 2);
-        cp_async4(S.m + o, src + 3);
+        cp_async4(&S.x[sl][q], src);
+        cp_async4(&S.y[sl][q], src + 1);
+        cp_async4(&S.z[sl][q], src + 2);
+        cp_async4(&S.m[sl][q], src + 3);
       } else {
-        S.x[o] = 1e18f;
-        S.y[o] = 1e18f;
-        S.z[o] = 1e18f;
-        S.m[o] = 0.f;
+        S.x[sl][q] = 1e18f;
+        S.y[sl][q] = 1e18f;
+        S.z[sl][q] = 1e18f;
+        S.m[sl][q] = 0.f;
       }
     };
     auto stage_chunk = [&](int k) {  // one cp.async group per chunk
@@ -1087,7 +1028,7 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
         cp_async_wait_all();
       __syncwarp();
       const int sl = c & 3;
-      const float4 v = ring_sums<POT, false, CH>(S, sl, S.tp[t], -1, eps2);
+      const float4 v = chunk_sums<POT, false, CH>(S.x[sl], S.y[sl], S.z[sl], S.m[sl], S.tp[t], -1, eps2);
       float4 v2;
       v2.x = __shfl_down_sync(0xffffffffu, v.x, nt);
       v2.y = __shfl_down_sync(0xffffffffu, v.y, nt);

@@ -68,23 +68,3 @@ def test_chunk_major_walk_invariants(nt):
         adds = walk(nt, C)
         for tt in range(nt):
             assert adds[tt] == list(range(C)), (nt, C, tt)
-
-
-def ring_pos(sl: int, q: int) -> int:
-    """Position of source q of ring slot sl (ring_pos in fmm_kernels.cuh)."""
-    return 16 * (q >> 2) + 4 * ((sl + (q >> 3)) & 3) + (q & 3)
-
-
-def test_ring_layout():
-    """The chunk ring (4 slots x 64 sources per coordinate): a bijection onto
-    256 floats; quad v of every slot in one 64-byte span (so the up to three
-    slots one 16-byte load reads are one 128-byte segment); the 32 floats one
-    staging instruction writes into a slot fall in 32 different banks."""
-    assert sorted(ring_pos(sl, q) for sl in range(4) for q in range(64)) == list(range(256))
-    for v in range(16):
-        assert {ring_pos(sl, 4 * v) // 16 for sl in range(4)} == {v}
-        for sl in range(4):
-            assert [ring_pos(sl, 4 * v + w) for w in range(4)] == [ring_pos(sl, 4 * v) + w for w in range(4)]
-    for sl in range(4):
-        for half in (0, 32):
-            assert len({ring_pos(sl, half + lane) % 32 for lane in range(32)}) == 32
