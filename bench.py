@@ -376,7 +376,60 @@ def measure_extras(dev, stream) -> dict:
     out["plummer_1M_p6_adjoint"] = {"forward_ms": ms_f, "vjp_ms_incl_recompute": ms_b,
                                     "ratio": ms_b / ms_f,
                                     "finite": bool(torch.isfinite(gx).all() and torch.isfinite(gm).all())}
+    out["gear_selector_2M"] = measure_gear_selector(dev, stream)
     return out
+
+
+def measure_gear_selector(dev, stream, n: int = 2097152, seed: int = 200, theta: float = 0.58) -> dict:
+    """Config 4: the learned gear selector (MLP, gears 2/4/6/8) on the theta
+    lists of a clustered system of a seed it never saw, against the plain
+    maximum-order pass and against the analytic selector (the Dehnen eq. 15
+    estimate at eps = the network's training budget) on the same lists:
+    p99 against an FP64 direct sum on 4,096 targets, the error each adds to
+    the plain pass (p99 over all particles), the gear fractions, algorithmic
+    M2L flops and M2L time."""
+    import torch
+
+    from jaccpot_b200 import _lib, engine, gears, tree, workloads
+
+    if not gears.DEFAULT_MODEL.exists():
+        return None
+    model = gears.GearModel.load()
+    pos, mass = workloads.clustered(n, seed)
+    d_pos, d_mass = torch.from_numpy(pos).to(dev), torch.from_numpy(mass).to(dev)
+    topo = tree.build_topology(pos, mass, leaf_size=32, theta=theta, device=dev)
+    ps = engine.Pass(engine.DeviceTopology(topo, dev), 8, G=1.0, eps2=0.0)
+    ps.load_particles(d_pos, d_mass)
+    plain = ps.run()[:, :3].clone()
+    tg = np.random.default_rng(3).choice(n, 4096, replace=False)
+    ts = torch.from_numpy(topo.inverse_permutation[tg].astype(np.int32)).to(dev)
+    ref = torch.empty((tg.size, 4), device=dev, dtype=torch.float64)
+    _lib.check(_lib.lib().jb_direct_f64(n, ps.ws.pos4.data_ptr(), tg.size, ts.data_ptr(), 1.0, 0.0, ref.data_ptr(),
+                                        stream.cuda_stream), "jb_direct_f64")
+    ref = ref[:, :3].cpu().numpy()
+    ps.set_gears(None, None)
+    ms_plain = _events_ms(ps.m2l, stream)
+
+    def with_gears(g):
+        ps.set_gears(g, model.orders)
+        acc = ps.run()[:, :3]
+        add = (torch.linalg.vector_norm(acc - plain, dim=1) /
+               torch.linalg.vector_norm(plain, dim=1).clamp_min(1e-30)).double().cpu().numpy()
+        e = workloads.relative_errors(acc[ts.long()].double().cpu().numpy(), ref)
+        gn = g.cpu().numpy()
+        res = {"p99": float(np.percentile(e, 99)), "added_p99": float(np.percentile(add, 99)),
+               "fraction": (np.bincount(gn, minlength=len(model.orders)) / max(1, gn.size)).tolist(),
+               "m2l_flop_frac": gears.m2l_flop_fraction(gn, model.orders), "m2l_ms": _events_ms(ps.m2l, stream)}
+        ps.set_gears(None, None)
+        return res
+
+    learned = with_gears(torch.as_tensor(gears.apply_gears(ps, model)).to(dev))
+    ps.run()  # the plain pass's multipoles and accelerations for the analytic estimate
+    analytic = with_gears(gears.analytic_gears(ps, model.budget, model.orders))
+    e0 = workloads.relative_errors(plain[ts.long()].double().cpu().numpy(), ref)
+    return {"N": n, "seed": seed, "theta": theta, "far_pairs": topo.num_far_pairs, "budget": model.budget,
+            "plain": {"p99": float(np.percentile(e0, 99)), "m2l_ms": ms_plain},
+            "learned": learned, "analytic_dehnen": analytic}
 
 
 # ---------------------------------------------------------------------------

@@ -159,6 +159,16 @@ JB_API int jb_node_dehnen_power(int p, int num_nodes, const float* mult, int row
 JB_API int jb_node_force_scale(int num_nodes, int num_internal, const int* left, const int* right,
                                const int* level_offsets_host, int num_levels, const int* node_ranges,
                                const float* acc4, float* scale, void* stream);
+/* The analytic per-pair gear of a fixed far list: for every pair e =
+ * (pair_tgt[e] <- far_src[e]) the lowest gear whose eq. (15) estimate (as in
+ * jb_dtree_adaptive_walk) is below max(eps * force_scale[t], 1e-24); the
+ * highest gear where none passes (the reference's order tags for its gear
+ * buckets under dehnen_paper, runtime/_adaptive_policy.py:2352-2358).
+ * com / radius: double, the tree's (JB_TREE_CENTERS_F64 / RADII_F64). */
+JB_API int jb_far_dehnen_gears(int64_t num_pairs, const int* pair_tgt, const int* far_src, const double* com,
+                               const double* radius, int num_degrees, const double* power, const float* force_scale,
+                               double G, double eps, int num_gears, const int* gear_orders, int* gears,
+                               void* stream);
 JB_API int jb_dtree_adaptive_walk(jb_dtree* t, int num_degrees, const double* power, const float* force_scale,
                                   double G, double eps, double theta_max, int num_gears, const int* gear_orders,
                                   void* stream);

@@ -90,6 +90,7 @@ _SIGNATURES = {
     "jb_dtree_free": [_P],
     "jb_dtree_adaptive_walk": [_P, _I, _P, _P, _D, _D, _D, _I, _P, _P],
     "jb_node_dehnen_power": [_I, _I, _P, _I, _P, _P],
+    "jb_far_dehnen_gears": [_I64, _P, _P, _P, _P, _I, _P, _P, _D, _D, _I, _P, _P, _P],
     "jb_node_force_scale": [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P],
     "jb_set_level_split": [_I, _I],
     "jb_set_leaf_form": [_I],

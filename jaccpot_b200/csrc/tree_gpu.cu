@@ -470,6 +470,23 @@ __global__ void k_awalk_emit(const int2* __restrict__ fr, int F, WalkCtx w, cons
   }
 }
 
+// The lowest gear whose eq. (15) estimate passes, for the given far pairs of
+// a fixed list (the analytic per-pair order choice the reference makes for
+// its gear buckets, with dehnen_paper); the highest gear where even it fails.
+__global__ void k_far_dehnen_gears(int64_t n, const int* __restrict__ pair_tgt, const int* __restrict__ far_src,
+                                   WalkCtx w, int* __restrict__ gears) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const int t = pair_tgt[e], s = far_src[e];
+  double d2 = 0;
+  for (int k = 0; k < 3; ++k) {
+    const double dd = w.com[3 * (int64_t)t + k] - w.com[3 * (int64_t)s + k];
+    d2 += dd * dd;
+  }
+  const int g = d2 > 0 ? error_gear(w, t, s, sqrt(d2), w.radius[t], w.radius[s]) : -1;
+  gears[e] = g < 0 ? w.num_gears - 1 : g;
+}
+
 // Moves the gear bits of sorted far keys into gears[] (CSR order).
 __global__ void k_take_gears(uint64_t* __restrict__ keys, int64_t n, int* __restrict__ gears) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -883,6 +900,34 @@ JB_API int jb_dtree_adaptive_walk(jb_dtree* t, int num_degrees, const double* po
     return JB_ERR_ALLOC;
   }
   return JB_OK;
+}
+
+JB_API int jb_far_dehnen_gears(int64_t num_pairs, const int* pair_tgt, const int* far_src, const double* com,
+                               const double* radius, int num_degrees, const double* power, const float* force_scale,
+                               double G, double eps, int num_gears, const int* gear_orders, int* gears,
+                               void* stream) {
+  if (num_pairs < 0 || num_degrees < 1 || num_gears < 1 || num_gears > kMaxGears || !gear_orders || !(eps > 0) ||
+      !(G > 0) || (num_pairs > 0 && (!pair_tgt || !far_src || !com || !radius || !power || !force_scale || !gears)))
+    return JB_ERR_ARG;
+  for (int g = 0; g < num_gears; ++g) {
+    const int p = gear_orders[g];
+    if (p < 0 || p > kMaxGearOrder || p >= num_degrees || (g > 0 && p <= gear_orders[g - 1])) return JB_ERR_ARG;
+  }
+  if (num_pairs == 0) return JB_OK;
+  WalkCtx w{};
+  w.com = com;
+  w.radius = radius;
+  w.power = power;
+  w.fscale = force_scale;
+  w.npow = num_degrees;
+  w.num_gears = num_gears;
+  for (int g = 0; g < num_gears; ++g) w.gear_order[g] = gear_orders[g];
+  w.G = G;
+  w.eps = eps;
+  w.theta_max = 1.0;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  k_far_dehnen_gears<<<nblocks(num_pairs, 256), 256, 0, st>>>(num_pairs, pair_tgt, far_src, w, gears);
+  return jb::cuda_status(cudaGetLastError());
 }
 
 JB_API int jb_dtree_info(const jb_dtree* t, jb_tree_info_t* info) {

@@ -142,6 +142,49 @@ def apply_gears(ps: engine.Pass, model: GearModel, symmetric: bool = False) -> n
     return gears.cpu().numpy()
 
 
+def analytic_gears(ps: engine.Pass, eps: float, orders=ORDERS) -> torch.Tensor:
+    """The method without the network: per far pair, the lowest gear whose
+    Dehnen eq. (15) error estimate is below eps x the target's force scale
+    (jb_far_dehnen_gears; runtime/_adaptive_policy.py:2352-2358), from the
+    multipoles and accelerations of the plain pass currently in the
+    workspace.  Returns int32 gear indices on the device."""
+    from . import adaptive
+
+    t, dt = ps.dt.topo, ps.dt
+    orders = tuple(int(o) for o in orders)
+    n = t.num_far_pairs
+    gears = torch.empty((max(n, 1),), device=dt.device, dtype=torch.int32)
+    if n == 0:
+        return gears[:0]
+    power = adaptive.node_dehnen_power(ps, max(orders))
+    fs = adaptive.node_force_scale(ps)
+    com = torch.from_numpy(np.ascontiguousarray(t.centers_f64)).to(dt.device)
+    rad = torch.from_numpy(np.ascontiguousarray(t.radii_f64)).to(dt.device)
+    pair_tgt = torch.from_numpy(t.far_pair_targets()).to(dt.device)
+    o = np.ascontiguousarray(np.asarray(orders, dtype=np.int32))
+    _lib.check(_lib.lib().jb_far_dehnen_gears(n, _ptr(pair_tgt), _ptr(dt.far_src), _ptr(com), _ptr(rad),
+                                              int(power.shape[1]), _ptr(power), _ptr(fs), ps.G, float(eps),
+                                              len(orders), o.ctypes.data, _ptr(gears), _stream()),
+               "jb_far_dehnen_gears")
+    return gears[:n]
+
+
+def m2l_flop_fraction(gears: np.ndarray, orders=ORDERS) -> float:
+    """Algorithmic M2L flops of a gear assignment over those of the top gear
+    for every pair (2 x (two rotation blocks + z-translation terms) per pair)."""
+    def per_pair(p):
+        rot = sum((2 * ell + 1) ** 2 for ell in range(p + 1))
+        zt = sum((2 if m else 1) * sum(1 for a in range(m, p + 1) for b in range(m, p + 1) if a + b <= p)
+                 for m in range(p + 1))
+        return 2.0 * (2 * rot + zt)
+
+    g = np.asarray(gears)
+    if g.size == 0:
+        return 1.0
+    cnt = np.bincount(g, minlength=len(orders))
+    return float(sum(c * per_pair(o) for c, o in zip(cnt, orders)) / (g.size * per_pair(orders[-1])))
+
+
 # ---------------------------------------------------------------------------
 # Training data
 # ---------------------------------------------------------------------------
