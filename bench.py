@@ -380,7 +380,7 @@ def measure_extras(dev, stream) -> dict:
     return out
 
 
-def measure_gear_selector(dev, stream, n: int = 2097152, seed: int = 200, theta: float = 0.58) -> dict:
+def measure_gear_selector(dev, stream, n: int = 2097152, seed: int = 200, theta: float = 0.55) -> dict:
     """Config 4: the learned gear selector (MLP, gears 2/4/6/8) on the theta
     lists of a clustered system of a seed it never saw, against the plain
     maximum-order pass and against the analytic selector (the Dehnen eq. 15

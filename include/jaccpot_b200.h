@@ -62,8 +62,10 @@ enum {
 };
 
 /* Most particles one leaf may hold in the leaf kernels (jb_leaf_eval*,
- * jb_adj_near).  Bits of the leaf error word (jb_leaf_eval_errors). */
-#define JB_MAX_LEAF_OCCUPANCY 32
+ * jb_adj_near; a leaf of more than 32 is evaluated in two passes of at most
+ * 32 targets); also the partial-row length (float4 per slot) of split
+ * leaves.  Bits of the leaf error word (jb_leaf_eval_errors). */
+#define JB_MAX_LEAF_OCCUPANCY 64
 enum {
   JB_LEAF_ERR_OCCUPANCY = 1, /* a unit's leaf holds more than JB_MAX_LEAF_OCCUPANCY particles: skipped */
   JB_LEAF_ERR_SLOT = 2       /* a partial-row slot at or beyond the slot count: not written / not read */
@@ -352,14 +354,14 @@ JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* 
  *                           self block and the far field of the leaf
  *   runs  int2[...]       = (first sorted particle, count): contiguous source
  *                           ranges (runs of consecutive neighbour leaves)
- * slot < 0: writes out_acc4 for the leaf's particles; slot >= 0: writes 32
- * float4 at partials[32*slot] (scratch), then split int4[num_split] = (leaf,
+ * slot < 0: writes out_acc4 for the leaf's particles; slot >= 0: writes 64
+ * float4 at partials[64*slot] (scratch), then split int4[num_split] = (leaf,
  * first slot, slot count, 0) is summed into out_acc4.  out_acc4[i] = (ax, ay,
  * az, potential) in sorted order; p2p_mode is a JB_P2P_* flag set.
  * Preconditions: every leaf a unit names holds at most JB_MAX_LEAF_OCCUPANCY
  * particles (check once with jb_validate_leaves; a unit breaking it writes
- * nothing and sets JB_LEAF_ERR_OCCUPANCY), and partials holds 32 float4 per
- * slot for every slot in aux / split. */
+ * nothing and sets JB_LEAF_ERR_OCCUPANCY), and partials holds
+ * JB_MAX_LEAF_OCCUPANCY float4 per slot for every slot in aux / split. */
 /* jb_leaf_eval with every particle pair scaled by
  * level_weights[max(rung_i, rung_j)] (rung: int32 per SORTED particle,
  * clamped to [0, num_level_weights); num_level_weights <= 32; device
@@ -391,8 +393,8 @@ JB_API int jb_leaf_eval_errors(int* flags, int clear, void* stream);
  * pass inputs and outputs.  Same arguments as jb_leaf_eval except that
  * `partials` is replaced by num_slots, which must be at least 1 + the largest
  * slot in aux and split (the schedule's slot count): the scratch is a static
- * device array of JB_LEAF_EVAL_NOALLOC_MAX_SLOTS x 32 float4 (16 MiB) that
- * every GPU loading the library holds until exit.  num_slots above the
+ * device array of JB_LEAF_EVAL_NOALLOC_MAX_SLOTS x JB_MAX_LEAF_OCCUPANCY
+ * float4 (16 MiB) that every GPU loading the library holds until exit.  num_slots above the
  * maximum returns JB_ERR_WORKSPACE; a slot at or beyond num_slots is neither
  * written nor read and sets JB_LEAF_ERR_SLOT (jb_leaf_eval_errors).  Leaves
  * as jb_leaf_eval (at most JB_MAX_LEAF_OCCUPANCY particles).  Allocates
@@ -401,7 +403,7 @@ JB_API int jb_leaf_eval_errors(int* flags, int clear, void* stream);
  * (cudaGetSymbolAddress); make that first call before any stream capture.
  * All calls share the one array: calls that overlap on the GPU (different
  * streams, no ordering between them) race. */
-#define JB_LEAF_EVAL_NOALLOC_MAX_SLOTS 32768
+#define JB_LEAF_EVAL_NOALLOC_MAX_SLOTS 16384
 JB_API int jb_leaf_eval_noalloc(int p, int p2p_mode, const float* pos4, int num_internal, int num_units,
                                 const int* units, const int* aux, const int* runs, const int* node_ranges,
                                 const float* centers, const float* locals, float G, float eps2, float* out_acc4,

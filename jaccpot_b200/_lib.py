@@ -27,8 +27,8 @@ ERRORS = {
 JB_MAX_ORDER = 10
 JB_M2L_FP32, JB_M2L_SPLIT_BF16 = 0, 1
 JB_P2P_FP32, JB_P2P_KAHAN, JB_P2P_POTENTIAL, JB_P2P_FAR_ONLY, JB_P2P_NEAR_ONLY = 0, 1, 2, 4, 8
-JB_LEAF_EVAL_NOALLOC_MAX_SLOTS = 32768
-JB_MAX_LEAF_OCCUPANCY = 32
+JB_LEAF_EVAL_NOALLOC_MAX_SLOTS = 16384
+JB_MAX_LEAF_OCCUPANCY = 64
 JB_LEAF_ERR_OCCUPANCY, JB_LEAF_ERR_SLOT = 1, 2
 (JB_SCHED_UNITS, JB_SCHED_AUX, JB_SCHED_RUNS, JB_SCHED_SPLIT, JB_SCHED_FAR_SOURCES, JB_SCHED_GEAR_OFFSETS,
  JB_SCHED_TARGETS, JB_SCHED_PAIRS_PER_GEAR) = range(8)

@@ -682,7 +682,7 @@ JB_API int jb_adj_near(const float* pos4, const float* w4, int num_internal, int
     if (rc) return rc;
   }
   if (num_split > 0) {
-    k_leaf_reduce<false><<<blocks_1d((int64_t)num_split * 32, 256), 256, 0, ST(stream)>>>(
+    k_leaf_reduce<false><<<blocks_1d((int64_t)num_split * kMaxLeaf, 256), 256, 0, ST(stream)>>>(
         num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(node_ranges),
         reinterpret_cast<const float4*>(partials), reinterpret_cast<float4*>(out_xm4), 0x7fffffff, nullptr);
     return launch_status();

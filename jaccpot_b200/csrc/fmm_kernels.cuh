@@ -41,12 +41,14 @@ extern int g_leaf_flat;
 inline int launch_status() { return cuda_status(cudaGetLastError()); }
 
 // Most particles a leaf may hold: the near-field kernels give each target of
-// a leaf one lane (or a lane group) of a warp and each split leaf one
-// partial row of kMaxLeaf float4.  A unit whose leaf holds more writes
-// nothing and sets JB_LEAF_ERR_OCCUPANCY in the error word; a partial-row
-// slot at or beyond the caller's slot count is skipped and sets
-// JB_LEAF_ERR_SLOT (jb_leaf_eval_errors reads the word).
-constexpr int kMaxLeaf = 32;
+// a leaf one lane (or a lane group) of a warp, a leaf of more than 32 in two
+// passes of at most 32 targets, and each split leaf one partial row of
+// kMaxLeaf float4.  A unit whose leaf holds more writes nothing and sets
+// JB_LEAF_ERR_OCCUPANCY in the error word; a partial-row slot at or beyond
+// the caller's slot count is skipped and sets JB_LEAF_ERR_SLOT
+// (jb_leaf_eval_errors reads the word).
+constexpr int kMaxLeaf = JB_MAX_LEAF_OCCUPANCY;
+static_assert(kMaxLeaf == 64, "leaves are evaluated in at most two passes of 32 targets");
 __device__ __forceinline__ void leaf_error(int* err, int bit) {
   if (err) atomicOr(err, bit);
 }
@@ -740,12 +742,17 @@ __device__ __forceinline__ void near_chunk(const NearStage& st, float4 ti, int h
   }
 }
 
+// The targets rg (at most 32: the leaf, or one of its two halves) of the
+// leaf whose particles are lr; row: where this pass's targets start in the
+// leaf's partial row (0 or 32).
 template <int G, bool KAHAN, bool POT, bool W, bool FTZ>
 __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
                                           const int2* __restrict__ runs, NearStage& sP, int lane, float G_,
                                           float eps2, float4* __restrict__ out, float4* __restrict__ partial,
                                           int max_slots, int* err, const int* __restrict__ rung = nullptr,
-                                          const float* tbl = nullptr, int nlw = 1) {
+                                          const float* tbl = nullptr, int nlw = 1, int2 lr = make_int2(0, -1),
+                                          int row = 0) {
+  if (lr.y < lr.x) lr = rg;
   const int tl = lane / G, h = lane % G;
   const int nt = rg.y - rg.x + 1;
   const bool active = tl < nt;
@@ -754,12 +761,15 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
   PairWeights pw{tbl, 0};
   if (W) pw.rt = active ? clamp_rung(rung[rg.x + tl]) : 0;
   NearAcc<KAHAN> a;
-  if (aux.y & 1) {
-    stage_source<G>(sP, lane, (lane < nt) ? pos4[rg.x + lane] : JB_PAD4);
-    if (W) stage_rung<G>(sP, lane, (lane < nt) ? clamp_rung(rung[rg.x + lane]) : 0);
-    __syncwarp();
-    near_chunk<G, KAHAN, POT, true, W, FTZ>(sP, ti, h, tl, eps2, a, pw);
-    __syncwarp();
+  if (aux.y & 1) {  // the self block: the leaf's particles in chunks of 32, the diagonal excluded
+    for (int b = lr.x; b <= lr.y; b += 32) {
+      const int j = b + lane;
+      stage_source<G>(sP, lane, (j <= lr.y) ? pos4[j] : JB_PAD4);
+      if (W) stage_rung<G>(sP, lane, (j <= lr.y) ? clamp_rung(rung[j]) : 0);
+      __syncwarp();
+      near_chunk<G, KAHAN, POT, true, W, FTZ>(sP, ti, h, rg.x + tl - b, eps2, a, pw);
+      __syncwarp();
+    }
   }
   const int nsrc = U.w;
   if (nsrc > 0) {
@@ -802,7 +812,7 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
       const float4 f = out[rg.x + tl];  // the far field k_leaf_l2p wrote
       out[rg.x + tl] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
     } else if (aux.x < max_slots) {
-      partial[(size_t)aux.x * kMaxLeaf + tl] = res;
+      partial[(size_t)aux.x * kMaxLeaf + row + tl] = res;
     } else {
       leaf_error(err, JB_LEAF_ERR_SLOT);
     }
@@ -833,20 +843,25 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
   const int4 U = units[u];
   const int2 ax = aux[u];
   const int2 rg = ranges[num_internal + U.x];
-  const int nt = rg.y - rg.x + 1;
-  if (nt > kMaxLeaf) {
+  const int ntl = rg.y - rg.x + 1;
+  if (ntl > kMaxLeaf) {
     if (lane == 0) leaf_error(err, JB_LEAF_ERR_OCCUPANCY);
     return;
   }
-  if (nt <= 8)
-    leaf_unit<4, KAHAN, POT, W, FTZ>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
-                                     rung, tbl, nlw);
-  else if (nt <= 16)
-    leaf_unit<2, KAHAN, POT, W, FTZ>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
-                                     rung, tbl, nlw);
-  else
-    leaf_unit<1, KAHAN, POT, W, FTZ>(pos4, rg, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
-                                     rung, tbl, nlw);
+  for (int row = 0; row < ntl; row += 32) {  // a leaf of more than 32 particles in two passes
+    const int2 rt = make_int2(rg.x + row, min(rg.y, rg.x + row + 31));
+    const int nt = rt.y - rt.x + 1;
+    if (row > 0) __syncwarp();  // the first pass's reads of the stage are done
+    if (nt <= 8)
+      leaf_unit<4, KAHAN, POT, W, FTZ>(pos4, rt, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
+                                       rung, tbl, nlw, rg, row);
+    else if (nt <= 16)
+      leaf_unit<2, KAHAN, POT, W, FTZ>(pos4, rt, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
+                                       rung, tbl, nlw, rg, row);
+    else
+      leaf_unit<1, KAHAN, POT, W, FTZ>(pos4, rt, U, ax, runs, sP[warp], lane, G, eps2, out, partial, max_slots, err,
+                                       rung, tbl, nlw, rg, row);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -960,23 +975,27 @@ template <bool KAHAN, bool POT>
 __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, int2 rg, int4 U, int2 aux,
                                                const int2* __restrict__ runs, FlatStage& S, int lane, float G_,
                                                float eps2, float4* __restrict__ out, float4* __restrict__ partial,
-                                               int max_slots, int* err) {
+                                               int max_slots, int* err, int2 lr, int row) {
   constexpr int CH = kFlatChunk;
-  const int nt = rg.y - rg.x + 1;  // 17..32
+  const int nt = rg.y - rg.x + 1;  // 17..32 targets (the leaf lr, or one of its halves)
   const bool tgt = lane < nt;
   const float4 me = tgt ? pos4[rg.x + lane] : JB_PAD4;
   S.tp[lane] = me;
   S.s[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (KAHAN) S.c[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (aux.y & 1) {  // the self block, lane per target, diagonal excluded
-    S.x[0][lane] = me.x;
-    S.y[0][lane] = me.y;
-    S.z[0][lane] = me.z;
-    S.m[0][lane] = me.w;
-    __syncwarp();
+  if (aux.y & 1) {  // the self block: the leaf's particles in chunks of 32, the diagonal excluded
     const float4 ti = tgt ? me : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 v = chunk_sums<POT, true>(S.x[0], S.y[0], S.z[0], S.m[0], ti, lane, eps2);
-    if (tgt) flat_add<KAHAN, POT>(S, lane, v);
+    for (int b = lr.x; b <= lr.y; b += 32) {
+      const float4 q = (b + lane <= lr.y) ? pos4[b + lane] : JB_PAD4;
+      __syncwarp();  // the previous chunk's reads are done
+      S.x[0][lane] = q.x;
+      S.y[0][lane] = q.y;
+      S.z[0][lane] = q.z;
+      S.m[0][lane] = q.w;
+      __syncwarp();
+      const float4 v = chunk_sums<POT, true>(S.x[0], S.y[0], S.z[0], S.m[0], ti, rg.x + lane - b, eps2);
+      if (tgt) flat_add<KAHAN, POT>(S, lane, v);
+    }
   }
   const int nsrc = U.w;
   if (nsrc > 0) {
@@ -1081,7 +1100,7 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
       const float4 f = out[rg.x + lane];  // the far field k_leaf_l2p wrote
       out[rg.x + lane] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
     } else if (aux.x < max_slots) {
-      partial[(size_t)aux.x * kMaxLeaf + lane] = res;
+      partial[(size_t)aux.x * kMaxLeaf + row + lane] = res;
     } else {
       leaf_error(err, JB_LEAF_ERR_SLOT);
     }
@@ -1103,19 +1122,25 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
   const int4 U = units[u];
   const int2 ax = aux[u];
   const int2 rg = ranges[num_internal + U.x];
-  const int nt = rg.y - rg.x + 1;
-  if (nt > kMaxLeaf) {
+  const int ntl = rg.y - rg.x + 1;
+  if (ntl > kMaxLeaf) {
     if (lane == 0) leaf_error(err, JB_LEAF_ERR_OCCUPANCY);
     return;
   }
-  if (nt <= 8)
-    leaf_unit<4, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial, max_slots,
-                                          err);
-  else if (nt <= 16)
-    leaf_unit<2, KAHAN, POT, false, true>(pos4, rg, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial, max_slots,
-                                          err);
-  else
-    leaf_unit_flat<KAHAN, POT>(pos4, rg, U, ax, runs, sW[warp].f, lane, G, eps2, out, partial, max_slots, err);
+  for (int row = 0; row < ntl; row += 32) {  // a leaf of more than 32 particles in two passes
+    const int2 rt = make_int2(rg.x + row, min(rg.y, rg.x + row + 31));
+    const int nt = rt.y - rt.x + 1;
+    if (row > 0) __syncwarp();  // the first pass's reads of the stage are done
+    if (nt <= 8)
+      leaf_unit<4, KAHAN, POT, false, true>(pos4, rt, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial,
+                                            max_slots, err, nullptr, nullptr, 1, rg, row);
+    else if (nt <= 16)
+      leaf_unit<2, KAHAN, POT, false, true>(pos4, rt, U, ax, runs, sW[warp].n, lane, G, eps2, out, partial,
+                                            max_slots, err, nullptr, nullptr, 1, rg, row);
+    else
+      leaf_unit_flat<KAHAN, POT>(pos4, rt, U, ax, runs, sW[warp].f, lane, G, eps2, out, partial, max_slots, err, rg,
+                                 row);
+  }
 }
 
 // Far field (L2P) of every leaf: warp per leaf (its unit with flags & 1),
@@ -1137,22 +1162,23 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
   const int node = num_internal + units[u].x;
   const int2 rg = ranges[node];
   if (rg.y - rg.x + 1 > kMaxLeaf) return;  // refused by the near-field kernel, which flags it
-  const bool act = rg.x + lane <= rg.y;
   if (zero) {  // near field alone: the sums start from zero
-    if (act) out[rg.x + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = rg.x + lane; i <= rg.y; i += 32) out[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     return;
   }
-  // the particle and the centre are fetched alongside the local's staging
+  // the first particle and the centre are fetched alongside the local's staging
   const float4 c = centers[node];
-  const float4 ti = act ? pos4[rg.x + lane] : c;
+  const float4 t0 = (rg.x + lane <= rg.y) ? pos4[rg.x + lane] : c;
   for (int k = lane; k < CS; k += 32) sF[warp][k] = locals[(size_t)node * CS + k];
   __syncwarp();
-  if (!act) return;
-  float U_[C];
-  solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
-  float phi, g[3];
-  l2p_eval<P>(SmemF{sF[warp]}, U_, &phi, g);
-  out[rg.x + lane] = make_float4(-G * g[0], -G * g[1], -G * g[2], -G * phi);
+  for (int i = rg.x + lane; i <= rg.y; i += 32) {  // two rounds for a leaf of more than 32
+    const float4 ti = (i == rg.x + lane) ? t0 : pos4[i];
+    float U_[C];
+    solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
+    float phi, g[3];
+    l2p_eval<P>(SmemF{sF[warp]}, U_, &phi, g);
+    out[i] = make_float4(-G * g[0], -G * g[1], -G * g[2], -G * phi);
+  }
 }
 
 // Sums the partial results of leaves whose work was split: split[i] = (leaf,
@@ -1163,7 +1189,7 @@ static __global__ void __launch_bounds__(256) k_leaf_reduce(int num_split, const
                                                      const int2* __restrict__ ranges, const float4* __restrict__ partial,
                                                      float4* __restrict__ out, int max_slots, int* err) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (int)(t >> 5), l = (int)(t & 31);
+  const int i = (int)(t / kMaxLeaf), l = (int)(t % kMaxLeaf);
   if (i >= num_split) return;
   const int4 sp = split[i];
   const int2 rg = ranges[num_internal + sp.x];
@@ -1370,7 +1396,7 @@ struct RunLeafEval {
       if (rc) return rc;
     }
     if (num_split > 0) {
-      k_leaf_reduce<true><<<blocks_for((int64_t)num_split * 32, 256), 256, 0, st>>>(
+      k_leaf_reduce<true><<<blocks_for((int64_t)num_split * kMaxLeaf, 256), 256, 0, st>>>(
           num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(ranges),
           reinterpret_cast<const float4*>(partial), reinterpret_cast<float4*>(out), max_slots, err);
       return launch_status();

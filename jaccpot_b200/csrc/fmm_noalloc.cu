@@ -20,7 +20,7 @@ JB_ORDERS_NA(JB_DECLARE_ORDER)
 
 namespace {
 
-// 32768 slots x 32 particles x float4 = 16 MiB per device.
+// 16384 slots x 64 particles x float4 = 16 MiB per device.
 static __device__ __align__(256) float4 g_leaf_scratch[(int64_t)JB_LEAF_EVAL_NOALLOC_MAX_SLOTS * jb::kMaxLeaf];
 
 jb::SymbolCache g_scratch_cache;

@@ -89,7 +89,7 @@ class DeviceTopology:
         nbad = int(bad.item())
         if nbad:
             raise _lib.JBError(f"{nbad} leaves hold more than {_lib.JB_MAX_LEAF_OCCUPANCY} particles "
-                               "(or none): the leaf kernels take leaf_size <= 32")
+                               f"(or none): the leaf kernels take leaf_size <= {_lib.JB_MAX_LEAF_OCCUPANCY}")
 
 
 @dataclass
@@ -167,8 +167,9 @@ class Pass:
                  leaf_unit_sources: int = 4096, gear_unit_pairs: int = 128):
         if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
             raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
-        if dt.topo.max_leaf_occupancy > 32:
-            raise ValueError("the leaf kernels take at most 32 particles per leaf (use leaf_size <= 32)")
+        if dt.topo.max_leaf_occupancy > _lib.JB_MAX_LEAF_OCCUPANCY:
+            raise ValueError(f"the leaf kernels take at most {_lib.JB_MAX_LEAF_OCCUPANCY} particles per leaf "
+                             f"(use leaf_size <= {_lib.JB_MAX_LEAF_OCCUPANCY})")
         self.dt = dt
         self.p = int(p)
         self.G = float(G)
@@ -217,7 +218,7 @@ class Pass:
         self.d_leaf_aux = up(self.leaf_sched.aux)
         self.d_leaf_runs = up(self.leaf_sched.runs)
         self.d_leaf_split = up(self.leaf_sched.split)
-        self.leaf_partials = torch.empty((max(self.leaf_sched.num_slots, 1) * 32, 4), device=dev, dtype=torch.float32)
+        self.leaf_partials = torch.empty((max(self.leaf_sched.num_slots, 1) * _lib.JB_MAX_LEAF_OCCUPANCY, 4), device=dev, dtype=torch.float32)
 
     def fork(self) -> "Pass":
         """A pass over the same topology and work-unit schedules (shared,
@@ -468,7 +469,7 @@ class Pass:
             self._adj["aux"] = up(self._adj_sched.aux)
             self._adj["runs"] = up(self._adj_sched.runs)
             self._adj["split"] = up(self._adj_sched.split)
-            self._adj["partials"] = torch.empty((max(self._adj_sched.num_slots, 1) * 32, 4), **f32)
+            self._adj["partials"] = torch.empty((max(self._adj_sched.num_slots, 1) * _lib.JB_MAX_LEAF_OCCUPANCY, 4), **f32)
         return self._adj
 
     def vjp(self, w: torch.Tensor, grad_pos: torch.Tensor, grad_mass: torch.Tensor, stream=None,

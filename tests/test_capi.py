@@ -57,7 +57,7 @@ def test_argument_errors_without_a_device():
 def test_leaf_checks_refuse_bad_arguments_without_a_device():
     lib = _lib.lib()
     # max_occupancy outside [1, JB_MAX_LEAF_OCCUPANCY], null arrays
-    assert lib.jb_validate_leaves(3, 1, 1, 33, 1, None) == 1
+    assert lib.jb_validate_leaves(3, 1, 1, 65, 1, None) == 1
     assert lib.jb_validate_leaves(3, 1, 1, 0, 1, None) == 1
     assert lib.jb_validate_leaves(3, 1, None, 32, 1, None) == 1
     assert lib.jb_leaf_eval_errors(None, 0, None) == 1

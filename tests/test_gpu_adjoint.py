@@ -21,7 +21,8 @@ from jaccpot_b200.autodiff import fmm_accelerations  # noqa: E402
 
 GRAD_P99 = 1e-4  # per-particle relative difference of the FP32 gradient vs the FP64 oracle
 
-CASES = [("uniform", 2048, 16, 0.5, 4), ("plummer", 4096, 16, 0.5, 6), ("clustered", 8192, 32, 0.6, 6)]
+CASES = [("uniform", 2048, 16, 0.5, 4), ("plummer", 4096, 16, 0.5, 6), ("clustered", 8192, 32, 0.6, 6),
+         ("plummer", 8192, 64, 0.6, 4)]
 
 
 def _ids(c):

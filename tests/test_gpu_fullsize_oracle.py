@@ -35,11 +35,13 @@ def _threads():
     oracle.set_threads(os.cpu_count() or 1)
 
 
-def test_plummer_1m_p6_every_acceleration_and_the_target_subset():
+@pytest.mark.parametrize("leaf", [32, 64])
+def test_plummer_1m_p6_every_acceleration_and_the_target_subset(leaf):
+    """leaf 64: the reference's large_n_gpu leaf target (jaccpot/solver.py:53)."""
     n = 1048576
     pos, mass = workloads.plummer(n, 0)
     fmm = FastMultipoleMethod(preset="large_n_gpu", theta=0.6, G=1.0, softening=0.0)
-    st = fmm.prepare_state(pos, mass, leaf_size=32, max_order=6)
+    st = fmm.prepare_state(pos, mass, leaf_size=leaf, max_order=6)
     got = fmm.evaluate_prepared_state(st)
     topo = st.topology
     perm = topo.permutation

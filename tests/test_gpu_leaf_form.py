@@ -23,7 +23,8 @@ from jaccpot_b200 import _lib, engine, tree, workloads  # noqa: E402
 
 CASES = [("clustered", 262_144, 32, 0.55, 4096), ("plummer", 131_072, 32, 0.6, 96),
          ("uniform", 65_536, 24, 0.5, 4096), ("clustered", 50_000, 20, 0.7, 40),
-         ("uniform", 3_000, 32, 0.6, 33)]
+         ("uniform", 3_000, 32, 0.6, 33), ("plummer", 131_072, 64, 0.6, 256),
+         ("clustered", 65_536, 48, 0.55, 100)]
 
 
 def _pass(kind, n, leaf, theta, unit_sources, p2p_mode, leaf_range=None):
@@ -34,6 +35,8 @@ def _pass(kind, n, leaf, theta, unit_sources, p2p_mode, leaf_range=None):
     ps = engine.Pass(dt, 4, G=1.0, eps2=1e-7, p2p_mode=p2p_mode, leaf_unit_sources=unit_sources,
                      leaf_range=leaf_range)
     ps.load_particles(torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda())
+    ps.upward()
+    ps.downward()  # the locals the far field reads
     return ps, topo
 
 

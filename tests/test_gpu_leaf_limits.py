@@ -1,5 +1,5 @@
 """Leaf-occupancy and slot preconditions of the leaf kernels, through the C
-ABI: leaves of more than JB_MAX_LEAF_OCCUPANCY (32) particles get a status,
+ABI: leaves of more than JB_MAX_LEAF_OCCUPANCY (64) particles get a status,
 not a write -- the GPU leaf schedule refuses them, jb_validate_leaves counts
 them, and a hand-made unit that names one writes nothing and sets the leaf
 error word; a partial-row slot beyond jb_leaf_eval_noalloc's num_slots is
@@ -31,9 +31,9 @@ def _errors(clear=True):
 
 def _topology_with_big_leaves():
     pos, mass = workloads.uniform_cube(20000, seed=5)
-    topo = tree.build_topology(pos, mass, leaf_size=48, theta=0.6)
+    topo = tree.build_topology(pos, mass, leaf_size=96, theta=0.6)
     occ = topo.node_ranges[topo.num_internal:, 1] - topo.node_ranges[topo.num_internal:, 0] + 1
-    assert occ.max() > 32
+    assert occ.max() > 64
     return pos, mass, topo, occ
 
 
@@ -43,9 +43,9 @@ def test_over_full_leaves_get_a_status_not_a_write():
     st = torch.cuda.current_stream().cuda_stream
     ranges = torch.from_numpy(topo.node_ranges.reshape(-1).astype(np.int32)).cuda()
     bad = torch.zeros(1, dtype=torch.int32, device="cuda")
-    _lib.check(lb.jb_validate_leaves(topo.num_nodes, topo.num_internal, ranges.data_ptr(), 32, bad.data_ptr(), st),
+    _lib.check(lb.jb_validate_leaves(topo.num_nodes, topo.num_internal, ranges.data_ptr(), 64, bad.data_ptr(), st),
                "jb_validate_leaves")
-    assert int(bad.item()) == int((occ > 32).sum())
+    assert int(bad.item()) == int((occ > 64).sum())
     # the engine refuses the topology up front
     with pytest.raises(ValueError):
         engine.Pass(engine.DeviceTopology(topo, "cuda"), 4)
@@ -72,7 +72,7 @@ def test_over_full_leaves_get_a_status_not_a_write():
     aux = torch.tensor([[-1, 1]], dtype=torch.int32, device="cuda")
     runs = torch.zeros((1, 2), dtype=torch.int32, device="cuda")
     out = torch.full((n, 4), 7.0, device="cuda")
-    partials = torch.zeros((32, 4), device="cuda")
+    partials = torch.zeros((64, 4), device="cuda")
     _errors()
     _lib.check(lb.jb_leaf_eval(4, 0, pos4.data_ptr(), topo.num_internal, 1, units.data_ptr(), aux.data_ptr(),
                                runs.data_ptr(), ranges.data_ptr(), centers.data_ptr(), locs.data_ptr(), 1.0, 0.0,

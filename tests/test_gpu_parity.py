@@ -33,6 +33,9 @@ CASES = [
     ("uniform", 16384, 16, 0.6, 8),
     ("plummer", 20000, 32, 0.6, 6),
     ("clustered", 32768, 32, 0.5, 8),
+    # leaves of 33..64 particles: evaluated in two passes of at most 32 targets
+    ("plummer", 40000, 64, 0.6, 6),
+    ("clustered", 32768, 48, 0.55, 8),
 ]
 
 
