@@ -9,7 +9,11 @@ numbers: as easy as 1, 2, 3", SC'11), keyed and counted the way JAX's
 two uint32 words; ``split(key, n)`` and ``random_bits(key, shape)`` hash the
 (hi, lo) words of the flat element index; 64-bit draws concatenate the two
 output words; floats take the top mantissa bits (``uniform``), ``normal`` is
-sqrt(2) * erfinv(u) with u uniform on (nextafter(-1, 0), 1).
+sqrt(2) * erfinv(u) with u uniform on (nextafter(-1, 0), 1).  ``randint``
+(int64, the default integer type with 64-bit mode on) draws two 64-bit words
+from the two halves of ``split(key)`` and folds them modulo the span, the
+higher word weighted by 2**64 mod span (JAX's documented construction that
+keeps the modulo bias at 2**-64 for any span).
 """
 
 from __future__ import annotations
@@ -83,13 +87,38 @@ def normal(k, shape):
     return np.sqrt(2.0) * erfinv(u)
 
 
+def randint(k, shape, minval: int, maxval: int):
+    """int64 integers on [minval, maxval) (jax.random.randint, 64-bit mode)."""
+    k1, k2 = split(k, 2)
+    higher = random_bits(k1, shape, 64)
+    lower = random_bits(k2, shape, 64)
+    span = int(maxval) - int(minval)
+    if span <= 0:
+        raise ValueError("empty range")
+    mult = (pow(2, 32, span) ** 2) % span  # 2**64 mod span, squared in halves
+    hi = np.array([int(h) % span for h in higher.ravel()], dtype=object)
+    lo = np.array([int(v) % span for v in lower.ravel()], dtype=object)
+    off = (hi * mult + lo) % span
+    return (int(minval) + off.astype(np.int64)).reshape(shape)
+
+
 def golden_inputs(distribution: str, n: int):
-    """Positions and masses of the reference's golden cases (uniform only:
-    the clustered case also needs jax.random.randint)."""
+    """Positions and masses of the reference's golden cases, drawn from
+    PRNGKey(0xC0FFEE) the way tests/characterization/test_fmm_golden.py:171-193
+    draws them ("uniform": uniform in [-1, 1)^3; "clustered": four Gaussian
+    blobs of width 0.08 around centres uniform in [-0.8, 0.8)^3, clipped to
+    [-1, 1])."""
     k = key(0xC0FFEE)
-    k_pos, k_mass, _k_blob = split(k, 3)
-    if distribution != "uniform":
-        raise ValueError("only the uniform goldens are regenerated")
-    pos = uniform(k_pos, (n, 3), -1.0, 1.0)
+    k_pos, k_mass, k_blob = split(k, 3)
+    if distribution == "uniform":
+        pos = uniform(k_pos, (n, 3), -1.0, 1.0)
+    elif distribution == "clustered":
+        n_blobs = 4
+        centers = uniform(k_blob, (n_blobs, 3), -0.8, 0.8)
+        assign = randint(k_pos, (n,), 0, n_blobs)
+        jitter = 0.08 * normal(k_mass, (n, 3))
+        pos = np.clip(centers[assign] + jitter, -1.0, 1.0)
+    else:
+        raise ValueError(f"unknown distribution {distribution!r}")
     mass = np.abs(normal(k_mass, (n,))) + 0.5
     return pos, mass

@@ -2,6 +2,7 @@
 
 The reference (jaccpot) commits outputs of its public API for seeded inputs:
   tests/characterization/golden/uni_real_n{256,1024}_p{2,4,6}.npz   accel (N,3) f64
+  tests/characterization/golden/clu_real_n256_p4.npz                accel (N,3) f64 (clustered)
   tests/characterization/golden_modes/bkt_uni_real_n256_p4.npz      accel, potential
   tests/characterization/golden_grad/uni_real_n{128,256}_p{2,4}.npz grad_positions, grad_masses
 They were produced with preset="accurate", theta 0.5, softening 1e-2, G 1
@@ -10,7 +11,7 @@ from jax.random.PRNGKey(0xC0FFEE), which tests/golden/jax_prng.py regenerates.
 
 Usage: python tests/golden/make_fixtures.py REFERENCE_ROOT
 (REFERENCE_ROOT: the jaccpot checkout holding tests/characterization/.)
-Writes tests/golden/reference_goldens.npz (uniform real-basis cases only).
+Writes tests/golden/reference_goldens.npz (real-basis cases only).
 """
 
 from __future__ import annotations
@@ -20,7 +21,8 @@ from pathlib import Path
 
 import numpy as np
 
-FORWARD = ["uni_real_n256_p2", "uni_real_n256_p4", "uni_real_n256_p6", "uni_real_n1024_p4"]
+FORWARD = ["uni_real_n256_p2", "uni_real_n256_p4", "uni_real_n256_p6", "uni_real_n1024_p4",
+           "clu_real_n256_p4"]
 MODES = ["bkt_uni_real_n256_p4"]
 GRAD = ["uni_real_n128_p2", "uni_real_n128_p4", "uni_real_n256_p4"]
 
