@@ -189,7 +189,8 @@ typedef struct {
 } jb_sched_info_t;
 enum {
   JB_SCHED_UNITS = 0,          /* int32[num_units][4] */
-  JB_SCHED_AUX = 1,            /* int32[num_units][2] (leaf schedule) */
+  JB_SCHED_AUX = 1,            /* int32[num_units][2] (leaf schedule); int32[num_units][4]
+                                  segment bounds (mixed gear schedule) */
   JB_SCHED_RUNS = 2,           /* int32[num_runs][2] (leaf schedule) */
   JB_SCHED_SPLIT = 3,          /* int32[num_split][4] */
   JB_SCHED_FAR_SOURCES = 4,    /* int32[num_far] regrouped by gear (gear schedule) */
@@ -207,6 +208,16 @@ JB_API int jb_leaf_schedule_device(int num_internal, int num_leaves, const int* 
 /* gears: int32 per far pair in [0, num_gears) (JB_ERR_INDEX otherwise). */
 JB_API int jb_gear_schedule_device(int num_nodes, const int64_t* far_off, const int* far_src, const int* gears,
                                    int num_gears, int max_pairs, void* stream, jb_dsched** out);
+/* The schedule of jb_m2l_mixed: each target's pairs sorted by order, highest
+ * first (stable inside), cut into units of at most max_pairs (<= 65535);
+ * slots numbered per target; units sorted by decreasing segment lengths,
+ * highest order first.  gear_orders (HOST, num_gears entries) must each be
+ * one of p_max - 2j, j < JB_MIXED_GEAR_SEGMENTS, >= 1 (JB_ERR_ARG
+ * otherwise); a gear outside [0, num_gears) gives JB_ERR_INDEX.  Fields:
+ * UNITS, AUX (bounds), SPLIT, FAR_SOURCES, PAIRS_PER_GEAR.                  */
+JB_API int jb_gear_mixed_schedule_device(int num_nodes, const int64_t* far_off, const int* far_src, const int* gears,
+                                         int num_gears, const int* gear_orders, int p_max, int max_pairs,
+                                         void* stream, jb_dsched** out);
 /* rev[e] = index of the reverse pair (s <- t) of every far pair e = (t <- s)
  * of a symmetric CSR far list (device arrays; rows sorted, as jb_tree_build
  * emits them); JB_ERR_INDEX when some pair has no reverse.  The host twin is
@@ -292,6 +303,14 @@ JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float*
                   const int* far_src, float* locals, float* partials, int num_split, const int* split,
                   void* stream);
 
+/* jb_m2l with far pair e's contribution scaled by far_w[e] (device float per
+ * CSR far entry): the block-step weighted far field of the mutual lane
+ * (jaccpot/mutual/force.py:920 _far_pair_weights there: a pair's weight is
+ * that of its finer node's level, the same for both directions). FP32.    */
+JB_API int jb_m2l_weighted(int p, int num_units, const int* units, const float* mult, const float* centers,
+                           const int* far_src, const float* far_w, float* locals, float* partials, int num_split,
+                           const int* split, void* stream);
+
 /* Far field with a per-pair expansion order (gear): the reference's
  * adaptive-order downward sweep, which buckets far pairs by gear and runs
  * each bucket's M2L at that gear's order (runtime/fmm_prepare.py:2400-2480,
@@ -301,16 +320,22 @@ JB_API int jb_m2l(int p, int mode, int num_units, const int* units, const float*
  * far_src is the source list regrouped so no unit mixes gears.  Rows of
  * mult / locals / partials have stride jb_coeff_stride(p_max); a gear reads
  * the degrees <= its order and writes zeros above them. */
-/* jb_m2l with far pair e's contribution scaled by far_w[e] (device float per
- * CSR far entry): the block-step weighted far field of the mutual lane
- * (jaccpot/mutual/force.py:920 _far_pair_weights there: a pair's weight is
- * that of its finer node's level, the same for both directions). FP32.    */
-JB_API int jb_m2l_weighted(int p, int num_units, const int* units, const float* mult, const float* centers,
-                           const int* far_src, const float* far_w, float* locals, float* partials, int num_split,
-                           const int* split, void* stream);
 JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orders, const int64_t* gear_unit_offsets,
                         const int* units, const float* mult, const float* centers, const int* far_src,
                         float* locals, float* partials, int num_split, const int* split, void* stream);
+
+/* The same far field in one launch, for gears whose orders lie on the ladder
+ * p_max, p_max-2, p_max-4, p_max-6 (those >= 1; JB_MIXED_GEAR_SEGMENTS at
+ * most): a unit (target, first, end, slot) is a slice of one target's list
+ * with its pairs sorted by order, highest first, and bounds[u] = (b1, b2, b3,
+ * end) cuts it into segments [b_j, b_j+1) (b_0 = first) evaluated at order
+ * p_max - 2j, all into one accumulator, so a target split over gears needs
+ * no partial rows.  units / bounds / far_src / split come from
+ * jb_gear_mixed_schedule_device (device arrays).  FP32.                     */
+#define JB_MIXED_GEAR_SEGMENTS 4
+JB_API int jb_m2l_mixed(int p_max, int num_units, const int* units, const int* bounds, const float* mult,
+                        const float* centers, const int* far_src, float* locals, float* partials, int num_split,
+                        const int* split, void* stream);
 
 /* Split-BF16 far field on the tensor cores (tcgen05.mma kind::f16, FP32
  * accumulation in TMEM): the M2L chain Dz(az) B Dz(-ax) r^-k K r^-(n+1) Dz(ax)

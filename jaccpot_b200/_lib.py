@@ -29,6 +29,7 @@ JB_M2L_FP32, JB_M2L_SPLIT_BF16 = 0, 1
 JB_P2P_FP32, JB_P2P_KAHAN, JB_P2P_POTENTIAL, JB_P2P_FAR_ONLY, JB_P2P_NEAR_ONLY = 0, 1, 2, 4, 8
 JB_LEAF_EVAL_NOALLOC_MAX_SLOTS = 16384
 JB_MAX_LEAF_OCCUPANCY = 64
+JB_MIXED_GEAR_SEGMENTS = 4
 JB_LEAF_ERR_OCCUPANCY, JB_LEAF_ERR_SLOT = 1, 2
 (JB_SCHED_UNITS, JB_SCHED_AUX, JB_SCHED_RUNS, JB_SCHED_SPLIT, JB_SCHED_FAR_SOURCES, JB_SCHED_GEAR_OFFSETS,
  JB_SCHED_TARGETS, JB_SCHED_PAIRS_PER_GEAR) = range(8)
@@ -100,6 +101,7 @@ _SIGNATURES = {
     "jb_m2l_schedule_device": [_I, _P, _I, _I, _P, _P, ctypes.POINTER(_P)],
     "jb_leaf_schedule_device": [_I, _I, _P, _P, _P, _I, _I, _I, _P, ctypes.POINTER(_P)],
     "jb_gear_schedule_device": [_I, _P, _P, _P, _I, _I, _P, ctypes.POINTER(_P)],
+    "jb_gear_mixed_schedule_device": [_I, _P, _P, _P, _I, _P, _I, _I, _P, ctypes.POINTER(_P)],
     "jb_dsched_info": [_P, _P],
     "jb_dsched_field": [_P, _I],
     "jb_dsched_free": [_P],
@@ -113,6 +115,7 @@ _SIGNATURES = {
     "jb_m2m_level": [_I, _I, _I, _P, _P, _P, _P, _P, _P],
     "jb_m2l": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_m2l_gears": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
+    "jb_m2l_mixed": [_I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_m2l_split": [_I, _I, _I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P],
     "jb_m2l_split_units": [_I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P],
     "jb_l2l_level": [_I, _I, _I, _P, _P, _P, _P, _P],

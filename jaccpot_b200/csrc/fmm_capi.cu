@@ -607,6 +607,17 @@ JB_API int jb_m2l_gears(int p_max, int mode, int num_gears, const int* gear_orde
   return JB_OK;
 }
 
+JB_API int jb_m2l_mixed(int p_max, int num_units, const int* units, const int* bounds, const float* mult,
+                        const float* centers, const int* far_src, float* locals, float* partials, int num_split,
+                        const int* split, void* stream) {
+  if (p_max < 1 || p_max > JB_MAX_ORDER) return JB_ERR_ORDER;
+  if (num_units < 0 || num_split < 0 || (num_split > 0 && (!split || !partials)))
+    return JB_ERR_ARG;
+  if (num_units > 0 && (!units || !bounds || !mult || !centers || !far_src || !locals)) return JB_ERR_ARG;
+  return dispatch<RunM2LMixed>(p_max, num_units, units, bounds, mult, centers, far_src, locals, partials, num_split,
+                               split, ST(stream));
+}
+
 JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* right, const float* centers,
                         float* locals, void* stream) {
   if (first < 0 || last < first || (last > first && (!left || !right || !centers || !locals))) return JB_ERR_ARG;

@@ -308,6 +308,101 @@ static __global__ void __launch_bounds__(256) k_m2l_reduce(int num_split, const 
 }
 
 // ---------------------------------------------------------------------------
+// M2L with per-pair orders (gears) in one launch.  The orders form the ladder
+// P, P-2, P-4, P-6 (those >= 1; kMixedSegs(P) of them).  A unit is a slice of
+// one target's far list whose pairs are sorted by order, highest first, so it
+// holds up to four segments: units[u] = (target, first pair, end pair, slot)
+// and bounds[u] = (b1, b2, b3, end): segment j = [b_j, b_{j+1}) with b_0 =
+// first pair, evaluated at order P - 2j into the same registers (a lower
+// order adds only to the degrees it has).  Thread per unit; every lane of a
+// warp finishes segment j (__syncwarp) before any starts segment j+1, so
+// lanes only diverge inside a segment.  Units are sorted by their segment
+// lengths (highest order first), so the lanes of a warp have similar ones.
+// Slots and the split reduce are k_m2l_units'.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int kMixedSegs(int P) { return (P + 1) / 2 < 4 ? (P + 1) / 2 : 4; }
+
+template <int P>
+__device__ __forceinline__ void m2l_segment(int e0, int e1, const float* __restrict__ mult,
+                                            const float4* __restrict__ centers, const int* __restrict__ far_src,
+                                            int rs, float4 ct, float4* row, float* acc) {
+  constexpr int C = csize(P), CS = cstride(P);
+  if (e1 <= e0) return;
+  const int s0 = far_src[e0];
+  int s1 = (e0 + 1 < e1) ? far_src[e0 + 1] : s0;
+  {
+    const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s0 * rs);
+#pragma unroll
+    for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
+    cp_async_commit();
+  }
+  float4 cs = centers[s0];
+  float4 cs1 = centers[s1];
+  for (int e = e0; e < e1; ++e) {
+    float v[C];
+    cp_async_wait_all();
+#pragma unroll
+    for (int k = 0; k < CS / 4; ++k) {
+      const float4 q = row[k];
+      if (4 * k + 0 < C) v[4 * k + 0] = q.x;
+      if (4 * k + 1 < C) v[4 * k + 1] = q.y;
+      if (4 * k + 2 < C) v[4 * k + 2] = q.z;
+      if (4 * k + 3 < C) v[4 * k + 3] = q.w;
+    }
+    if (e + 1 < e1) {
+      const float4* src = reinterpret_cast<const float4*>(mult + (size_t)s1 * rs);
+#pragma unroll
+      for (int k = 0; k < CS / 4; ++k) cp_async16(row + k, src + k);
+      cp_async_commit();
+    }
+    const int s2 = (e + 2 < e1) ? __ldg(far_src + e + 2) : s1;
+    m2l_kfold_acc<P, false>(v, acc, ct.x - cs.x, ct.y - cs.y, ct.z - cs.z, 1.f);
+    cs = cs1;
+    cs1 = centers[s2];
+    s1 = s2;
+  }
+}
+
+template <int P, int J = 0>
+__device__ __forceinline__ void m2l_segments(const int* b, const float* __restrict__ mult,
+                                             const float4* __restrict__ centers, const int* __restrict__ far_src,
+                                             int rs, float4 ct, float4* row, float* acc) {
+  if constexpr (J < kMixedSegs(P)) {
+    m2l_segment<P - 2 * J>(b[J], b[J + 1], mult, centers, far_src, rs, ct, row, acc);
+    __syncwarp();
+    m2l_segments<P, J + 1>(b, mult, centers, far_src, rs, ct, row, acc);
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_mixed(int num_units, const int4* __restrict__ units,
+                                                              const int4* __restrict__ bounds,
+                                                              const float* __restrict__ mult,
+                                                              const float4* __restrict__ centers,
+                                                              const int* __restrict__ far_src,
+                                                              float* __restrict__ locals,
+                                                              float* __restrict__ partials, int rs) {
+  constexpr int C = csize(P);
+  extern __shared__ float4 m2l_smem[];
+  float4* row = m2l_smem + threadIdx.x * row4(P);
+  const int u = blockIdx.x * kM2LThreads + threadIdx.x;
+  const bool ok = u < num_units;  // lanes past the end run empty segments to the warp barriers
+  const int4 U = ok ? units[u] : make_int4(0, 0, 0, -1);
+  const int4 B = ok ? bounds[u] : make_int4(0, 0, 0, 0);
+  const int b[5] = {U.y, B.x, B.y, B.z, B.w};
+  float acc[C];
+#pragma unroll
+  for (int k = 0; k < C; ++k) acc[k] = 0.f;
+  const float4 ct = ok ? centers[U.x] : make_float4(0.f, 0.f, 0.f, 0.f);
+  m2l_segments<P>(b, mult, centers, far_src, rs, ct, row, acc);
+  if (!ok) return;
+  float* dst = (U.w < 0) ? locals + (size_t)U.x * rs : partials + (size_t)U.w * rs;
+#pragma unroll
+  for (int k = 0; k < C; ++k) dst[k] = acc[k];
+  for (int k = C; k < rs; ++k) dst[k] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
 // M2M / L2L, one level, degrees split over four warps.
 //
 // A translation's rotations and B products act on each degree separately;
@@ -1328,6 +1423,29 @@ struct RunM2L {
 };
 
 template <int P>
+struct RunM2LMixed {
+  static int run(int num_units, const int* units, const int* bounds, const float* mult, const float* centers,
+                 const int* far_src, float* locals, float* partials, int num_split, const int* split, cudaStream_t st) {
+    const int rs = cstride(P);
+    if (num_units > 0) {
+      const size_t sm = sizeof(float4) * kM2LThreads * row4(P);
+      cudaFuncSetAttribute(k_m2l_mixed<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_m2l_mixed<P><<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
+          num_units, reinterpret_cast<const int4*>(units), reinterpret_cast<const int4*>(bounds), mult,
+          reinterpret_cast<const float4*>(centers), far_src, locals, partials, rs);
+      const int rc = launch_status();
+      if (rc) return rc;
+    }
+    if (num_split > 0) {
+      k_m2l_reduce<<<blocks_for((int64_t)num_split * rs, 256), 256, 0, st>>>(
+          num_split, reinterpret_cast<const int4*>(split), partials, locals, rs);
+      return launch_status();
+    }
+    return JB_OK;
+  }
+};
+
+template <int P>
 struct RunL2L {
   static int run(int first, int last, const int* left, const int* right, const float* centers, float* locals,
                  cudaStream_t st) {
@@ -1426,6 +1544,7 @@ struct RunTargets {
   extern template struct jb::RunP2M<PP>;      \
   extern template struct jb::RunM2M<PP>;      \
   extern template struct jb::RunM2L<PP>;      \
+  extern template struct jb::RunM2LMixed<PP>; \
   extern template struct jb::RunL2L<PP>;      \
   extern template struct jb::RunLeafEval<PP>; \
   extern template struct jb::RunTargets<PP>;  \

@@ -8,6 +8,7 @@
 template struct jb::RunP2M<JB_ORDER>;
 template struct jb::RunM2M<JB_ORDER>;
 template struct jb::RunM2L<JB_ORDER>;
+template struct jb::RunM2LMixed<JB_ORDER>;
 template struct jb::RunL2L<JB_ORDER>;
 template struct jb::RunLeafEval<JB_ORDER>;
 template struct jb::RunTargets<JB_ORDER>;

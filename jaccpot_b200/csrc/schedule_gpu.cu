@@ -16,6 +16,10 @@
 // * Gears: each target's far pairs regrouped by gear (stable), cut per
 //   (target, gear) into units of at most max_pairs; slots numbered per target;
 //   units ordered by gear, then decreasing length (stable).
+// * Mixed gears (gear_m2l_mixed_schedule): each target's far pairs sorted by
+//   order, highest first (stable), the list cut into units of at most
+//   max_pairs with their segment bounds; slots numbered per target; units
+//   ordered by decreasing segment lengths, highest order first (stable).
 // Stable orders come from the LSD radix sort (keys with the index order as
 // the tie-break), prefix sums from the tile scan of dev_prims.cuh; integer
 // work only, and the only atomics are order-independent counts and maxima.
@@ -698,6 +702,171 @@ void build_gears(jb_dsched& d, int num_nodes, const int64_t* far_off, const int*
 }
 
 // ---------------------------------------------------------------------------
+// Mixed gear schedule (jb_m2l_mixed): each target's pairs sorted by segment
+// (order, highest first; stable inside), the whole list cut into units of at
+// most max_pairs, each unit's segment bounds read off the sorted keys.
+// ---------------------------------------------------------------------------
+constexpr int kMixedSegMax = JB_MIXED_GEAR_SEGMENTS;
+
+struct GearSegments {
+  int seg[64];  // segment of each gear index
+};
+
+__global__ void __launch_bounds__(256) k_mixed_keys(const int* __restrict__ row, const int* __restrict__ gears,
+                                                    int64_t P, int num_gears, GearSegments gs,
+                                                    uint64_t* __restrict__ key, unsigned long long* __restrict__ ppg,
+                                                    int* __restrict__ bad) {
+  __shared__ unsigned int hist[64];
+  if (threadIdx.x < 64) hist[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < P) {
+    int g = gears[e];
+    if (g < 0 || g >= num_gears) {
+      atomicAdd(bad, 1);
+      g = 0;
+    }
+    key[e] = ((uint64_t)row[e] << 2) | (uint64_t)gs.seg[g];
+    atomicAdd(&hist[g], 1u);
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < num_gears && hist[threadIdx.x]) atomicAdd(&ppg[threadIdx.x], (unsigned long long)hist[threadIdx.x]);
+}
+
+__global__ void k_mixed_nu(const int64_t* __restrict__ off, int nodes, int max_pairs, int* __restrict__ nu,
+                           int* __restrict__ mnp, int* __restrict__ sflag) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nodes) return;
+  const int u = (int)((off[t + 1] - off[t] + max_pairs - 1) / max_pairs);
+  nu[t] = u;
+  mnp[t] = u > 1 ? u : 0;
+  sflag[t] = u > 1 ? 1 : 0;
+}
+
+// Thread per target: the segment starts by binary search in its sorted keys
+// (the low two bits, non-decreasing inside a row), then its units.
+__global__ void k_mixed_emit(const int64_t* __restrict__ off, int nodes, const uint64_t* __restrict__ key,
+                             int max_pairs, int nb, const int* __restrict__ nu, const int* __restrict__ unit_off,
+                             const int* __restrict__ slot_base, int4* __restrict__ units, int4* __restrict__ bounds,
+                             uint64_t* __restrict__ ukey) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nodes) return;
+  const int a = (int)off[t], b = (int)off[t + 1];
+  if (a == b) return;
+  int sb[kMixedSegMax + 1];
+  sb[0] = a;
+  sb[kMixedSegMax] = b;
+  for (int j = 1; j < kMixedSegMax; ++j) {
+    int lo = a, hi = b;
+    while (lo < hi) {
+      const int mid = lo + (hi - lo) / 2;
+      if ((int)(key[mid] & 3u) < j) lo = mid + 1;
+      else hi = mid;
+    }
+    sb[j] = lo;
+  }
+  const int n = nu[t];
+  for (int q = 0; q < n; ++q) {
+    const int u = unit_off[t] + q;
+    const int s = a + q * max_pairs, e = min(s + max_pairs, b);
+    int bd[kMixedSegMax + 1];
+    bd[0] = s;
+    bd[kMixedSegMax] = e;
+    for (int j = 1; j < kMixedSegMax; ++j) bd[j] = min(max(sb[j], s), e);
+    units[u] = make_int4(t, s, e, n > 1 ? slot_base[t] + q : -1);
+    bounds[u] = make_int4(bd[1], bd[2], bd[3], e);
+    uint64_t k = 0;
+    for (int j = 0; j < kMixedSegMax; ++j) k = (k << nb) | (uint64_t)(max_pairs - (bd[j + 1] - bd[j]));
+    ukey[u] = k;
+  }
+}
+
+void build_gears_mixed(jb_dsched& d, int num_nodes, const int64_t* far_off, const int* far_src, const int* gears,
+                       int num_gears, const GearSegments& gs, int max_pairs, cudaStream_t st) {
+  Scratch s;
+  ck(s.total.alloc(64));
+  int* d_tot = tot32(s);
+  int64_t P = 0;
+  ck(cudaMemcpyAsync(&P, far_off + num_nodes, 8, cudaMemcpyDeviceToHost, st));
+  ck(cudaStreamSynchronize(st));
+  if (P > (int64_t)0x7fffffff - max_pairs) throw Fail{JB_ERR_ARG};  // unit bounds are int32
+  ck(d.pairs_per_gear.alloc((size_t)num_gears * 8));
+  ck(cudaMemsetAsync(d.pairs_per_gear.p, 0, (size_t)num_gears * 8, st));
+  ck(d.far_src.alloc((size_t)std::max<int64_t>(P, 1) * 4));
+  if (P == 0) {
+    ck(d.units.alloc(16));
+    ck(d.aux.alloc(16));
+    ck(d.split.alloc(16));
+    ck(cudaStreamSynchronize(st));
+    return;
+  }
+  DBuf row, k0, k1, v0, v1;
+  ck(row.alloc((size_t)P * 4));
+  k_expand_rows<<<nblocks(num_nodes, 128), 128, 0, st>>>(far_off, 0, num_nodes, 0, row.as<int>());
+  ck_launch();
+  ck(k0.alloc((size_t)P * 8));
+  ck(k1.alloc((size_t)P * 8));
+  ck(v0.alloc((size_t)P * 4));
+  ck(v1.alloc((size_t)P * 4));
+  ck(cudaMemsetAsync(d_tot + 3, 0, 4, st));
+  k_mixed_keys<<<nblocks(P, 256), 256, 0, st>>>(row.as<int>(), gears, P, num_gears, gs, k0.as<uint64_t>(),
+                                                d.pairs_per_gear.as<unsigned long long>(), d_tot + 3);
+  ck_launch();
+  if (read_word(d_tot + 3, st) != 0) throw Fail{JB_ERR_INDEX};
+  k_iota<<<nblocks(P, 256), 256, 0, st>>>(v0.as<int>(), P);
+  ck_launch();
+  radix_sort(k0.as<uint64_t>(), v0.as<int>(), k1.as<uint64_t>(), v1.as<int>(), P, bits_for(num_nodes) + 2, s, st);
+  k_gather_rows<int><<<nblocks(P, 256), 256, 0, st>>>(far_src, v0.as<int>(), P, d.far_src.as<int>());
+  ck_launch();
+  row.release();
+  k1.release();
+  v1.release();
+  v0.release();
+  DBuf nu, mnp, sflag, unit_off, slot_base, spos;
+  for (DBuf* b : {&nu, &mnp, &sflag, &unit_off, &slot_base, &spos}) ck(b->alloc((size_t)std::max(num_nodes, 1) * 4));
+  k_mixed_nu<<<nblocks(num_nodes, 256), 256, 0, st>>>(far_off, num_nodes, max_pairs, nu.as<int>(), mnp.as<int>(),
+                                                     sflag.as<int>());
+  ck_launch();
+  exclusive_scan<int>(nu.as<int>(), unit_off.as<int>(), num_nodes, d_tot, s, st);
+  exclusive_scan<int>(mnp.as<int>(), slot_base.as<int>(), num_nodes, d_tot + 1, s, st);
+  exclusive_scan<int>(sflag.as<int>(), spos.as<int>(), num_nodes, d_tot + 2, s, st);
+  int tot[3];
+  ck(cudaMemcpyAsync(tot, d_tot, sizeof(tot), cudaMemcpyDeviceToHost, st));
+  ck(cudaStreamSynchronize(st));
+  const int U = tot[0], S = tot[2];
+  d.info.num_units = U;
+  d.info.num_slots = tot[1];
+  d.info.num_split = S;
+  const int nb = bits_for(max_pairs + 1);
+  DBuf raw_u, raw_b, uk0, uk1, idx0, idx1;
+  ck(raw_u.alloc((size_t)U * 16));
+  ck(raw_b.alloc((size_t)U * 16));
+  ck(uk0.alloc((size_t)U * 8));
+  ck(uk1.alloc((size_t)U * 8));
+  ck(idx0.alloc((size_t)U * 4));
+  ck(idx1.alloc((size_t)U * 4));
+  k_mixed_emit<<<nblocks(num_nodes, 128), 128, 0, st>>>(far_off, num_nodes, k0.as<uint64_t>(), max_pairs, nb,
+                                                       nu.as<int>(), unit_off.as<int>(), slot_base.as<int>(),
+                                                       raw_u.as<int4>(), raw_b.as<int4>(), uk0.as<uint64_t>());
+  ck_launch();
+  k0.release();
+  k_iota<<<nblocks(U, 256), 256, 0, st>>>(idx0.as<int>(), U);
+  ck_launch();
+  radix_sort(uk0.as<uint64_t>(), idx0.as<int>(), uk1.as<uint64_t>(), idx1.as<int>(), U, kMixedSegMax * nb, s, st);
+  ck(d.units.alloc((size_t)U * 16));
+  ck(d.aux.alloc((size_t)U * 16));
+  k_gather_rows<int4><<<nblocks(U, 256), 256, 0, st>>>(raw_u.as<int4>(), idx0.as<int>(), U, d.units.as<int4>());
+  ck_launch();
+  k_gather_rows<int4><<<nblocks(U, 256), 256, 0, st>>>(raw_b.as<int4>(), idx0.as<int>(), U, d.aux.as<int4>());
+  ck_launch();
+  ck(d.split.alloc((size_t)std::max(S, 1) * 16));
+  k_node_split<<<nblocks(num_nodes, 256), 256, 0, st>>>(num_nodes, nu.as<int>(), spos.as<int>(), slot_base.as<int>(),
+                                                        d.split.as<int4>());
+  ck_launch();
+  ck(cudaStreamSynchronize(st));
+}
+
+// ---------------------------------------------------------------------------
 // Reverse index of a symmetric far list: rev[e] for the pair e = (t <- s) is
 // the entry (s <- t), found by binary search in row s (rows are sorted).
 // Thread per row; a missing reverse is counted in *bad.
@@ -789,6 +958,25 @@ JB_API int jb_gear_schedule_device(int num_nodes, const int64_t* far_off, const 
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   return run_builder(out, st, [&](jb_dsched& d) {
     build_gears(d, num_nodes, far_off, far_src, gears, num_gears, max_pairs, st);
+  });
+}
+
+JB_API int jb_gear_mixed_schedule_device(int num_nodes, const int64_t* far_off, const int* far_src, const int* gears,
+                                         int num_gears, const int* gear_orders, int p_max, int max_pairs,
+                                         void* stream, jb_dsched** out) {
+  if (num_nodes < 0 || !far_off || !far_src || !gears || !gear_orders || num_gears < 1 || num_gears > 64 ||
+      max_pairs < 1 || max_pairs > 65535 || p_max < 1 || p_max > JB_MAX_ORDER)
+    return JB_ERR_ARG;
+  const int nseg = std::min(kMixedSegMax, (p_max + 1) / 2);
+  GearSegments gs{};
+  for (int g = 0; g < num_gears; ++g) {
+    const int o = gear_orders[g], d = p_max - o;
+    if (o < 1 || d < 0 || (d & 1) || d / 2 >= nseg) return JB_ERR_ARG;
+    gs.seg[g] = d / 2;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  return run_builder(out, st, [&](jb_dsched& d) {
+    build_gears_mixed(d, num_nodes, far_off, far_src, gears, num_gears, gs, max_pairs, st);
   });
 }
 

@@ -11,6 +11,7 @@ only; every arithmetic step is a kernel of libjaccpot_b200.so.
 from __future__ import annotations
 
 import copy
+import dataclasses
 
 from dataclasses import dataclass
 
@@ -18,8 +19,9 @@ import numpy as np
 import torch
 
 from . import _lib
-from .schedule import (gear_m2l_schedule, gear_m2l_schedule_device, leaf_schedule, leaf_schedule_device,
-                       m2l_schedule, m2l_schedule_device, tc_m2l_schedule)
+from .schedule import (MixedGearM2LSchedule, gear_m2l_mixed_schedule, gear_m2l_mixed_schedule_device,
+                       gear_m2l_schedule, gear_m2l_schedule_device, leaf_schedule, leaf_schedule_device,
+                       m2l_schedule, m2l_schedule_device, mixed_ladder, tc_m2l_schedule)
 from .tree import Topology
 
 
@@ -157,6 +159,22 @@ def _restrict_gears(gs, targets, num_nodes: int, dev):
     return GearM2LSchedule(units, split, gs.num_slots, gs.far_src, new_offs.numpy(), gs.orders, gs.pairs_per_gear)
 
 
+def _restrict_mixed(gs, targets, num_nodes: int, dev):
+    """The mixed gear schedule's units (with their bounds) and split entries
+    of the given target nodes only; units keep their order and slots."""
+    units = torch.as_tensor(gs.units).to(dev)
+    bounds = torch.as_tensor(gs.bounds).to(dev)
+    split = torch.as_tensor(gs.split).to(dev)
+    keep = torch.zeros(num_nodes, dtype=torch.bool, device=dev)
+    keep[torch.as_tensor(np.asarray(targets, dtype=np.int64)).to(dev)] = True
+    if units.shape[0]:
+        mask = keep[units[:, 0].long()]
+        units, bounds = units[mask].contiguous(), bounds[mask].contiguous()
+    if split.shape[0]:
+        split = split[keep[split[:, 0].long()]].contiguous()
+    return dataclasses.replace(gs, units=units, bounds=bounds, split=split)
+
+
 class Pass:
     """One evaluation pass over a resident topology; every method enqueues
     kernels on `stream` (default: torch's current stream) and returns."""
@@ -164,7 +182,7 @@ class Pass:
     def __init__(self, dt: DeviceTopology, p: int, *, G: float = 1.0, eps2: float = 0.0,
                  m2l_mode: int = _lib.JB_M2L_FP32, p2p_mode: int = _lib.JB_P2P_FP32,
                  leaf_range: tuple[int, int] | None = None, m2l_unit_pairs: int | None = None,
-                 leaf_unit_sources: int = 4096, gear_unit_pairs: int = 128):
+                 leaf_unit_sources: int = 4096, gear_unit_pairs: int = 128, gear_form: str = "mixed"):
         if not (1 <= int(p) <= _lib.JB_MAX_ORDER):
             raise ValueError(f"max_order must be in [1, {_lib.JB_MAX_ORDER}], got {p}")
         if dt.topo.max_leaf_occupancy > _lib.JB_MAX_LEAF_OCCUPANCY:
@@ -184,6 +202,11 @@ class Pass:
         # work-unit sizes (pairs per M2L unit, per gear unit; sources per leaf
         # unit), measured at clustered N=4M, p=8
         self.gear_unit_pairs = int(gear_unit_pairs)
+        # per-pair gears: "mixed" (one launch, jb_m2l_mixed) when the orders lie
+        # on mixed_ladder(p), else (or "per_gear") one launch per gear
+        if gear_form not in ("mixed", "per_gear"):
+            raise ValueError(f"gear_form must be 'mixed' or 'per_gear', got {gear_form!r}")
+        self.gear_form = gear_form
         if m2l_unit_pairs is None:  # the tensor-core form steps a group's units together: shorter units
             m2l_unit_pairs = 64 if self.m2l_mode == _lib.JB_M2L_SPLIT_BF16 else 512
         self.m2l_unit_pairs = int(m2l_unit_pairs)
@@ -265,14 +288,30 @@ class Pass:
         orders = tuple(int(o) for o in orders)
         if max(orders) > self.p or min(orders) < 1:
             raise ValueError(f"gear orders must lie in [1, {self.p}]")
+        dev = self.dt.device
+        up = lambda a: _up(a, dev)
+        if (self.gear_form == "mixed" and self.m2l_mode == _lib.JB_M2L_FP32
+                and all(o in mixed_ladder(self.p) for o in orders)):
+            if _on_gpu(self.dt):
+                gs = gear_m2l_mixed_schedule_device(self.dt, gears, orders, self.p, max_pairs=self.gear_unit_pairs)
+            else:
+                gs = gear_m2l_mixed_schedule(self.dt.topo, np.asarray(gears), orders, self.p,
+                                             max_pairs=self.gear_unit_pairs)
+            if getattr(self, "_range_targets", None) is not None:
+                gs = _restrict_mixed(gs, self._range_targets, self.dt.topo.num_nodes, dev)
+            self.gear_sched = gs
+            self.d_gear_units = up(gs.units)
+            self.d_gear_bounds = up(gs.bounds)
+            self.d_gear_split = up(gs.split)
+            self.d_gear_src = up(gs.far_src)
+            self.gear_partials = torch.empty((max(gs.num_slots, 1), self.ws.stride), device=dev, dtype=torch.float32)
+            return
         if _on_gpu(self.dt):
             gs = gear_m2l_schedule_device(self.dt, gears, orders, max_pairs=self.gear_unit_pairs)
         else:
             gs = gear_m2l_schedule(self.dt.topo, np.asarray(gears), orders, max_pairs=self.gear_unit_pairs)
         if getattr(self, "_range_targets", None) is not None:
             gs = _restrict_gears(gs, self._range_targets, self.dt.topo.num_nodes, self.dt.device)
-        dev = self.dt.device
-        up = lambda a: _up(a, dev)
         self.gear_sched = gs
         self.d_gear_units = up(gs.units)
         self.d_gear_split = up(gs.split)
@@ -288,6 +327,12 @@ class Pass:
             self._m2l_split(s)
             return
         gs = getattr(self, "gear_sched", None)
+        if isinstance(gs, MixedGearM2LSchedule):
+            _lib.check(self.lib.jb_m2l_mixed(
+                self.p, int(gs.units.shape[0]), _ptr(self.d_gear_units), _ptr(self.d_gear_bounds), _ptr(ws.mult),
+                _ptr(ws.centers), _ptr(self.d_gear_src), _ptr(ws.locals), _ptr(self.gear_partials),
+                int(gs.split.shape[0]), _ptr(self.d_gear_split), s), "jb_m2l_mixed")
+            return
         if gs is not None:
             _lib.check(self.lib.jb_m2l_gears(
                 self.p, self.m2l_mode, len(gs.orders), self.h_gear_orders.ctypes.data,
@@ -539,7 +584,9 @@ class Pass:
         reduce, one L2L per level, the leaf L2P + P2P and their split reduce."""
         t = self.dt.topo
         gs = getattr(self, "gear_sched", None)
-        if gs is not None and self.m2l_mode == _lib.JB_M2L_FP32:
+        if isinstance(gs, MixedGearM2LSchedule):
+            m2l = int(gs.units.shape[0] > 0) + int(gs.split.shape[0] > 0)
+        elif gs is not None and self.m2l_mode == _lib.JB_M2L_FP32:
             m2l = int((np.diff(np.asarray(gs.gear_offsets)) > 0).sum()) + int(gs.split.shape[0] > 0)
         else:
             m2l = 1 + int(self.m2l_sched.split.shape[0] > 0)

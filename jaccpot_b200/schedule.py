@@ -136,6 +136,90 @@ def gear_m2l_schedule(topo: Topology, gears: np.ndarray, orders, max_pairs: int 
                            tuple(int(o) for o in orders), ppg)
 
 
+MIXED_SEGMENTS = 4
+
+
+def mixed_ladder(p_max: int) -> tuple:
+    """Orders the one-launch gear M2L (jb_m2l_mixed) evaluates: p_max,
+    p_max-2, p_max-4, p_max-6, those >= 1."""
+    return tuple(o for o in range(p_max, p_max - 2 * MIXED_SEGMENTS, -2) if o >= 1)
+
+
+@dataclass
+class MixedGearM2LSchedule:
+    """M2L units for per-pair gears whose orders lie on ``mixed_ladder(p_max)``,
+    run in one launch (jb_m2l_mixed).
+
+    ``far_src`` is the CSR source list with each target's pairs sorted by
+    order, highest first (stable inside); ``units`` (target, first, end, slot)
+    are slices of at most ``max_pairs`` of one target's list and ``bounds``
+    (b1, b2, b3, end) cut a unit into the segments [b_j, b_j+1) (b_0 = first)
+    of order p_max - 2j.  Units are sorted by decreasing segment lengths,
+    highest order first (stable), so neighbouring units have similar ones.
+    Targets covered by more than one unit write scratch slots that ``split``
+    sums in slot order."""
+
+    units: np.ndarray  # int32[U, 4]
+    bounds: np.ndarray  # int32[U, 4]
+    split: np.ndarray  # int32[S, 4]
+    num_slots: int
+    far_src: np.ndarray  # int32[num_far] sorted by order inside each target
+    orders: tuple
+    pairs_per_gear: np.ndarray  # int64[G]
+    p_max: int
+
+
+def _mixed_segments(orders, p_max: int) -> np.ndarray:
+    ladder = mixed_ladder(p_max)
+    if any(int(o) not in ladder for o in orders):
+        raise ValueError(f"gear orders {tuple(orders)} are not on the ladder {ladder}")
+    return np.array([(p_max - int(o)) // 2 for o in orders], dtype=np.int64)
+
+
+def gear_m2l_mixed_schedule(topo: Topology, gears: np.ndarray, orders, p_max: int,
+                            max_pairs: int = 128) -> MixedGearM2LSchedule:
+    gears = np.asarray(gears, dtype=np.int64).reshape(-1)
+    if gears.shape[0] != topo.num_far_pairs:
+        raise ValueError("one gear per far pair is required")
+    ng = len(orders)
+    if gears.size and (gears.min() < 0 or gears.max() >= ng):
+        raise ValueError("gear index out of range")
+    seg_of = _mixed_segments(orders, p_max)
+    off = topo.far_offsets.astype(np.int64)
+    nodes = topo.num_nodes
+    tgt = np.repeat(np.arange(nodes, dtype=np.int64), np.diff(off))
+    seg = seg_of[gears] if gears.size else np.zeros(0, np.int64)
+    order = np.lexsort((seg, tgt))  # by target, then segment (stable inside)
+    far_src = topo.far_sources[order].astype(np.int32)
+    ppg = np.bincount(gears, minlength=ng).astype(np.int64)
+    z4 = np.zeros((0, 4), np.int32)
+    if order.size == 0:
+        return MixedGearM2LSchedule(z4, z4, z4, 0, far_src, tuple(orders), ppg, int(p_max))
+    # segment starts of every target: off + counts of the higher segments
+    cnt = np.zeros((nodes, MIXED_SEGMENTS), np.int64)
+    np.add.at(cnt, (tgt, seg), 1)
+    starts = off[:-1, None] + np.concatenate([np.zeros((nodes, 1), np.int64), np.cumsum(cnt, axis=1)], axis=1)
+    n_t = np.diff(off)
+    nu = (n_t + max_pairs - 1) // max_pairs
+    u_t = np.repeat(np.arange(nodes, dtype=np.int64), nu)
+    k = np.arange(int(nu.sum())) - np.repeat(np.cumsum(nu) - nu, nu)
+    u_s = off[u_t] + k * max_pairs
+    u_e = np.minimum(u_s + max_pairs, off[u_t + 1])
+    bd = np.clip(starts[u_t], u_s[:, None], u_e[:, None])  # [U, 5]: b_0 = first .. b_4 = end
+    slot, first_slot = _slots(nu[nu > 0])
+    units = np.stack([u_t, u_s, u_e, slot], axis=1).astype(np.int32)
+    bounds = np.stack([bd[:, 1], bd[:, 2], bd[:, 3], u_e], axis=1).astype(np.int32)
+    c = np.diff(bd, axis=1)  # segment lengths
+    srt = np.lexsort(tuple(-c[:, j] for j in range(MIXED_SEGMENTS - 1, -1, -1)))
+    t_nonempty = np.nonzero(nu > 0)[0]
+    sp = nu[t_nonempty] > 1
+    split = np.stack([t_nonempty[sp], first_slot[sp], nu[t_nonempty][sp], np.zeros(int(sp.sum()), np.int64)],
+                     axis=1).astype(np.int32)
+    return MixedGearM2LSchedule(np.ascontiguousarray(units[srt]), np.ascontiguousarray(bounds[srt]),
+                                np.ascontiguousarray(split), int((slot >= 0).sum()), far_src,
+                                tuple(int(o) for o in orders), ppg, int(p_max))
+
+
 @dataclass
 class TcM2LSchedule:
     """Tiles of 128 consecutive far pairs (CSR order, sorted by target) for the
@@ -330,6 +414,34 @@ def leaf_schedule_device(dt, max_sources: int = 4096, leaf_range: tuple[int, int
     finally:
         free()
     return LeafSchedule(units, aux, runs, split, int(info.num_slots))
+
+
+def gear_m2l_mixed_schedule_device(dt, gears, orders, p_max: int, max_pairs: int = 128) -> MixedGearM2LSchedule:
+    """GPU twin of :func:`gear_m2l_mixed_schedule`."""
+    import torch
+
+    from . import _lib
+
+    _mixed_segments(orders, p_max)  # the library checks the same; this gives the message
+    t = dt.topo
+    g = torch.as_tensor(gears).to(device=dt.device, dtype=torch.int32).reshape(-1).contiguous()
+    if g.numel() != t.num_far_pairs:
+        raise ValueError("one gear per far pair is required")
+    ng = len(orders)
+    ho = np.ascontiguousarray(np.array(orders, dtype=np.int32))
+    info, field, free = _run_device("jb_gear_mixed_schedule_device",
+                                    [t.num_nodes, _ptr(dt.far_off), _ptr(dt.far_src), _ptr(g), ng, ho.ctypes.data,
+                                     int(p_max), int(max_pairs)], dt.device)
+    try:
+        units = field(_lib.JB_SCHED_UNITS, (info.num_units, 4), np.int32)
+        bounds = field(_lib.JB_SCHED_AUX, (info.num_units, 4), np.int32)
+        split = field(_lib.JB_SCHED_SPLIT, (info.num_split, 4), np.int32)
+        far_src = field(_lib.JB_SCHED_FAR_SOURCES, (t.num_far_pairs,), np.int32)
+        ppg = field(_lib.JB_SCHED_PAIRS_PER_GEAR, (ng,), np.int64).cpu().numpy()
+    finally:
+        free()
+    return MixedGearM2LSchedule(units, bounds, split, int(info.num_slots), far_src, tuple(int(o) for o in orders),
+                                ppg, int(p_max))
 
 
 def gear_m2l_schedule_device(dt, gears, orders, max_pairs: int = 64) -> GearM2LSchedule:

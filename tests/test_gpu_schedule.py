@@ -86,6 +86,26 @@ def test_gear_schedule(topo, ng):
         schedule.gear_m2l_schedule_device(dt, bad, orders)
 
 
+@pytest.mark.parametrize("orders,max_pairs", [((2, 4, 6, 8), 128), ((2, 4, 6, 8), 5), ((6, 8), 64), ((8,), 128)])
+def test_mixed_gear_schedule(topo, orders, max_pairs):
+    dt = topo[0]
+    ng = len(orders)
+    rng = np.random.default_rng(ng + max_pairs)
+    gears = rng.integers(0, ng, size=dt.topo.num_far_pairs)
+    gears[: gears.size // 2] = np.sort(gears[: gears.size // 2])
+    want = schedule.gear_m2l_mixed_schedule(dt.topo, gears, orders, 8, max_pairs=max_pairs)
+    got = schedule.gear_m2l_mixed_schedule_device(dt, gears, orders, 8, max_pairs=max_pairs)
+    for f in ("units", "bounds", "split", "far_src", "pairs_per_gear"):
+        same(getattr(got, f), getattr(want, f), f)
+    assert got.num_slots == want.num_slots
+    bad = gears.copy()
+    bad[5] = ng
+    with pytest.raises(_lib.JBError):
+        schedule.gear_m2l_mixed_schedule_device(dt, bad, orders, 8)
+    with pytest.raises(ValueError):
+        schedule.gear_m2l_mixed_schedule_device(dt, gears, tuple(o - 1 for o in orders), 8)
+
+
 def test_pass_is_identical_through_either_schedule(topo):
     dt, pos, mass = topo
     ps = engine.Pass(dt, 6, G=1.0, eps2=1e-6, p2p_mode=_lib.JB_P2P_KAHAN)  # device schedules
