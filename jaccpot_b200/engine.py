@@ -58,6 +58,11 @@ class DeviceTopology:
         self.m2l_targets = up(topo.m2l_targets if topo.m2l_targets.size else np.zeros(1, np.int32), torch.int32)
         self.num_m2l_targets = int(topo.m2l_targets.size)
         self.level_offsets = [int(x) for x in topo.level_offsets]
+        # the L2L levels above the shallowest internal far target move zeros
+        # (every local there is zero): the sweep starts at that level
+        ni = topo.num_internal
+        tgt = np.nonzero(np.diff(np.asarray(topo.far_offsets))[:ni] > 0)[0]
+        self.l2l_first_level = int(np.asarray(topo.node_level)[tgt].min()) if tgt.size else int(topo.num_levels)
 
     def far_reverse_index(self) -> torch.Tensor:
         """int32[num_far] on the device: the reverse pair (s <- t) of every far
@@ -440,7 +445,7 @@ class Pass:
     def l2l(self, stream=None) -> None:
         t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)
         lo = dt.level_offsets
-        for lev in range(t.num_levels):
+        for lev in range(dt.l2l_first_level, t.num_levels):
             _lib.check(self.lib.jb_l2l_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
                                              _ptr(ws.centers), _ptr(ws.locals), s), "jb_l2l_level")
 
@@ -581,7 +586,8 @@ class Pass:
     def launches_per_run(self) -> int:
         """This library's kernel launches in one run(): P2M, one M2M per level,
         the M2L (one launch per non-empty gear with gears) and its split
-        reduce, one L2L per level, the leaf L2P + P2P and their split reduce."""
+        reduce, one L2L per level from the first with a non-zero local, the
+        leaf L2P + P2P and their split reduce."""
         t = self.dt.topo
         gs = getattr(self, "gear_sched", None)
         if isinstance(gs, MixedGearM2LSchedule):
@@ -590,4 +596,5 @@ class Pass:
             m2l = int((np.diff(np.asarray(gs.gear_offsets)) > 0).sum()) + int(gs.split.shape[0] > 0)
         else:
             m2l = 1 + int(self.m2l_sched.split.shape[0] > 0)
-        return (1 + t.num_levels + m2l + t.num_levels + 2 + int(self.leaf_sched.split.shape[0] > 0))
+        l2l = t.num_levels - self.dt.l2l_first_level
+        return (1 + t.num_levels + m2l + l2l + 2 + int(self.leaf_sched.split.shape[0] > 0))
