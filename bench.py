@@ -65,11 +65,13 @@ ERR_TARGETS = 32768
 ERR_BOUND = 1e-4
 # Each form's accuracy parameter is chosen in the run: the largest value on
 # its grid whose p99 on a selection sample of ERR_TARGETS targets (and on its
-# first 4,096) stays within SELECT_BOUND; errors are then reported on a
-# disjoint sample of the same size.
+# first 4,096) stays within SELECT_BOUND, refined by EPS_REFINE bisection
+# steps towards the failing grid value above it; errors are then reported on
+# a disjoint sample of the same size.
 SELECT_BOUND = 0.9 * ERR_BOUND
 THETA_GRID = (0.6, 0.59, 0.58, 0.57, 0.56, 0.55, 0.53, 0.5)
 EPS_GRID = (5e-5, 4e-5, 3.5e-5, 3e-5, 2.5e-5, 2e-5, 1.5e-5, 1e-5)
+EPS_REFINE = 2
 GEARS = (2, 4, 6, 8)
 
 
@@ -380,6 +382,38 @@ def measure_extras(dev, stream) -> dict:
     return out
 
 
+def measure_monitor(fmm, state, d_pos, d_mass, targets: int = 256, reps: int = 3) -> dict:
+    """The facade's sampled error monitor on the chosen pass at the headline
+    size: a whole re-evaluation (differentiable_accelerations on resident
+    inputs) without and with one FP64 direct-sum check of `targets` random
+    particles; wall clock around synchronised calls (the check reads its
+    percentiles back)."""
+    import torch
+
+    from jaccpot_b200.solver import _monitor_config
+
+    def wall(k):
+        ts = []
+        for _ in range(k):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fmm.differentiable_accelerations(state, d_pos, d_mass)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * float(np.median(ts))
+
+    saved = fmm.error_monitor
+    fmm.error_monitor = None
+    off = wall(reps)
+    fmm.error_monitor = _monitor_config({"targets": targets, "bound": ERR_BOUND})
+    on = wall(reps)
+    last = dict(fmm.error_history[-1])
+    fmm.error_monitor = saved
+    return {"targets": targets, "pass_ms": off, "pass_with_check_ms": on, "check_ms": on - off,
+            "last_check": last, "note": "advanced={'error_monitor': ...}: FP64 direct sum on sampled targets "
+                                        "after each whole-pass evaluation (jb_direct_f64), wall clock"}
+
+
 def measure_gear_selector(dev, stream, n: int = 2097152, seed: int = 200, theta: float = 0.55) -> dict:
     """Config 4: the learned gear selector (MLP, gears 2/4/6/8) on the theta
     lists of a clustered system of a seed it never saw, against the plain
@@ -508,17 +542,27 @@ def main() -> None:
     # theta walk; theta = the largest of THETA_GRID that meets the bound on the
     # selection sample (whole-tree passes, identical on every rank)
     sel = {"bound": SELECT_BOUND, "targets": int(tg_sel.size), "plain": [], "chosen": []}
-    plain_theta = THETA_GRID[-1]
-    for th in THETA_GRID:
+    def try_theta(th) -> bool:
         topo_t = tree.build_topology(pos, mass, leaf_size=cfg["leaf_size"], theta=th, device=dev)
         ps_t = engine.Pass(engine.DeviceTopology(topo_t, dev), cfg["order"], G=1.0, eps2=0.0)
         ps_t.load_particles(d_pos, d_mass)
         e = errors_of(ps_t.run(), topo_t, tg_sel, ref_sel)
         sel["plain"].append({"theta": th, "p99": e["p99"], "p99_first_4096": e["p99_first_4096"]})
         del ps_t
-        if meets(e):
+        return meets(e)
+
+    plain_theta, failed_theta = THETA_GRID[-1], None
+    for th in THETA_GRID:
+        if try_theta(th):
             plain_theta = th
             break
+        failed_theta = th
+    for _ in range(EPS_REFINE if failed_theta is not None else 0):  # the same refinement as the chosen form's
+        mid = round(0.5 * (plain_theta + failed_theta), 6)
+        if try_theta(mid):
+            plain_theta = mid
+        else:
+            failed_theta = mid
     cfg["theta"] = plain_theta
 
     # chosen: the error-controlled walk (Dehnen eq. 15/16a acceptance, per-pair
@@ -530,15 +574,27 @@ def main() -> None:
                                    adaptive_error_model="dehnen_paper", adaptive_eps=eps,
                                    mac_force_scale_mode="paper", device=dev, nearfield_compensated=True)
 
-    chosen_eps = EPS_GRID[-1]
-    for eps in EPS_GRID:
+    def try_eps(eps) -> bool:
         st_e = chosen_solver(eps).prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
         e = errors_of(st_e.pass_.evaluate(), st_e.topology, tg_sel, ref_sel)
         sel["chosen"].append({"eps": eps, "p99": e["p99"], "p99_first_4096": e["p99_first_4096"]})
         del st_e
-        if meets(e):
+        return meets(e)
+
+    chosen_eps, failed_eps = EPS_GRID[-1], None
+    for eps in EPS_GRID:
+        if try_eps(eps):
             chosen_eps = eps
             break
+        failed_eps = eps
+    # then EPS_REFINE log-space bisection steps between the passing eps and
+    # the failing grid value above it
+    for _ in range(EPS_REFINE if failed_eps is not None else 0):
+        mid = float(np.sqrt(chosen_eps * failed_eps))
+        if try_eps(mid):
+            chosen_eps = mid
+        else:
+            failed_eps = mid
 
     fmm = chosen_solver(chosen_eps)
     torch.cuda.synchronize()
@@ -760,6 +816,8 @@ def main() -> None:
                          f"M2L of the nodes meeting the slice, L2P + P2P of its leaves"}
 
     extras = measure_extras(dev, stream) if (rank == 0 and world == 1 and not args.no_extras) else None
+    if extras is not None:
+        extras["error_monitor"] = measure_monitor(fmm, state, d_pos, d_mass)
     prep = measure_prepare(pos, mass, cfg, dev, with_host=not args.no_extras, fmm=fmm) if rank == 0 else None
     launches = passes["chosen"].launches_per_run() + 2  # + gather + unsort
     if rank == 0:

@@ -2,7 +2,10 @@
 #include "device_symbol.cuh"
 #include "fmm_adjoint.cuh"
 
+#include <cooperative_groups.h>
 #include <mutex>
+
+namespace cg = cooperative_groups;
 
 #define JB_ORDERS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 JB_ORDERS(JB_DECLARE_ORDER)
@@ -133,29 +136,39 @@ static int dispatch_adj(int p, Fn&& fn) {
 // ---------------------------------------------------------------------------
 // Verification: FP64 direct sum on sampled targets (the error report every
 // result carries; runtime/reference.py:292 semantics, self pair excluded).
-// Block per target, threads stride over all sources, FP64 tree reduction.
+// A cluster of kDirectParts blocks per target: block r of the cluster sums
+// the sources of its r-th share with 256 threads in FP64 and reduces them
+// in shared memory; after the cluster barrier, block 0 adds the blocks'
+// sums in rank order through distributed shared memory, so the result does
+// not depend on scheduling and needs no scratch.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_direct_f64(int64_t n, const float4* __restrict__ pos4, int64_t nt,
-                                                    const int* __restrict__ tsorted, double G, double eps2,
-                                                    double* __restrict__ out) {
+constexpr int kDirectParts = 8;
+
+__global__ void __cluster_dims__(kDirectParts, 1, 1) __launch_bounds__(256)
+    k_direct_f64(int64_t n, const float4* __restrict__ pos4, int64_t nt, const int* __restrict__ tsorted, double G,
+                 double eps2, double* __restrict__ out) {
   __shared__ double red[4][256];
-  const int64_t q = blockIdx.x;
-  if (q >= nt) return;
-  const int i = tsorted[q];
-  const float4 ti = pos4[i];
-  const double xi = ti.x, yi = ti.y, zi = ti.z;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int part = (int)cluster.block_rank();
+  const int64_t q = blockIdx.x / kDirectParts;  // every block of a cluster has the same target
+  const int i = q < nt ? tsorted[q] : -1;
   double ax = 0, ay = 0, az = 0, ph = 0;
-  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
-    if (j == i) continue;
-    const float4 s = pos4[j];
-    const double dx = xi - s.x, dy = yi - s.y, dz = zi - s.z;
-    const double d2 = dx * dx + dy * dy + dz * dz + eps2;
-    const double ir = 1.0 / sqrt(d2);
-    const double w = (double)s.w * ir * ir * ir;
-    ax += w * dx;
-    ay += w * dy;
-    az += w * dz;
-    ph += (double)s.w * ir;
+  if (q < nt) {
+    const float4 ti = pos4[i];
+    const double xi = ti.x, yi = ti.y, zi = ti.z;
+    const int64_t j0 = n * part / kDirectParts, j1 = n * (part + 1) / kDirectParts;
+    for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+      if (j == i) continue;
+      const float4 s = pos4[j];
+      const double dx = xi - s.x, dy = yi - s.y, dz = zi - s.z;
+      const double d2 = dx * dx + dy * dy + dz * dz + eps2;
+      const double ir = rsqrt(d2);
+      const double w = (double)s.w * ir * ir * ir;
+      ax += w * dx;
+      ay += w * dy;
+      az += w * dz;
+      ph += (double)s.w * ir;
+    }
   }
   red[0][threadIdx.x] = ax;
   red[1][threadIdx.x] = ay;
@@ -167,12 +180,13 @@ __global__ void __launch_bounds__(256) k_direct_f64(int64_t n, const float4* __r
       for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    out[4 * q + 0] = -G * red[0][0];
-    out[4 * q + 1] = -G * red[1][0];
-    out[4 * q + 2] = -G * red[2][0];
-    out[4 * q + 3] = -G * red[3][0];
+  cluster.sync();  // every block's sum is in its shared memory
+  if (part == 0 && q < nt && threadIdx.x < 4) {
+    double sum = 0;
+    for (int r = 0; r < kDirectParts; ++r) sum += cluster.map_shared_rank(&red[0][0], r)[threadIdx.x * 256];
+    out[4 * q + threadIdx.x] = -G * sum;
   }
+  cluster.sync();  // the other blocks' shared memory stays until block 0 has read it
 }
 
 // Throughput probe.  mode 0: FP32 FMA chains (8 independent per thread);
@@ -472,8 +486,9 @@ JB_API int jb_direct_f64(int64_t n, const float* pos4, int64_t num_targets, cons
                          double eps2, double* out4, void* stream) {
   if (n < 1 || num_targets < 0 || (num_targets > 0 && (!pos4 || !targets_sorted || !out4))) return JB_ERR_ARG;
   if (num_targets == 0) return JB_OK;
-  k_direct_f64<<<(unsigned)num_targets, 256, 0, ST(stream)>>>(n, reinterpret_cast<const float4*>(pos4), num_targets,
-                                                              targets_sorted, G, eps2, out4);
+  if (num_targets > (int64_t)0x7fffffff / kDirectParts) return JB_ERR_ARG;
+  k_direct_f64<<<(unsigned)(num_targets * kDirectParts), 256, 0, ST(stream)>>>(
+      n, reinterpret_cast<const float4*>(pos4), num_targets, targets_sorted, G, eps2, out4);
   return launch_status();
 }
 

@@ -71,7 +71,28 @@ _GEOMETRY_MODES = ("com", "exact", "tree", "tree_approx", "runtime")
 # Options of this implementation that the reference's constructor does not
 # have; they are taken from ``advanced`` (a dict or an object with these
 # attributes) or as extra keywords, like the reference's legacy keywords.
-_EXTENSIONS = {"device": "cuda", "nearfield_compensated": False, "gear_model": None}
+_EXTENSIONS = {"device": "cuda", "nearfield_compensated": False, "gear_model": None, "error_monitor": None}
+
+
+def _monitor_config(cfg) -> Optional[dict]:
+    """error_monitor: None (off), an int (targets per check), or a dict with
+    targets (default 256), every (check every k-th whole-pass evaluation,
+    default 1), bound (p99 relative error a check is judged against, default
+    1e-4), seed (default 0), keep (checks kept, default 1000)."""
+    if cfg is None or cfg is False:
+        return None
+    if isinstance(cfg, (int, np.integer)) and not isinstance(cfg, bool):
+        cfg = {"targets": int(cfg)}
+    if not isinstance(cfg, dict):
+        raise TypeError("error_monitor must be None, an int or a dict")
+    unknown = sorted(set(cfg) - {"targets", "every", "bound", "seed", "keep"})
+    if unknown:
+        raise TypeError(f"unknown error_monitor options: {unknown}")
+    out = {"targets": int(cfg.get("targets", 256)), "every": int(cfg.get("every", 1)),
+           "bound": float(cfg.get("bound", 1e-4)), "seed": int(cfg.get("seed", 0)), "keep": int(cfg.get("keep", 1000))}
+    if out["targets"] < 1 or out["every"] < 1 or out["keep"] < 1 or not out["bound"] > 0.0:
+        raise ValueError("error_monitor: targets, every and keep must be >= 1 and bound > 0")
+    return out
 
 
 def _advanced_options(advanced, legacy: dict) -> dict:
@@ -200,6 +221,10 @@ class FastMultipoleMethod:
         self._force_scale_cache = None  # per-particle |a| of the last evaluation (input order)
         self._counters = {"prepare_state": 0, "evaluate": 0, "reuse_hits": 0, "reuse_rebuilds": 0,
                           "adaptive_prepares": 0, "force_scale_prepasses": 0, "force_scale_reused": 0}
+        # sampled FP64 direct-sum checks of whole-pass evaluations (off by default)
+        self.error_monitor = _monitor_config(ext["error_monitor"])
+        self.error_history: list = []
+        self._monitor_calls = 0
 
     # ------------------------------------------------------------------ prepare
     def _gear_orders(self, max_order: int) -> tuple:
@@ -422,6 +447,8 @@ class FastMultipoleMethod:
             acc = out[:, :3].contiguous()
             pot = out[:, 3].contiguous() if return_potential else None
         self._counters["evaluate"] += 1
+        if target_indices is None:
+            self._monitor_check(state)
         if (target_indices is None and self.adaptive_error_model == "dehnen_paper"
                 and self.mac_force_scale_mode in ("prev", "paper_cached")):
             # the next error-controlled prepare takes its force scale from here
@@ -479,6 +506,7 @@ class FastMultipoleMethod:
         ps.load_particles(pos, mass)
         ps.run()
         ps.unsort(acc, None)
+        self._monitor_check(state)
         if not host:
             return acc
         if out is None:
@@ -696,12 +724,49 @@ class FastMultipoleMethod:
             history = history.cpu().numpy()
         return out, (st if return_prepared_state else None), history
 
+    # ------------------------------------------------------------ error monitor
+    def _monitor_check(self, state: FMMPreparedState) -> None:
+        """One sampled check of the whole-pass evaluation just run on
+        ``state`` (its sorted results are in the pass's acc4): an FP64 direct
+        sum (jb_direct_f64, the same G and softening, self pair excluded) on
+        ``targets`` random particles, their relative force errors summarised
+        into ``error_history``.  Synchronises the stream."""
+        m = self.error_monitor
+        if m is None:
+            return
+        self._monitor_calls += 1
+        if (self._monitor_calls - 1) % m["every"]:
+            return
+        ps = state.pass_
+        n = state.num_particles
+        dev = state.device_topology.device
+        k = min(m["targets"], n)
+        rng = np.random.default_rng((m["seed"], self._monitor_calls))
+        ts = torch.from_numpy(rng.choice(n, size=k, replace=False).astype(np.int32)).to(dev)
+        ref = torch.empty((k, 4), device=dev, dtype=torch.float64)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().jb_direct_f64(n, ps.ws.pos4.data_ptr(), k, ts.data_ptr(), float(ps.G), float(ps.eps2),
+                                            ref.data_ptr(), stream), "jb_direct_f64")
+        got = ps.ws.acc4[ts.long(), :3].double()
+        r = ref[:, :3]
+        e = (torch.linalg.vector_norm(got - r, dim=1) / torch.linalg.vector_norm(r, dim=1).clamp_min(1e-300)).cpu()
+        q = torch.quantile(e, torch.tensor([0.5, 0.99], dtype=torch.float64)).tolist()
+        rec = {"evaluation": self._monitor_calls, "targets": k, "p50": q[0], "p99": q[1], "max": float(e.max()),
+               "within_bound": q[1] <= m["bound"]}
+        self.error_history.append(rec)
+        del self.error_history[:-m["keep"]]
+        self._counters["error_checks"] = self._counters.get("error_checks", 0) + 1
+        if not rec["within_bound"]:
+            self._counters["error_checks_over_bound"] = self._counters.get("error_checks_over_bound", 0) + 1
+
     # ------------------------------------------------------ caches, counters
     def get_runtime_diagnostics(self) -> dict:
         """Counters of this solver (solver.py:2049 there): prepares,
         evaluations, reuse hits, refresh statistics, adaptive prepares and
         force-scale prepasses.  Not a stable schema."""
         d = dict(self._counters)
+        if self.error_history:
+            d["last_error_check"] = dict(self.error_history[-1])
         d["refresh"] = dict(getattr(self, "refresh_stats", {}))
         d["has_last_state"] = self._last_state is not None
         return d

@@ -139,3 +139,18 @@ def test_strict_run_v2_requires_refresh_every_one():
     with pytest.raises(ValueError, match="refresh_every=1"):
         f.strict_run_v2(state=np.zeros((4, 2, 3)), masses=np.ones(4), dt=0.1, num_steps=2, refresh_every=2,
                         leaf_size=8, max_order=4)
+
+
+def test_error_monitor_options():
+    assert FastMultipoleMethod().error_monitor is None
+    f = FastMultipoleMethod(advanced={"error_monitor": 64})
+    assert f.error_monitor == {"targets": 64, "every": 1, "bound": 1e-4, "seed": 0, "keep": 1000}
+    f = FastMultipoleMethod(error_monitor={"targets": 8, "every": 5, "bound": 2e-4})
+    assert (f.error_monitor["every"], f.error_monitor["bound"]) == (5, 2e-4)
+    assert f.error_history == [] and "last_error_check" not in f.get_runtime_diagnostics()
+    with pytest.raises(ValueError):
+        FastMultipoleMethod(advanced={"error_monitor": {"targets": 0}})
+    with pytest.raises(TypeError):
+        FastMultipoleMethod(advanced={"error_monitor": {"sample": 3}})
+    with pytest.raises(TypeError):
+        FastMultipoleMethod(advanced={"error_monitor": "often"})
