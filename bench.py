@@ -153,7 +153,7 @@ def _peaks() -> dict:
 # DRAM bytes (read + write) per launch of the dominant kernels at the bench
 # workload, scaled from single-launch ncu captures of a 1M-particle case by
 # the units processed (far pairs / particle pairs); see profiles/.
-TRAFFIC_PER_UNIT = {"k_m2l_units": 7.8, "k_m2l_tc_units": 12.3, "k_leaf_units_flat": 0.0133}
+TRAFFIC_PER_UNIT = {"k_m2l_units": 7.8, "k_m2l_mixed": 10.7, "k_m2l_tc_units": 12.3, "k_leaf_units_flat": 0.0124}
 
 
 def _traffic(kernel: str, units: float | None = None):
@@ -164,7 +164,7 @@ def _traffic(kernel: str, units: float | None = None):
 
 
 # ---------------------------------------------------------------------------
-REF_THETA = 0.58  # the theta the plain form's in-run selection picks for this workload
+REF_THETA = 0.5875  # the theta the plain form's in-run selection picks for this workload
 REF_SLICES = 8
 
 
@@ -476,6 +476,9 @@ def main() -> None:
     ap.add_argument("--n", type=int, default=WORKLOAD["N"], help="particle count (default: the headline 4M)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extras", action="store_true", help="skip the target-subset and adjoint measurements")
+    ap.add_argument("--profile", choices=["chosen", "plain", "split_bf16", "learned_gears"], default=None,
+                    help="after the warm-up, run one step of this form between cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -691,6 +694,11 @@ def main() -> None:
         for _ in range(args.warmup):
             step(ps)
         torch.cuda.synchronize()
+    if args.profile is not None and args.profile in passes:
+        torch.cuda.profiler.start()
+        step(passes[args.profile])
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
     # every form timed in turn; clocks sampled over all timed regions
     timings = {}
     with ClockSampler(local) as cs:
