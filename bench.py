@@ -18,11 +18,15 @@ reported on another):
   split_bf16, learned_gears -- reported beside (plain's lists with the
              tensor-core M2L, or with the MLP-selected gears).
 
-`value` is particles/s of the chosen form with inputs resident in HBM; `e2e`
-is the same metric through the public API (FastMultipoleMethod.
-differentiable_accelerations on the prepared state) from pinned host buffers,
-H2D + pass + D2H inside the timed region.  L2 is flushed (256 MiB write)
-between timed steps; each step is timed with CUDA events on its stream.
+`value` is particles/s of the chosen form with inputs resident in HBM, its step
+(gather + pass + un-permute) replayed as a CUDA graph (Pass.capture); `e2e` is
+the same metric through the public API (FastMultipoleMethod.
+differentiable_accelerations on the prepared state, whose cuda_graph option
+replays the same graph) from pinned host buffers, H2D + pass + D2H inside the
+timed region.  Each form is also timed launching one kernel at a time with an
+event between stages (`config.eager`, the stage times).  L2 is flushed
+(256 MiB write) between timed steps; each step is timed with CUDA events on
+its stream.
 
 `--impl reference` times the CPU restatement of the same pass (the reference
 itself is JAX, which is not installed) on the host cores.
@@ -572,10 +576,11 @@ def main() -> None:
     # gears GEARS) + FP32 M2L + Kahan-compensated P2P, through the public API
     # (adaptive_error_model="dehnen_paper"); eps = the largest of EPS_GRID that
     # meets the bound on the selection sample
-    def chosen_solver(eps):
+    def chosen_solver(eps, graph=False):
         return FastMultipoleMethod(theta=0.6, G=1.0, softening=0.0, adaptive_order=True, p_gears=GEARS,
                                    adaptive_error_model="dehnen_paper", adaptive_eps=eps,
-                                   mac_force_scale_mode="paper", device=dev, nearfield_compensated=True)
+                                   mac_force_scale_mode="paper", device=dev,
+                                   advanced={"nearfield_compensated": True, "cuda_graph": graph})
 
     def try_eps(eps) -> bool:
         st_e = chosen_solver(eps).prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
@@ -599,7 +604,7 @@ def main() -> None:
         else:
             failed_eps = mid
 
-    fmm = chosen_solver(chosen_eps)
+    fmm = chosen_solver(chosen_eps, graph=True)  # the public API's deployed path: a CUDA graph of the step
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     state = fmm.prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
@@ -699,14 +704,39 @@ def main() -> None:
         step(passes[args.profile])
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
-    # every form timed in turn; clocks sampled over all timed regions
-    timings = {}
+    def timed_graph(g, steps: int) -> float:
+        for _ in range(args.warmup):
+            g.replay()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        per = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.replay()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            per.append(e0.elapsed_time(e1))
+        if world > 1:
+            dist.barrier()
+        return float(np.mean(per))
+
+    # every form timed in turn, eagerly with an event between stages; then the
+    # chosen and plain steps as CUDA graphs (Pass.capture: gather + pass +
+    # un-permute, the same launches); clocks sampled over all timed regions
+    timings, graph_ms = {}, {}
     with ClockSampler(local) as cs:
         cs.wait_first()
         for name, ps in passes.items():
             timings[name] = timed(ps, args.steps)
             if name == "split_bf16":
                 ps.check_tc_status()  # a timed-out MMA barrier voids the form's numbers
+        for name in ("chosen", "plain"):
+            g = passes[name].capture(d_pos, d_mass, acc_out)
+            graph_ms[name] = timed_graph(g, args.steps)
+            del g
     clocks = cs.summary()
 
     def reduce_max(x: float) -> float:
@@ -717,7 +747,8 @@ def main() -> None:
         return float(t.item())
 
     ms = {k: reduce_max(v[0]) for k, v in timings.items()}
-    ms_plain, ms_chosen = ms["plain"], ms["chosen"]
+    gms = {k: reduce_max(v) for k, v in graph_ms.items()}
+    ms_plain, ms_chosen = gms["plain"], gms["chosen"]  # the headline: the steps as graphs
     stage_chosen, stage_plain = timings["chosen"][1], timings["plain"][1]
 
     # accuracy of every form against the FP64 direct sum on the report sample
@@ -837,6 +868,10 @@ def main() -> None:
                      "plain's lists with the MLP-selected gears + Kahan P2P"),
             "selection": sel,
             "chosen_vs_plain": ms_plain / ms_chosen,
+            "eager": {"chosen_ms_per_step": ms["chosen"], "plain_ms_per_step": ms["plain"],
+                      "chosen_vs_plain": ms["plain"] / ms["chosen"],
+                      "note": "the same steps launched one kernel at a time with an event between stages "
+                              "(stage_ms_* come from these runs)"},
             "chosen": {"eps": chosen_eps, "gears": list(GEARS), "theta_max": 1.0, "theta_prepass": 0.6,
                        "far_pairs": atopo.num_far_pairs, "far_pairs_per_gear": [int(c) for c in gear_pairs],
                        "near_leaf_pairs": atopo.num_near_pairs, "near_interactions": near_inter,
@@ -866,7 +901,9 @@ def main() -> None:
             "plain_near_interactions": topo.near_pair_interactions(),
             "l2": "flushed (256 MiB write) between timed steps",
             "parallelism": f"target-leaf ranges over {world} rank(s)",
-            "timing": "CUDA events per step on the launching stream; max over ranks",
+            "timing": ("CUDA events around each step on the launching stream (the chosen and plain steps "
+                       "replayed as CUDA graphs; `eager` and the stage times from the same steps launched one "
+                       "kernel at a time); max over ranks"),
         })
         line = {
             "metric": METRIC, "value": n / (ms_chosen / 1e3), "unit": "particles/s", "n_gpus": world,

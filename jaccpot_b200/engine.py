@@ -492,6 +492,37 @@ class Pass:
         self.downward(stream)
         return self.evaluate(stream)
 
+    def capture(self, positions: torch.Tensor, masses: torch.Tensor, acc: torch.Tensor,
+                potential: torch.Tensor | None = None, warmup: int = 2) -> torch.cuda.CUDAGraph:
+        """A CUDA graph of the whole step on this pass's topology: gather of
+        `positions` (N,3) / `masses` (N,) into Morton order, the pass, and the
+        un-permute into `acc` (N,3) (and `potential` (N,), evaluated then).
+        Replaying it (``graph.replay()``, on the current stream) re-evaluates
+        the pass on whatever those buffers hold at that moment: the graph
+        fixes their addresses, so later inputs are copied into them.  The
+        launches are this object's (the same kernels, order and arguments as
+        the eager calls), so a replay gives the eager step's bits; the workspace
+        is shared with eager use of the same pass."""
+        pot = potential is not None
+
+        def step():
+            self.load_particles(positions, masses)
+            self.upward()
+            self.downward()
+            self.evaluate(potential=pot)
+            self.unsort(acc, potential)
+
+        side = torch.cuda.Stream(device=self.dt.device)
+        side.wait_stream(torch.cuda.current_stream(self.dt.device))
+        with torch.cuda.stream(side):  # the first launches of each kind, outside the capture
+            for _ in range(max(1, int(warmup))):
+                step()
+        torch.cuda.current_stream(self.dt.device).wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            step()
+        return graph
+
     # -- adjoint --------------------------------------------------------------
     def _adj_buffers(self):
         if getattr(self, "_adj", None) is None:

@@ -71,7 +71,8 @@ _GEOMETRY_MODES = ("com", "exact", "tree", "tree_approx", "runtime")
 # Options of this implementation that the reference's constructor does not
 # have; they are taken from ``advanced`` (a dict or an object with these
 # attributes) or as extra keywords, like the reference's legacy keywords.
-_EXTENSIONS = {"device": "cuda", "nearfield_compensated": False, "gear_model": None, "error_monitor": None}
+_EXTENSIONS = {"device": "cuda", "nearfield_compensated": False, "gear_model": None, "error_monitor": None,
+               "cuda_graph": False}
 
 
 def _monitor_config(cfg) -> Optional[dict]:
@@ -223,6 +224,9 @@ class FastMultipoleMethod:
                           "adaptive_prepares": 0, "force_scale_prepasses": 0, "force_scale_reused": 0}
         # sampled FP64 direct-sum checks of whole-pass evaluations (off by default)
         self.error_monitor = _monitor_config(ext["error_monitor"])
+        # whole re-evaluations (differentiable_accelerations without gradients)
+        # replay a CUDA graph captured once per prepared state
+        self.cuda_graph = bool(ext["cuda_graph"])
         self.error_history: list = []
         self._monitor_calls = 0
 
@@ -492,6 +496,8 @@ class FastMultipoleMethod:
         host = not (isinstance(positions, torch.Tensor) and positions.is_cuda)
         pos = _to_torch(positions, dev, torch.float32) if not isinstance(positions, torch.Tensor) else positions
         mass = _to_torch(masses, dev, torch.float32) if not isinstance(masses, torch.Tensor) else masses
+        if self.cuda_graph:
+            return self._replay(state, pos, mass, host, out)
         if host:
             if state.scratch.get("pos") is None:
                 state.scratch["pos"] = torch.empty((state.num_particles, 3), device=dev, dtype=torch.float32)
@@ -723,6 +729,34 @@ class FastMultipoleMethod:
         if history is not None and as_np:
             history = history.cpu().numpy()
         return out, (st if return_prepared_state else None), history
+
+    def _replay(self, state: FMMPreparedState, pos, mass, host: bool, out):
+        """differentiable_accelerations' whole re-evaluation through a CUDA
+        graph of the step (Pass.capture), captured on the state's first call
+        into fixed device buffers that later inputs are copied into."""
+        sc = state.scratch
+        if sc.get("graph") is None:
+            dev = state.device_topology.device
+            n = state.num_particles
+            sc["g_pos"] = torch.empty((n, 3), device=dev, dtype=torch.float32)
+            sc["g_mass"] = torch.empty((n,), device=dev, dtype=torch.float32)
+            sc["g_acc"] = torch.empty((n, 3), device=dev, dtype=torch.float32)
+            sc["g_pos"].copy_(pos)
+            sc["g_mass"].copy_(mass)
+            sc["graph"] = state.pass_.capture(sc["g_pos"], sc["g_mass"], sc["g_acc"])
+            self._counters["graph_captures"] = self._counters.get("graph_captures", 0) + 1
+        sc["g_pos"].copy_(pos, non_blocking=True)
+        sc["g_mass"].copy_(mass, non_blocking=True)
+        sc["graph"].replay()
+        self._counters["graph_replays"] = self._counters.get("graph_replays", 0) + 1
+        self._monitor_check(state)
+        acc = sc["g_acc"]
+        if not host:
+            return acc.clone()
+        if out is None:
+            return acc.cpu()
+        out.copy_(acc, non_blocking=True)
+        return out
 
     # ------------------------------------------------------------ error monitor
     def _monitor_check(self, state: FMMPreparedState) -> None:
