@@ -471,6 +471,107 @@ def measure_gear_selector(dev, stream, n: int = 2097152, seed: int = 200, theta:
 
 
 # ---------------------------------------------------------------------------
+SWEEP_PLAIN_THETAS = (0.5, 0.55, 0.5875, 0.6, 0.65, 0.7)
+SWEEP_ADAPTIVE = (((8,), (1e-5, 2e-5, 3e-5, 5e-5)),
+                  ((2, 4, 6, 8), (1e-5, 2e-5, 3e-5, 3.24e-5, 4e-5, 5e-5, 8e-5)),
+                  ((2, 4, 6, 8, 10), (3e-5, 5e-5, 8e-5, 1.2e-4)))
+
+
+def run_sweep(args) -> None:
+    """The accuracy / time frontier of both acceptance rules at the headline
+    workload: the plain theta walk at order 8 over SWEEP_PLAIN_THETAS, and the
+    error-controlled walk over eps for each gear set of SWEEP_ADAPTIVE.  One
+    JSON line per point: far pairs, near interactions, stage times (CUDA
+    events, L2 flushed before each step), the step as a CUDA graph, and the
+    errors against an FP64 direct sum on ERR_TARGETS random targets."""
+    import torch
+
+    from jaccpot_b200 import _lib, engine, tree, workloads
+    from jaccpot_b200.solver import FastMultipoleMethod
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cfg = dict(WORKLOAD)
+    n = cfg["N"] = args.n
+    pos, mass = workloads.GENERATORS[cfg["generator"]](n, cfg["seed"])
+    d_pos, d_mass = torch.from_numpy(pos).to(dev), torch.from_numpy(mass).to(dev)
+    stream = torch.cuda.current_stream()
+    tg = np.random.default_rng(54321).choice(n, size=min(ERR_TARGETS, n), replace=False)
+    base_topo = tree.build_topology(pos, mass, leaf_size=cfg["leaf_size"], theta=0.6, device=dev)
+    base = engine.Pass(engine.DeviceTopology(base_topo, dev), 1)
+    base.load_particles(d_pos, d_mass)
+    ts = torch.from_numpy(base_topo.inverse_permutation[tg].astype(np.int32)).to(dev)
+    ref = torch.empty((tg.size, 4), device=dev, dtype=torch.float64)
+    _lib.check(_lib.lib().jb_direct_f64(n, base.ws.pos4.data_ptr(), tg.size, ts.data_ptr(), 1.0, 0.0,
+                                        ref.data_ptr(), stream.cuda_stream), "jb_direct_f64")
+    ref = ref[:, :3].cpu().numpy()
+    del base
+    acc_out = torch.empty((n, 3), device=dev, dtype=torch.float32)
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
+
+    def measure(ps, topo, point):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        stage = np.zeros(5)
+        for k in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            ev[0].record(stream)
+            ps.load_particles(d_pos, d_mass)
+            ps.upward()
+            ev[1].record(stream)
+            ps.m2l()
+            ev[2].record(stream)
+            ps.l2l()
+            ev[3].record(stream)
+            acc = ps.evaluate()
+            ev[4].record(stream)
+            ps.unsort(acc_out, None)
+            ev[5].record(stream)
+            torch.cuda.synchronize()
+            if k >= args.warmup:
+                stage += [ev[i].elapsed_time(ev[i + 1]) for i in range(5)]
+        stage /= args.steps
+        g = ps.capture(d_pos, d_mass, acc_out)
+        per = []
+        for k in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.replay()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if k >= args.warmup:
+                per.append(e0.elapsed_time(e1))
+        del g
+        ps.run()
+        idx = torch.from_numpy(topo.inverse_permutation[tg].astype(np.int64)).to(dev)
+        got = ps.evaluate()[idx, :3].double().cpu().numpy()
+        e = workloads.relative_errors(got, ref)
+        point.update({"far_pairs": int(topo.num_far_pairs), "near_interactions": int(topo.near_pair_interactions()),
+                      "stage_ms": dict(zip(("upward", "m2l", "l2l", "leaf_eval", "unsort"),
+                                           [round(float(x), 4) for x in stage])),
+                      "graph_ms": round(float(np.mean(per)), 4), "p99": float(np.percentile(e, 99)),
+                      "p50": float(np.median(e)), "meets_1e-4": bool(np.percentile(e, 99) <= ERR_BOUND)})
+        print(json.dumps(point), flush=True)
+
+    for th in SWEEP_PLAIN_THETAS:
+        topo = tree.build_topology(pos, mass, leaf_size=cfg["leaf_size"], theta=th, device=dev)
+        ps = engine.Pass(engine.DeviceTopology(topo, dev), cfg["order"], G=1.0, eps2=0.0)
+        measure(ps, topo, {"form": "plain", "theta": th, "order": cfg["order"]})
+        del ps
+    for gears, eps_list in SWEEP_ADAPTIVE:
+        for eps in eps_list:
+            fmm = FastMultipoleMethod(theta=0.6, G=1.0, softening=0.0, adaptive_order=True, p_gears=gears,
+                                      adaptive_error_model="dehnen_paper", adaptive_eps=eps,
+                                      mac_force_scale_mode="paper", device=dev,
+                                      advanced={"nearfield_compensated": True})
+            st = fmm.prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=max(gears))
+            per_gear = np.bincount(st.topology.far_gears, minlength=len(gears)) if st.topology.num_far_pairs else []
+            measure(st.pass_, st.topology, {"form": "error-controlled", "gears": list(gears), "eps": eps,
+                                            "far_pairs_per_gear": [int(c) for c in per_gear]})
+            del st, fmm
+    torch.cuda.synchronize()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -483,11 +584,16 @@ def main() -> None:
     ap.add_argument("--profile", choices=["chosen", "plain", "split_bf16", "learned_gears"], default=None,
                     help="after the warm-up, run one step of this form between cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off)")
+    ap.add_argument("--sweep", action="store_true",
+                    help="instead of the bench line: the theta / eps x gear-set accuracy-time table (one GPU)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.sweep:
+        run_sweep(args)
         return
 
     import torch
