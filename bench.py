@@ -74,9 +74,11 @@ ERR_BOUND = 1e-4
 # a disjoint sample of the same size.
 SELECT_BOUND = 0.9 * ERR_BOUND
 THETA_GRID = (0.6, 0.59, 0.58, 0.57, 0.56, 0.55, 0.53, 0.5)
-EPS_GRID = (5e-5, 4e-5, 3.5e-5, 3e-5, 2.5e-5, 2e-5, 1.5e-5, 1e-5)
+EPS_GRID = (6e-5, 5e-5, 4e-5, 3.5e-5, 3e-5, 2.5e-5, 2e-5, 1.5e-5, 1e-5)
 EPS_REFINE = 2
 GEARS = (2, 4, 6, 8)
+# the chosen form's candidate gear sets: order 8 alone, or the gear ladder
+GEAR_SETS = ((8,), GEARS)
 
 
 def m2l_flops_per_pair(p: int) -> float:
@@ -678,39 +680,74 @@ def main() -> None:
             failed_theta = mid
     cfg["theta"] = plain_theta
 
-    # chosen: the error-controlled walk (Dehnen eq. 15/16a acceptance, per-pair
-    # gears GEARS) + FP32 M2L + Kahan-compensated P2P, through the public API
-    # (adaptive_error_model="dehnen_paper"); eps = the largest of EPS_GRID that
-    # meets the bound on the selection sample
-    def chosen_solver(eps, graph=False):
-        return FastMultipoleMethod(theta=0.6, G=1.0, softening=0.0, adaptive_order=True, p_gears=GEARS,
+    # chosen: the error-controlled walk (Dehnen eq. 15/16a acceptance) + FP32
+    # M2L + Kahan-compensated P2P, through the public API
+    # (adaptive_error_model="dehnen_paper").  For each gear set of GEAR_SETS,
+    # eps = the largest of EPS_GRID that meets the bound on the selection
+    # sample (refined as the plain form's theta); the gear set whose step is
+    # faster at its eps is the chosen form.
+    def chosen_solver(eps, gears, graph=False):
+        return FastMultipoleMethod(theta=0.6, G=1.0, softening=0.0, adaptive_order=True, p_gears=gears,
                                    adaptive_error_model="dehnen_paper", adaptive_eps=eps,
                                    mac_force_scale_mode="paper", device=dev,
                                    advanced={"nearfield_compensated": True, "cuda_graph": graph})
 
-    def try_eps(eps) -> bool:
-        st_e = chosen_solver(eps).prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
+    def try_eps(eps, gears) -> bool:
+        st_e = chosen_solver(eps, gears).prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
         e = errors_of(st_e.pass_.evaluate(), st_e.topology, tg_sel, ref_sel)
-        sel["chosen"].append({"eps": eps, "p99": e["p99"], "p99_first_4096": e["p99_first_4096"]})
+        sel["chosen"].append({"gears": list(gears), "eps": eps, "p99": e["p99"],
+                              "p99_first_4096": e["p99_first_4096"]})
         del st_e
         return meets(e)
 
-    chosen_eps, failed_eps = EPS_GRID[-1], None
-    for eps in EPS_GRID:
-        if try_eps(eps):
-            chosen_eps = eps
-            break
-        failed_eps = eps
-    # then EPS_REFINE log-space bisection steps between the passing eps and
-    # the failing grid value above it
-    for _ in range(EPS_REFINE if failed_eps is not None else 0):
-        mid = float(np.sqrt(chosen_eps * failed_eps))
-        if try_eps(mid):
-            chosen_eps = mid
-        else:
-            failed_eps = mid
+    def select_eps(gears) -> float:
+        good, failed = EPS_GRID[-1], None
+        for eps in EPS_GRID:
+            if try_eps(eps, gears):
+                good = eps
+                break
+            failed = eps
+        # then EPS_REFINE log-space bisection steps between the passing eps and
+        # the failing grid value above it
+        for _ in range(EPS_REFINE if failed is not None else 0):
+            mid = float(np.sqrt(good * failed))
+            if try_eps(mid, gears):
+                good = mid
+            else:
+                failed = mid
+        return good
 
-    fmm = chosen_solver(chosen_eps, graph=True)  # the public API's deployed path: a CUDA graph of the step
+    def step_ms(eps, gears) -> float:  # the step as a CUDA graph, L2 flushed, median of 5
+        st_e = chosen_solver(eps, gears).prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
+        out = torch.empty((n, 3), device=dev, dtype=torch.float32)
+        g = st_e.pass_.capture(d_pos, d_mass, out)
+        fl = torch.empty(256 * 1024 * 1024 // 4, device=dev, dtype=torch.float32)
+        per = []
+        for k in range(8):
+            fl.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.replay()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if k >= 3:
+                per.append(e0.elapsed_time(e1))
+        del g, st_e, fl
+        return float(np.median(per))
+
+    gear_choice = []
+    for gs in GEAR_SETS:
+        eps_g = select_eps(gs)
+        gear_choice.append({"gears": list(gs), "eps": eps_g, "step_ms": step_ms(eps_g, gs)})
+    best = min(gear_choice, key=lambda c: c["step_ms"])
+    if world > 1:  # every rank takes rank 0's choice (timings differ slightly between ranks)
+        pick = torch.tensor([gear_choice.index(best)], device=dev)
+        dist.broadcast(pick, 0)
+        best = gear_choice[int(pick.item())]
+    gears, chosen_eps = tuple(best["gears"]), best["eps"]
+    sel["gear_sets"] = gear_choice
+
+    fmm = chosen_solver(chosen_eps, gears, graph=True)  # the public API's deployed path: a CUDA graph of the step
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     state = fmm.prepare_state(pos, mass, leaf_size=cfg["leaf_size"], max_order=cfg["order"])
@@ -735,7 +772,7 @@ def main() -> None:
         passes["chosen"] = engine.Pass(state.device_topology, cfg["order"], G=1.0, eps2=0.0,
                                        p2p_mode=_lib.JB_P2P_KAHAN,
                                        leaf_range=((La * rank) // world, (La * (rank + 1)) // world))
-        passes["chosen"].set_gears(torch.from_numpy(atopo.far_gears).to(dev), GEARS)
+        passes["chosen"].set_gears(torch.from_numpy(atopo.far_gears).to(dev), gears)
     else:
         passes["chosen"] = state.pass_
     # the learned selector (MLP gears on the theta walk), reported beside:
@@ -898,8 +935,8 @@ def main() -> None:
     peaks = _peaks()
     near_inter = atopo.near_pair_interactions()
     p2p_flops = 20.0 * near_inter
-    gear_pairs = np.bincount(atopo.far_gears, minlength=len(GEARS)) if atopo.num_far_pairs else np.zeros(len(GEARS))
-    m2l_flops = float(sum(int(c) * m2l_flops_per_pair(o) for c, o in zip(gear_pairs, GEARS)))
+    gear_pairs = np.bincount(atopo.far_gears, minlength=len(gears)) if atopo.num_far_pairs else np.zeros(len(gears))
+    m2l_flops = float(sum(int(c) * m2l_flops_per_pair(o) for c, o in zip(gear_pairs, gears)))
     m2l_flops_plain = m2l_flops_per_pair(cfg["order"]) * topo.num_far_pairs
     # measured FP32 FMA peak (in-run probe, 148 SMs x 8 blocks x 256 thr)
     sink = torch.empty(256, device=dev)
@@ -968,7 +1005,7 @@ def main() -> None:
     if rank == 0:
         cfg.update({
             "form": (f"chosen = error-controlled walk (Dehnen eq. 15/16a acceptance, eps={chosen_eps:g}, "
-                     f"per-pair gears {GEARS}) + FP32 rotate+scale M2L + Kahan-compensated P2P; plain = theta walk "
+                     f"per-pair gears {gears}, chosen in the run from {GEAR_SETS}) + FP32 rotate+scale M2L + Kahan-compensated P2P; plain = theta walk "
                      f"(theta={plain_theta:g}) + FP32 M2L + FP32 P2P at the maximum order p={cfg['order']}; "
                      "split_bf16 = plain's lists with the tcgen05 split-BF16 M2L + Kahan P2P; learned_gears = "
                      "plain's lists with the MLP-selected gears + Kahan P2P"),
@@ -978,7 +1015,7 @@ def main() -> None:
                       "chosen_vs_plain": ms["plain"] / ms["chosen"],
                       "note": "the same steps launched one kernel at a time with an event between stages "
                               "(stage_ms_* come from these runs)"},
-            "chosen": {"eps": chosen_eps, "gears": list(GEARS), "theta_max": 1.0, "theta_prepass": 0.6,
+            "chosen": {"eps": chosen_eps, "gears": list(gears), "theta_max": 1.0, "theta_prepass": 0.6,
                        "far_pairs": atopo.num_far_pairs, "far_pairs_per_gear": [int(c) for c in gear_pairs],
                        "near_leaf_pairs": atopo.num_near_pairs, "near_interactions": near_inter,
                        "m2l_algorithmic_flop": m2l_flops},
