@@ -772,7 +772,8 @@ def main() -> None:
         passes["chosen"] = engine.Pass(state.device_topology, cfg["order"], G=1.0, eps2=0.0,
                                        p2p_mode=_lib.JB_P2P_KAHAN,
                                        leaf_range=((La * rank) // world, (La * (rank + 1)) // world))
-        passes["chosen"].set_gears(torch.from_numpy(atopo.far_gears).to(dev), gears)
+        if len(gears) > 1:  # as the facade: a single order runs the plain units
+            passes["chosen"].set_gears(torch.from_numpy(atopo.far_gears).to(dev), gears)
     else:
         passes["chosen"] = state.pass_
     # the learned selector (MLP gears on the theta walk), reported beside:

@@ -245,6 +245,16 @@ JB_API int jb_set_level_split(int m2m_max_parents, int l2l_max_parents);
  * Process-wide setting.                                                   */
 JB_API int jb_set_leaf_form(int chunk_major);
 
+/* Source-row fetch of the single-order FP32 M2L (jb_m2l, jb_m2l_gears,
+ * jb_m2l_weighted, jb_adj_m2l; jb_m2l_mixed always fetches per thread):
+ * 1 (default) copies the rows of a warp's 32
+ * work units together, one cp.async instruction per row (lane k takes
+ * 16-byte word k); 0 lets each thread copy its own row word by word (every
+ * warp instruction then touches 32 rows).  The same arithmetic either way;
+ * the compiler may fuse a multiply and an add differently in the two
+ * kernels, so results agree to FP32 rounding.  Process-wide setting.       */
+JB_API int jb_set_m2l_fetch(int warp_rows);
+
 /* Row stride (floats) of a coefficient array of order p: (p+1)^2 rounded up
  * to a multiple of 4.  Returns 0 for an unsupported order. */
 JB_API int jb_coeff_stride(int p);

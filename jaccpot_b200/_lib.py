@@ -95,6 +95,7 @@ _SIGNATURES = {
     "jb_node_force_scale": [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P],
     "jb_set_level_split": [_I, _I],
     "jb_set_leaf_form": [_I],
+    "jb_set_m2l_fetch": [_I],
     "jb_far_reverse_index": [_I, _P, _P, _P, _P],
     "jb_m2l_weighted": [_I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_leaf_eval_weighted": [_I, _I, _P, _P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _I, _P, _P],

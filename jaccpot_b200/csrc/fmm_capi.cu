@@ -15,6 +15,7 @@ namespace jb {
 static thread_local char g_err[256] = {0};
 int g_split_max_parents[2] = {1 << 30, 2048};  // measured at clustered N=4M, p=8
 int g_leaf_flat = 1;
+int g_m2l_coop = 1;
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return JB_OK;
@@ -421,6 +422,12 @@ JB_API int jb_set_level_split(int m2m_max_parents, int l2l_max_parents) {
 JB_API int jb_set_leaf_form(int chunk_major) {
   if (chunk_major != 0 && chunk_major != 1) return JB_ERR_ARG;
   jb::g_leaf_flat = chunk_major;
+  return JB_OK;
+}
+
+JB_API int jb_set_m2l_fetch(int warp_rows) {
+  if (warp_rows != 0 && warp_rows != 1) return JB_ERR_ARG;
+  jb::g_m2l_coop = warp_rows;
   return JB_OK;
 }
 

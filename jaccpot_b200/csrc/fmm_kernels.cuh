@@ -38,6 +38,9 @@ extern int g_split_max_parents[2];
 // Nonzero: leaves of more than 16 particles take the chunk-major near-field
 // form (k_leaf_units_flat) in jb_leaf_eval (jb_set_leaf_form).
 extern int g_leaf_flat;
+// Nonzero: the single-order FP32 M2L fetches source rows with the whole warp
+// (k_m2l_units_coop) rather than thread by thread (jb_set_m2l_fetch).
+extern int g_m2l_coop;
 inline int launch_status() { return cuda_status(cudaGetLastError()); }
 
 // Most particles a leaf may hold: the near-field kernels give each target of
@@ -287,6 +290,112 @@ __global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units(int num_units, con
     cs1 = centers[s2];
     s1 = s2;
   }
+  float* dst = (slot < 0) ? locals + (size_t)tgt * rs : partials + (size_t)slot * rs;
+#pragma unroll
+  for (int k = 0; k < C; ++k) dst[k] = acc[k];
+  for (int k = C; k < rs; ++k) dst[k] = 0.f;
+}
+
+// The warp's next source rows, fetched together: lane j's row s_j (-1: none)
+// goes to wrows + j * R4, one cp.async instruction per row, lane k copying
+// 16-byte word k (k < NW); one cp.async group.  ids: the warp's 32 ints of
+// shared memory.  The caller has made sure every lane is done with its row
+// and with the previous ids (a __syncwarp after the last read).
+template <int NW, int R4>
+__device__ __forceinline__ void warp_rows_fetch(float4* wrows, int* ids, int lane, int s, const float* mult, int rs) {
+  ids[lane] = s;
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int4 sq = reinterpret_cast<const int4*>(ids)[q];
+    const int sj[4] = {sq.x, sq.y, sq.z, sq.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (sj[i] >= 0 && lane < NW)
+        cp_async16(wrows + (4 * q + i) * R4 + lane, reinterpret_cast<const float4*>(mult + (size_t)sj[i] * rs) + lane);
+  }
+  cp_async_commit();
+}
+
+// k_m2l_units with each source row fetched by the whole warp: per pair the
+// lanes publish their next source ids, and for each of the warp's 32 rows one
+// cp.async instruction copies it, lane k taking 16-byte word k.  A row is then
+// 2-3 cache lines for one instruction, where a thread copying its own row
+// issues one instruction per word with all 32 lanes on different lines (32
+// L1 wavefronts each).  The lanes step through their units together (units
+// are sorted longest first, so a warp's lengths are close); a lane past its
+// unit's end only takes part in the copies.  The same arithmetic as
+// k_m2l_units (the compiler may fuse a multiply and an add differently in the
+// two kernels: the sums agree to FP32 rounding).  At the headline workload
+// this fetch takes the M2L from 2.96 to 2.68 ms (order 8).  The mixed-order
+// kernel keeps the per-thread fetch: there the lanes' segment lengths differ
+// more, and stepping them together measured slower (5.88 -> 5.94 ms).
+template <int P, bool NEG, bool W = false>
+__global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units_coop(int num_units, const int4* __restrict__ units,
+                                                                   const float* __restrict__ mult,
+                                                                   const float4* __restrict__ centers,
+                                                                   const int* __restrict__ far_src,
+                                                                   float* __restrict__ locals,
+                                                                   float* __restrict__ partials, int rs,
+                                                                   const float* __restrict__ far_w = nullptr) {
+  constexpr int C = csize(P), CS = cstride(P), R4 = row4(P), NW = CS / 4;
+  static_assert(NW <= 32, "one warp instruction copies a row");
+  extern __shared__ float4 m2l_smem[];
+  const int lane = threadIdx.x & 31;
+  float4* wrows = m2l_smem + (threadIdx.x & ~31) * R4;  // the warp's 32 rows
+  float4* row = wrows + lane * R4;
+  int* ids = reinterpret_cast<int*>(m2l_smem + kM2LThreads * R4) + (threadIdx.x & ~31);
+  const int u = blockIdx.x * kM2LThreads + threadIdx.x;
+  const bool ok = u < num_units;
+  const int4 U = ok ? units[u] : make_int4(0, 0, 0, -1);
+  const int tgt = U.x, e0 = U.y, slot = U.w;
+  const int n = ok ? U.z - U.y : 0;
+  const int nmax = __reduce_max_sync(0xffffffffu, n);
+  auto fetch = [&](int s) { warp_rows_fetch<NW, R4>(wrows, ids, lane, s, mult, rs); };
+  float acc[C];
+#pragma unroll
+  for (int k = 0; k < C; ++k) acc[k] = 0.f;
+  const float4 ct = ok ? centers[tgt] : make_float4(0.f, 0.f, 0.f, 0.f);
+  int s0 = -1, s1 = -1;
+  float4 cs = ct, cs1 = ct;
+  if (n > 0) {
+    s0 = far_src[e0];
+    s1 = (n > 1) ? far_src[e0 + 1] : s0;
+    cs = centers[s0];
+    cs1 = centers[s1];
+  }
+  fetch(s0);
+  for (int it = 0; it < nmax; ++it) {
+    const bool act = it < n;
+    float v[C];
+    cp_async_wait_all();
+    __syncwarp();  // the copies every lane issued into the warp's rows have landed
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < CS / 4; ++k) {
+        const float4 q = row[k];
+        if (4 * k + 0 < C) v[4 * k + 0] = q.x;
+        if (4 * k + 1 < C) v[4 * k + 1] = q.y;
+        if (4 * k + 2 < C) v[4 * k + 2] = q.z;
+        if (4 * k + 3 < C) v[4 * k + 3] = q.w;
+      }
+    }
+    __syncwarp();  // every row (and every id) read before the next copies
+    fetch(act && it + 1 < n ? s1 : -1);
+    if (act) {
+      const int e = e0 + it;
+      const int s2 = (it + 2 < n) ? __ldg(far_src + e + 2) : s1;
+      const float dx = NEG ? cs.x - ct.x : ct.x - cs.x;
+      const float dy = NEG ? cs.y - ct.y : ct.y - cs.y;
+      const float dz = NEG ? cs.z - ct.z : ct.z - cs.z;
+      m2l_kfold_acc<P, W>(v, acc, dx, dy, dz, W ? __ldg(far_w + e) : 1.f);
+      cs = cs1;
+      cs1 = centers[s2];
+      s1 = s2;
+    }
+  }
+  cp_async_wait_all();  // nothing in flight (the last fetch copies nothing)
+  if (!ok) return;
   float* dst = (slot < 0) ? locals + (size_t)tgt * rs : partials + (size_t)slot * rs;
 #pragma unroll
   for (int k = 0; k < C; ++k) dst[k] = acc[k];
@@ -1404,8 +1513,11 @@ struct RunM2L {
                  int rs = 0, const float* far_w = nullptr) {
     if (rs <= 0) rs = cstride(P);
     if (num_units > 0) {
-      const size_t sm = sizeof(float4) * kM2LThreads * row4(P);
-      auto kern = far_w ? k_m2l_units<P, false, true> : (neg ? k_m2l_units<P, true> : k_m2l_units<P, false>);
+      const bool coop = g_m2l_coop != 0;
+      const size_t sm = sizeof(float4) * kM2LThreads * row4(P) + (coop ? sizeof(int) * kM2LThreads : 0);
+      auto kern = coop ? (far_w ? k_m2l_units_coop<P, false, true>
+                                : (neg ? k_m2l_units_coop<P, true> : k_m2l_units_coop<P, false>))
+                       : (far_w ? k_m2l_units<P, false, true> : (neg ? k_m2l_units<P, true> : k_m2l_units<P, false>));
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
           num_units, reinterpret_cast<const int4*>(units), mult, reinterpret_cast<const float4*>(centers), far_src,
