@@ -159,7 +159,8 @@ def _peaks() -> dict:
 # DRAM bytes (read + write) per launch of the dominant kernels at the bench
 # workload, scaled from single-launch ncu captures of a 1M-particle case by
 # the units processed (far pairs / particle pairs); see profiles/.
-TRAFFIC_PER_UNIT = {"k_m2l_units": 7.8, "k_m2l_mixed": 10.7, "k_m2l_tc_units": 12.3, "k_leaf_units_flat": 0.0124}
+TRAFFIC_PER_UNIT = {"k_m2l_units": 7.8, "k_m2l_units_coop": 8.9, "k_m2l_mixed": 10.7, "k_m2l_tc_units": 12.3,
+                    "k_leaf_units_flat": 0.0124}
 
 
 def _traffic(kernel: str, units: float | None = None):
@@ -970,9 +971,10 @@ def main() -> None:
                 "traffic": _traffic("k_m2l_tc_units", atopo.num_far_pairs), "fp32_pipe_frac": ach / fp32_peak}
     elif stage_names[dom] == "m2l":
         ach = m2l_flops / (stage_chosen[1] / 1e3) / 1e12
-        roof = {"kernel": "k_m2l_units<2,4,6,8> (one launch per gear)", "bound": "fp32", "achieved": ach,
+        kname = "k_m2l_units_coop" if len(gears) == 1 else "k_m2l_mixed"
+        roof = {"kernel": f"{kname}<{cfg['order']}>", "bound": "fp32", "achieved": ach,
                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
-                "traffic": _traffic("k_m2l_units", atopo.num_far_pairs)}
+                "traffic": _traffic(kname, atopo.num_far_pairs)}
     else:
         ach = p2p_flops / (stage_chosen[3] / 1e3) / 1e12
         pairs_per_s = near_inter / (stage_chosen[3] / 1e3)
@@ -1019,7 +1021,10 @@ def main() -> None:
             "chosen": {"eps": chosen_eps, "gears": list(gears), "theta_max": 1.0, "theta_prepass": 0.6,
                        "far_pairs": atopo.num_far_pairs, "far_pairs_per_gear": [int(c) for c in gear_pairs],
                        "near_leaf_pairs": atopo.num_near_pairs, "near_interactions": near_inter,
-                       "m2l_algorithmic_flop": m2l_flops},
+                       "m2l_algorithmic_flop": m2l_flops,
+                       "m2l_kernel": "k_m2l_units_coop" if len(gears) == 1 else "k_m2l_mixed",
+                       "m2l_tflops": m2l_flops / (stage_chosen[1] / 1e3) / 1e12,
+                       "m2l_frac_of_fp32_probe": m2l_flops / (stage_chosen[1] / 1e3) / 1e12 / fp32_peak},
             "learned_gears": None if learned_err is None else {
                 "ms_per_step": ms["learned_gears"], "particles_per_s": n / (ms["learned_gears"] / 1e3),
                 "stage_ms": dict(zip(stage_names, [float(x) for x in timings["learned_gears"][1]])),
