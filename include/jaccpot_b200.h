@@ -457,6 +457,14 @@ JB_API int jb_eval_targets(int p, const float* pos4, int num_internal, const int
 JB_API int jb_scatter_unsorted(int64_t n, const float* acc4, const int64_t* perm, float* out_acc,
                                float* out_pot, void* stream);
 
+/* The same un-permute from the inverse permutation (inv_perm[perm[i]] = i):
+ * out_acc[j] = acc4[inv_perm[j]].xyz, out_pot (optional) likewise.  The
+ * output is written in order (coalesced) and only the reads scatter: 0.043
+ * against 0.113 ms at N = 4M.  The values are the same
+ * (runtime/fmm_evaluate.py:526-538).                                      */
+JB_API int jb_gather_unsorted(int64_t n, const float* acc4, const int64_t* inv_perm, float* out_acc,
+                              float* out_pot, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Adjoint (vector-Jacobian product) at fixed topology.                     */
 /*                                                                          */

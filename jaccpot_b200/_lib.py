@@ -138,6 +138,7 @@ _SIGNATURES = {
     "jb_gear_adam": [_I, _P, _F, _F, _F, _F, _F, _I, _P, _P, _P, _P, _P],
     "jb_gear_select": [_I64, _P, _P, _P, _P, _P, _P, _F, _P, _P, _F, _F, _P, _P],
     "jb_scatter_unsorted": [_I64, _P, _P, _P, _P, _P],
+    "jb_gather_unsorted": [_I64, _P, _P, _P, _P, _P],
     "jb_direct_f64": [_I64, _P, _I64, _P, _D, _D, _P, _P],
     "jb_probe_throughput": [_I, _I, _I, _P, _P],
 }

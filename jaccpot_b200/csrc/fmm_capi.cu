@@ -60,6 +60,20 @@ __global__ void k_scatter_unsorted(int64_t n, const float4* __restrict__ acc4, c
   if (out_pot) out_pot[o] = a.w;
 }
 
+// The same un-permute as a gather: out[j] = acc4[inv_perm[j]], so the 12-byte
+// output rows are written in order (coalesced) and only the 16-byte reads
+// scatter; the scatter form writes each row into a different place.
+__global__ void k_gather_unsorted(int64_t n, const float4* __restrict__ acc4, const int64_t* __restrict__ inv_perm,
+                                  float* __restrict__ out_acc, float* __restrict__ out_pot) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const float4 a = acc4[inv_perm[j]];
+  out_acc[3 * j] = a.x;
+  out_acc[3 * j + 1] = a.y;
+  out_acc[3 * j + 2] = a.z;
+  if (out_pot) out_pot[j] = a.w;
+}
+
 // ---------------------------------------------------------------------------
 // List validation (prepare time).
 // ---------------------------------------------------------------------------
@@ -449,6 +463,15 @@ JB_API int jb_scatter_unsorted(int64_t n, const float* acc4, const int64_t* perm
   if (n == 0) return JB_OK;
   k_scatter_unsorted<<<blocks_1d(n, 256), 256, 0, ST(stream)>>>(n, reinterpret_cast<const float4*>(acc4), perm,
                                                                   out_acc, out_pot);
+  return launch_status();
+}
+
+JB_API int jb_gather_unsorted(int64_t n, const float* acc4, const int64_t* inv_perm, float* out_acc, float* out_pot,
+                              void* stream) {
+  if (n < 0 || (n > 0 && (!acc4 || !inv_perm || !out_acc))) return JB_ERR_ARG;
+  if (n == 0) return JB_OK;
+  k_gather_unsorted<<<blocks_1d(n, 256), 256, 0, ST(stream)>>>(n, reinterpret_cast<const float4*>(acc4), inv_perm,
+                                                                 out_acc, out_pot);
   return launch_status();
 }
 

@@ -55,6 +55,7 @@ class DeviceTopology:
         self.near_src = up(topo.near_leaves if topo.num_near_pairs else np.zeros(1, np.int32), torch.int32)
         self.leaf_of = up(topo.leaf_of_particle, torch.int32)
         self.perm = up(topo.permutation, torch.int64)
+        self.inv_perm = up(topo.inverse_permutation, torch.int64)
         self.m2l_targets = up(topo.m2l_targets if topo.m2l_targets.size else np.zeros(1, np.int32), torch.int32)
         self.num_m2l_targets = int(topo.m2l_targets.size)
         self.level_offsets = [int(x) for x in topo.level_offsets]
@@ -479,8 +480,8 @@ class Pass:
 
     def unsort(self, acc: torch.Tensor, pot: torch.Tensor | None, stream=None) -> None:
         n = self.dt.topo.num_particles
-        _lib.check(self.lib.jb_scatter_unsorted(n, _ptr(self.ws.acc4), _ptr(self.dt.perm), _ptr(acc),
-                                                _ptr(pot), _stream_handle(stream)), "jb_scatter_unsorted")
+        _lib.check(self.lib.jb_gather_unsorted(n, _ptr(self.ws.acc4), _ptr(self.dt.inv_perm), _ptr(acc),
+                                               _ptr(pot), _stream_handle(stream)), "jb_gather_unsorted")
 
     def downward(self, stream=None) -> None:
         self.m2l(stream)
@@ -611,8 +612,8 @@ class Pass:
         _lib.check(lb.jb_adj_p2m(self.p, _ptr(ws.pos4), t.num_nodes, t.num_internal, _ptr(dt.node_ranges),
                                  _ptr(ws.centers), _ptr(A["mbar"]), _ptr(A["cbar4"]), _ptr(A["xm4"]), s),
                    "jb_adj_p2m")
-        _lib.check(lb.jb_scatter_unsorted(t.num_particles, _ptr(A["xm4"]), _ptr(dt.perm), _ptr(grad_pos),
-                                          _ptr(grad_mass), s), "jb_scatter_unsorted(grad)")
+        _lib.check(lb.jb_gather_unsorted(t.num_particles, _ptr(A["xm4"]), _ptr(dt.inv_perm), _ptr(grad_pos),
+                                         _ptr(grad_mass), s), "jb_gather_unsorted(grad)")
 
     def launches_per_run(self) -> int:
         """This library's kernel launches in one run(): P2M, one M2M per level,

@@ -246,3 +246,29 @@ def test_errors_are_reported_not_trapped():
     assert lb.jb_m2l(s.p, 7, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0) == 8  # unknown mode
     with pytest.raises(_lib.JBError):
         _lib.coeff_stride(0)
+
+
+@pytest.mark.parametrize("with_pot", [False, True])
+def test_unsort_gather_equals_scatter(with_pot):
+    """jb_gather_unsorted (out[j] = acc4[inv_perm[j]]) moves the same values as
+    jb_scatter_unsorted (out[perm[i]] = acc4[i]), bit for bit."""
+    lb = _lib.lib()
+    n = 100_003
+    rng = np.random.default_rng(5)
+    perm = rng.permutation(n).astype(np.int64)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(n)
+    d_perm, d_inv = torch.from_numpy(perm).cuda(), torch.from_numpy(inv).cuda()
+    acc4 = torch.randn((n, 4), device="cuda")
+    outs = []
+    for fn, idx in ((lb.jb_scatter_unsorted, d_perm), (lb.jb_gather_unsorted, d_inv)):
+        a = torch.full((n, 3), float("nan"), device="cuda")
+        p = torch.full((n,), float("nan"), device="cuda")
+        _lib.check(fn(n, acc4.data_ptr(), idx.data_ptr(), a.data_ptr(), p.data_ptr() if with_pot else None,
+                      torch.cuda.current_stream().cuda_stream), "unsort")
+        outs.append((a, p))
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][0], acc4[torch.from_numpy(inv).cuda(), :3])
+    if with_pot:
+        assert torch.equal(outs[0][1], outs[1][1])
