@@ -379,6 +379,18 @@ JB_API int jb_m2l_split_units(int p, int num_units, const int* units, const floa
 JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* right,
                         const float* centers, float* locals, void* stream);
 
+/* The downward sweep straight to the leaves (the same operator, l2l_real,
+ * operators/real_translations.py:604, composed): units[u] = (leaf node,
+ * first, end, unused) over anc[], the leaf's ancestors that received far
+ * pairs (nearest first); locals[leaf] += sum_a L2L(a -> leaf)(locals[a]).
+ * Call after the M2L, on locals holding each node's own M2L sum, instead of
+ * the jb_l2l_level sweep.  Shifting a degree-p expansion is exact, so the
+ * leaves' locals equal the cascade's up to rounding; the internal nodes keep
+ * their own M2L sums (the adjoint, which reads them, uses the cascade).
+ * Device pointers; units and anc come from the caller's schedule.          */
+JB_API int jb_l2l_leaves(int p, int num_units, const int* units, const int* anc, const float* centers,
+                         float* locals, void* stream);
+
 /* Leaf evaluation over work units: L2P of each leaf's local at its particles
  * (runtime/kernels/_evaluate.py:2106-2484, evaluate_local_real_with_grad) plus
  * the near field over the self leaf and the leaf's neighbour list

@@ -119,6 +119,7 @@ _SIGNATURES = {
     "jb_m2l_mixed": [_I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_m2l_split": [_I, _I, _I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P],
     "jb_m2l_split_units": [_I, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P],
+    "jb_l2l_leaves": [_I, _I, _P, _P, _P, _P, _P],
     "jb_l2l_level": [_I, _I, _I, _P, _P, _P, _P, _P],
     "jb_leaf_eval": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _I, _P, _P],
     "jb_leaf_eval_noalloc": [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _I, _I, _P, _P],

@@ -25,7 +25,7 @@ class FMMAccelerations(torch.autograd.Function):
     def forward(ctx, positions: torch.Tensor, masses: torch.Tensor, pass_: Pass, keep_bytes: int = DEFAULT_KEEP_BYTES):
         n = pass_.dt.topo.num_particles
         pass_.load_particles(positions.detach(), masses.detach())
-        pass_.run()
+        pass_.run(cascade=True)  # the backward reads every node's complete local
         acc = torch.empty((n, 3), device=pass_.dt.device, dtype=torch.float32)
         pass_.unsort(acc, None)
         ws = pass_.ws

@@ -663,6 +663,12 @@ JB_API int jb_m2l_mixed(int p_max, int num_units, const int* units, const int* b
                                split, ST(stream));
 }
 
+JB_API int jb_l2l_leaves(int p, int num_units, const int* units, const int* anc, const float* centers,
+                         float* locals, void* stream) {
+  if (num_units < 0 || (num_units > 0 && (!units || !anc || !centers || !locals))) return JB_ERR_ARG;
+  return dispatch<RunL2LLeaves>(p, num_units, units, anc, centers, locals, ST(stream));
+}
+
 JB_API int jb_l2l_level(int p, int first, int last, const int* left, const int* right, const float* centers,
                         float* locals, void* stream) {
   if (first < 0 || last < first || (last > first && (!left || !right || !centers || !locals))) return JB_ERR_ARG;

@@ -402,6 +402,80 @@ __global__ void __launch_bounds__(kM2LThreads, 4) k_m2l_units_coop(int num_units
   for (int k = C; k < rs; ++k) dst[k] = 0.f;
 }
 
+// L2L straight to the leaves (jb_l2l_leaves): a leaf's local is its own M2L
+// sum plus, for each ancestor a that received far pairs, L2L(a -> leaf) of a's
+// own M2L sum.  Shifting the centre of a degree-P local expansion is exact,
+// so this equals the level-by-level cascade up to rounding, and only the
+// leaves' locals -- all that L2P reads -- are formed; the internal nodes keep
+// their own M2L sums.  units[u] = (leaf node, first, end, unused) over anc[]
+// (the leaf's ancestors with far pairs, nearest first); thread per leaf, the
+// warp's ancestor rows fetched together as in k_m2l_units_coop.  One launch
+// with every leaf's chain in parallel, where the cascade runs one dependent
+// launch per level.
+template <int P>
+__global__ void __launch_bounds__(kM2LThreads, 4) k_l2l_leaves(int num_units, const int4* __restrict__ units,
+                                                               const int* __restrict__ anc,
+                                                               const float4* __restrict__ centers,
+                                                               float* __restrict__ locals) {
+  constexpr int C = csize(P), CS = cstride(P), R4 = row4(P), NW = CS / 4;
+  extern __shared__ float4 m2l_smem[];
+  const int lane = threadIdx.x & 31;
+  float4* wrows = m2l_smem + (threadIdx.x & ~31) * R4;
+  float4* row = wrows + lane * R4;
+  int* ids = reinterpret_cast<int*>(m2l_smem + kM2LThreads * R4) + (threadIdx.x & ~31);
+  const int u = blockIdx.x * kM2LThreads + threadIdx.x;
+  const bool ok = u < num_units;
+  const int4 U = ok ? units[u] : make_int4(0, 0, 0, -1);
+  const int leaf = U.x, e0 = U.y;
+  const int n = ok ? U.z - U.y : 0;
+  const int nmax = __reduce_max_sync(0xffffffffu, n);
+  float acc[C];
+#pragma unroll
+  for (int k = 0; k < C; ++k) acc[k] = 0.f;
+  const float4 cl = ok ? centers[leaf] : make_float4(0.f, 0.f, 0.f, 0.f);
+  int s0 = -1, s1 = -1;
+  float4 ca = cl, ca1 = cl;
+  if (n > 0) {
+    s0 = anc[e0];
+    s1 = (n > 1) ? anc[e0 + 1] : s0;
+    ca = centers[s0];
+    ca1 = centers[s1];
+  }
+  warp_rows_fetch<NW, R4>(wrows, ids, lane, s0, locals, CS);
+  for (int it = 0; it < nmax; ++it) {
+    const bool act = it < n;
+    float v[C];
+    cp_async_wait_all();
+    __syncwarp();  // the copies every lane issued into the warp's rows have landed
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < CS / 4; ++k) {
+        const float4 q = row[k];
+        if (4 * k + 0 < C) v[4 * k + 0] = q.x;
+        if (4 * k + 1 < C) v[4 * k + 1] = q.y;
+        if (4 * k + 2 < C) v[4 * k + 2] = q.z;
+        if (4 * k + 3 < C) v[4 * k + 3] = q.w;
+      }
+    }
+    __syncwarp();  // every row (and every id) read before the next copies
+    warp_rows_fetch<NW, R4>(wrows, ids, lane, act && it + 1 < n ? s1 : -1, locals, CS);
+    if (act) {
+      const int s2 = (it + 2 < n) ? __ldg(anc + e0 + it + 2) : s1;
+      l2l_pair<P>(v, ca.x - cl.x, ca.y - cl.y, ca.z - cl.z);
+#pragma unroll
+      for (int k = 0; k < C; ++k) acc[k] += v[k];
+      ca = ca1;
+      ca1 = centers[s2];
+      s1 = s2;
+    }
+  }
+  cp_async_wait_all();
+  if (!ok || n == 0) return;
+  float* dst = locals + (size_t)leaf * CS;
+#pragma unroll
+  for (int k = 0; k < C; ++k) dst[k] += acc[k];
+}
+
 // Sums the partial rows of targets whose list was split: split[i] =
 // (target, first slot, number of slots, unused).  Thread per (target, coefficient).
 static __global__ void __launch_bounds__(256) k_m2l_reduce(int num_split, const int4* __restrict__ split,
@@ -1574,6 +1648,19 @@ struct RunL2L {
 };
 
 template <int P>
+struct RunL2LLeaves {
+  static int run(int num_units, const int* units, const int* anc, const float* centers, float* locals,
+                 cudaStream_t st) {
+    if (num_units <= 0) return JB_OK;
+    const size_t sm = sizeof(float4) * kM2LThreads * row4(P) + sizeof(int) * kM2LThreads;
+    cudaFuncSetAttribute(k_l2l_leaves<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_l2l_leaves<P><<<blocks_for(num_units, kM2LThreads), kM2LThreads, sm, st>>>(
+        num_units, reinterpret_cast<const int4*>(units), anc, reinterpret_cast<const float4*>(centers), locals);
+    return launch_status();
+  }
+};
+
+template <int P>
 struct RunLeafEval {
   template <bool K, bool PT>
   static void go(unsigned nb, cudaStream_t st, const float4* pos4, int num_internal, int num_units, const int4* units,
@@ -1658,6 +1745,7 @@ struct RunTargets {
   extern template struct jb::RunM2L<PP>;      \
   extern template struct jb::RunM2LMixed<PP>; \
   extern template struct jb::RunL2L<PP>;      \
+  extern template struct jb::RunL2LLeaves<PP>; \
   extern template struct jb::RunLeafEval<PP>; \
   extern template struct jb::RunTargets<PP>;  \
   JB_DECLARE_ADJ_##PP

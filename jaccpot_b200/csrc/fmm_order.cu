@@ -10,6 +10,7 @@ template struct jb::RunM2M<JB_ORDER>;
 template struct jb::RunM2L<JB_ORDER>;
 template struct jb::RunM2LMixed<JB_ORDER>;
 template struct jb::RunL2L<JB_ORDER>;
+template struct jb::RunL2LLeaves<JB_ORDER>;
 template struct jb::RunLeafEval<JB_ORDER>;
 template struct jb::RunTargets<JB_ORDER>;
 #if JB_ORDER <= 9

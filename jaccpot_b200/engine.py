@@ -138,6 +138,40 @@ def _on_gpu(dt) -> bool:
     return torch.device(dt.device).type == "cuda"
 
 
+def l2l_leaf_schedule(topo: Topology, leaf_range: tuple[int, int]):
+    """Work units of jb_l2l_leaves for the leaves [lo, hi): (units int32[U,4]
+    = (leaf node, first, end, -1), anc int32[...]) where anc[first:end] are the
+    leaf's ancestors that received far pairs, nearest first; leaves without
+    any are left out; units ordered by their length, longest first (a warp's
+    lanes step through their lists together)."""
+    ni = topo.num_internal
+    lo, hi = leaf_range
+    leaves = np.arange(ni + lo, ni + hi, dtype=np.int64)
+    has_far = np.diff(np.asarray(topo.far_offsets)) > 0
+    parent = np.asarray(topo.parent).astype(np.int64)
+    rows, cols = [], []
+    idx = np.arange(leaves.size, dtype=np.int64)
+    cur = parent[leaves] if leaves.size else leaves
+    while cur.size:
+        ok = cur >= 0
+        idx, cur = idx[ok], cur[ok]
+        m = has_far[cur]
+        rows.append(idx[m])
+        cols.append(cur[m])
+        cur = parent[cur]
+    rows = np.concatenate(rows) if rows else np.zeros(0, np.int64)
+    cols = np.concatenate(cols) if cols else np.zeros(0, np.int64)
+    order = np.argsort(rows, kind="stable")  # nearest ancestor first within a leaf
+    rows, cols = rows[order], cols[order]
+    cnt = np.bincount(rows, minlength=leaves.size)
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    have = np.nonzero(cnt)[0]
+    have = have[np.argsort(-cnt[have], kind="stable")]
+    units = np.stack([leaves[have], off[have], off[have + 1], np.full(have.size, -1)], axis=1).astype(np.int32)
+    anc = cols.astype(np.int32) if cols.size else np.zeros(1, np.int32)
+    return np.ascontiguousarray(units.reshape(-1, 4)), np.ascontiguousarray(anc)
+
+
 def _restrict_gears(gs, targets, num_nodes: int, dev):
     """The gear schedule's units and split entries of the given target nodes
     only (a leaf range's M2L), the per-gear unit ranges recounted.  Units keep
@@ -248,6 +282,13 @@ class Pass:
         self.d_leaf_runs = up(self.leaf_sched.runs)
         self.d_leaf_split = up(self.leaf_sched.split)
         self.leaf_partials = torch.empty((max(self.leaf_sched.num_slots, 1) * _lib.JB_MAX_LEAF_OCCUPANCY, 4), device=dev, dtype=torch.float32)
+        # the downward sweep straight to this pass's leaves (jb_l2l_leaves);
+        # l2l(cascade=True) runs the level-by-level sweep instead
+        self.l2l_direct = True
+        units, anc = l2l_leaf_schedule(t, self.leaf_range)
+        self.num_l2l_units = int(units.shape[0])
+        self.d_l2l_units = up(units)
+        self.d_l2l_anc = up(anc)
 
     def fork(self) -> "Pass":
         """A pass over the same topology and work-unit schedules (shared,
@@ -443,8 +484,17 @@ class Pass:
             raise _lib.JBError("tensor-core M2L: an MMA barrier wait and its drain timed out; the CUDA context "
                                "must not be used further")
 
-    def l2l(self, stream=None) -> None:
+    def l2l(self, stream=None, cascade: bool = False) -> None:
+        """Downward sweep after the M2L.  By default straight to the leaves:
+        each leaf adds L2L(a -> leaf) of every ancestor a with far pairs
+        (jb_l2l_leaves, one launch; the internal nodes keep their own M2L
+        sums).  cascade=True: level by level (jb_l2l_level), every node's
+        local complete -- what the adjoint reads."""
         t, dt, ws, s = self.dt.topo, self.dt, self.ws, _stream_handle(stream)
+        if self.l2l_direct and not cascade:
+            _lib.check(self.lib.jb_l2l_leaves(self.p, self.num_l2l_units, _ptr(self.d_l2l_units), _ptr(self.d_l2l_anc),
+                                              _ptr(ws.centers), _ptr(ws.locals), s), "jb_l2l_leaves")
+            return
         lo = dt.level_offsets
         for lev in range(dt.l2l_first_level, t.num_levels):
             _lib.check(self.lib.jb_l2l_level(self.p, lo[lev], lo[lev + 1], _ptr(dt.left), _ptr(dt.right),
@@ -483,14 +533,15 @@ class Pass:
         _lib.check(self.lib.jb_gather_unsorted(n, _ptr(self.ws.acc4), _ptr(self.dt.inv_perm), _ptr(acc),
                                                _ptr(pot), _stream_handle(stream)), "jb_gather_unsorted")
 
-    def downward(self, stream=None) -> None:
+    def downward(self, stream=None, cascade: bool = False) -> None:
         self.m2l(stream)
-        self.l2l(stream)
+        self.l2l(stream, cascade=cascade)
 
-    def run(self, stream=None) -> torch.Tensor:
-        """Whole pass on the particles already in ws.pos4; returns sorted acc4."""
+    def run(self, stream=None, cascade: bool = False) -> torch.Tensor:
+        """Whole pass on the particles already in ws.pos4; returns sorted acc4
+        (cascade: the level-by-level downward sweep, see l2l)."""
         self.upward(stream)
-        self.downward(stream)
+        self.downward(stream, cascade=cascade)
         return self.evaluate(stream)
 
     def capture(self, positions: torch.Tensor, masses: torch.Tensor, acc: torch.Tensor,
@@ -569,9 +620,9 @@ class Pass:
         t, dt, ws, lb, s = self.dt.topo, self.dt, self.ws, self.lib, _stream_handle(stream)
         A = self._adj_buffers()
         sc = self._adj_sched
-        if recompute:
+        if recompute:  # the reverse sweeps read every node's complete local
             self.upward(stream)
-            self.downward(stream)
+            self.downward(stream, cascade=True)
         w = w.to(device=dt.device, dtype=torch.float32).contiguous()
         _lib.check(lb.jb_gather_sorted(t.num_particles, _ptr(w), _ptr(A["zeros"]), _ptr(dt.perm), _ptr(A["w4"]), s),
                    "jb_gather_sorted(w)")

@@ -36,7 +36,7 @@ def test_split_and_thread_level_kernels_agree(p):
             ps.load_particles(d_pos, d_mass)
             ps.upward()
             ps.m2l()
-            ps.l2l()
+            ps.l2l(cascade=True)  # the level kernels
             torch.cuda.synchronize()
             out[name] = (ps.ws.centers.clone(), ps.ws.mult.clone(), ps.ws.locals.clone())
     finally:

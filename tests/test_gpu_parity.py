@@ -130,12 +130,36 @@ def test_l2l_parity(case):
     torch.cuda.synchronize()
     cen = s.ps.ws.centers.double().cpu().numpy()[:, :3]
     loc0 = s.coeffs(s.ps.ws.locals)
-    s.ps.l2l()
+    s.ps.l2l(cascade=True)
     torch.cuda.synchronize()
     ref = s.orc.l2l_cascade(s.p, cen, loc0)
     got = s.coeffs(s.ps.ws.locals)
     nz = np.abs(ref).max(axis=1) > 0
     err = row_rel(got[nz], ref[nz])
+    assert np.percentile(err, 99) <= COEF_RTOL, np.percentile(err, [50, 99, 100])
+    assert err.max() <= 50 * COEF_RTOL
+
+
+@pytest.mark.parametrize("case", CASES, ids=_ids)
+def test_l2l_straight_to_the_leaves_parity(case):
+    """jb_l2l_leaves (the pass's default downward sweep): every leaf's local
+    against the oracle's level-by-level cascade; the internal nodes keep their
+    own M2L sums."""
+    s = setup(case)
+    s.ps.upward()
+    s.ps.m2l()
+    torch.cuda.synchronize()
+    cen = s.ps.ws.centers.double().cpu().numpy()[:, :3]
+    loc0 = s.coeffs(s.ps.ws.locals)
+    s.ps.l2l()
+    torch.cuda.synchronize()
+    ref = s.orc.l2l_cascade(s.p, cen, loc0)
+    got = s.coeffs(s.ps.ws.locals)
+    ni = s.ps.dt.topo.num_internal
+    assert np.array_equal(got[:ni], loc0[:ni])
+    gl, rl = got[ni:], ref[ni:]
+    nz = np.abs(rl).max(axis=1) > 0
+    err = row_rel(gl[nz], rl[nz])
     assert np.percentile(err, 99) <= COEF_RTOL, np.percentile(err, [50, 99, 100])
     assert err.max() <= 50 * COEF_RTOL
 

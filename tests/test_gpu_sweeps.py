@@ -31,12 +31,12 @@ def test_skipped_l2l_levels_change_nothing(kind, n, leaf, theta, p):
     assert dt.l2l_first_level == (lev[tgt].min() if tgt.size else topo.num_levels)
     ps = engine.Pass(dt, p, G=1.0, eps2=1e-6)
     ps.load_particles(torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda())
-    a = ps.run().clone()
+    a = ps.run(cascade=True).clone()  # the level-by-level sweep (the one that skips levels)
     la = ps.ws.locals.clone()
     first = dt.l2l_first_level
     dt.l2l_first_level = 0
     try:
-        b = ps.run().clone()
+        b = ps.run(cascade=True).clone()
         lb = ps.ws.locals.clone()
     finally:
         dt.l2l_first_level = first
