@@ -110,6 +110,39 @@ def test_work_unit_schedules_cover_the_lists(topo):
         assert np.array_equal(np.sort(us[:, 3]), np.sort([ls.runs[u[1]:u[2], 1].sum() for u in us]))
 
 
+@pytest.mark.parametrize("leaf_range", [None, (3, 40)])
+def test_leaf_ancestor_schedule(topo, leaf_range):
+    """engine.l2l_leaf_schedule (the units of jb_l2l_leaves): one unit per leaf
+    of the range that has an ancestor with far pairs, listing exactly those
+    ancestors, nearest first; longest lists first.  With the far lists the
+    chains cover every far pair whose target contains the leaf, once."""
+    from jaccpot_b200 import engine
+
+    t, _, _ = topo
+    rng = (0, t.num_leaves) if leaf_range is None else leaf_range
+    units, anc = engine.l2l_leaf_schedule(t, rng)
+    ni = t.num_internal
+    has_far = np.diff(t.far_offsets) > 0
+    lens = units[:, 2] - units[:, 1]
+    assert (lens > 0).all() and (np.diff(lens) <= 0).all() and (units[:, 3] == -1).all()
+    seen = set()
+    for leaf, a, b, _ in units:
+        assert rng[0] <= leaf - ni < rng[1] and leaf not in seen
+        seen.add(int(leaf))
+        chain, c = [], int(t.parent[leaf])
+        while c >= 0:
+            if has_far[c]:
+                chain.append(c)
+            c = int(t.parent[c])
+        assert list(anc[a:b]) == chain
+    for lf in range(rng[0], rng[1]):  # leaves left out have no such ancestor
+        if ni + lf not in seen:
+            c = int(t.parent[ni + lf])
+            while c >= 0:
+                assert not has_far[c]
+                c = int(t.parent[c])
+
+
 def test_single_leaf_tree():
     pos = np.random.default_rng(0).normal(size=(10, 3))
     t = tree.build_topology(pos, np.ones(10), leaf_size=16, theta=0.6)
