@@ -151,7 +151,11 @@ def test_l2l_straight_to_the_leaves_parity(case):
     torch.cuda.synchronize()
     cen = s.ps.ws.centers.double().cpu().numpy()[:, :3]
     loc0 = s.coeffs(s.ps.ws.locals)
-    s.ps.l2l()
+    s.ps.l2l_direct = True  # the kernel, whatever the order's default
+    try:
+        s.ps.l2l()
+    finally:
+        s.ps.l2l_direct = s.p <= 8
     torch.cuda.synchronize()
     ref = s.orc.l2l_cascade(s.p, cen, loc0)
     got = s.coeffs(s.ps.ws.locals)
