@@ -172,6 +172,39 @@ def l2l_leaf_schedule(topo: Topology, leaf_range: tuple[int, int]):
     return np.ascontiguousarray(units.reshape(-1, 4)), np.ascontiguousarray(anc)
 
 
+def l2l_leaf_schedule_device(dt: "DeviceTopology", leaf_range: tuple[int, int]):
+    """l2l_leaf_schedule on the device (torch operations over the resident
+    far offsets and the uploaded parents): the same arrays, as device
+    tensors."""
+    t, dev = dt.topo, dt.device
+    ni = t.num_internal
+    lo, hi = leaf_range
+    parent = torch.from_numpy(np.asarray(t.parent).astype(np.int64)).to(dev)
+    has_far = (dt.far_off[1:] - dt.far_off[:-1]) > 0
+    leaves = torch.arange(ni + lo, ni + hi, device=dev, dtype=torch.int64)
+    idx = torch.arange(leaves.numel(), device=dev, dtype=torch.int64)
+    cur = parent[leaves]
+    rows, cols = [], []
+    while cur.numel():
+        ok = cur >= 0
+        idx, cur = idx[ok], cur[ok]
+        m = has_far[cur]
+        rows.append(idx[m])
+        cols.append(cur[m])
+        cur = parent[cur]
+    z = torch.zeros(0, dtype=torch.int64, device=dev)
+    rows = torch.cat(rows) if rows else z
+    cols = torch.cat(cols) if cols else z
+    order = torch.sort(rows, stable=True).indices  # nearest ancestor first within a leaf
+    rows, cols = rows[order], cols[order]
+    cnt = torch.bincount(rows, minlength=leaves.numel())
+    off = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), torch.cumsum(cnt, 0)])
+    have = torch.nonzero(cnt).flatten()
+    have = have[torch.sort(-cnt[have], stable=True).indices]
+    units = torch.stack([leaves[have], off[have], off[have + 1], torch.full_like(have, -1)], dim=1)
+    return units.to(torch.int32).contiguous(), cols.to(torch.int32).contiguous()
+
+
 def _restrict_gears(gs, targets, num_nodes: int, dev):
     """The gear schedule's units and split entries of the given target nodes
     only (a leaf range's M2L), the per-gear unit ranges recounted.  Units keep
@@ -286,7 +319,10 @@ class Pass:
         # orders <= 8; l2l(cascade=True), and orders 9-10 (where the direct
         # chain measured slower: 1.07 against 0.88 ms at 4M), run it level by level
         self.l2l_direct = self.p <= 8
-        units, anc = l2l_leaf_schedule(t, self.leaf_range)
+        if _on_gpu(dt):
+            units, anc = l2l_leaf_schedule_device(dt, self.leaf_range)
+        else:
+            units, anc = l2l_leaf_schedule(t, self.leaf_range)
         self.num_l2l_units = int(units.shape[0])
         self.d_l2l_units = up(units)
         self.d_l2l_anc = up(anc)

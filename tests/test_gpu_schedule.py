@@ -36,6 +36,20 @@ def same(dev, host, what):
     assert np.array_equal(d, h), what
 
 
+@pytest.mark.parametrize("part", [None, (0.25, 0.6)])
+def test_leaf_ancestor_schedule(topo, part):
+    """The direct L2L's (leaf -> ancestors with far pairs) units: the device
+    builder equals the host one entry for entry, whole and on a leaf range."""
+    dt = topo[0]
+    L = dt.topo.num_leaves
+    rng = (0, L) if part is None else (int(part[0] * L), int(part[1] * L))
+    hu, ha = engine.l2l_leaf_schedule(dt.topo, rng)
+    du, da = engine.l2l_leaf_schedule_device(dt, rng)
+    same(du.reshape(-1, 4), hu, "units")
+    if hu.shape[0]:
+        same(da, ha, "ancestors")
+
+
 @pytest.mark.parametrize("max_pairs", [64, 16, 1])
 def test_m2l_schedule(topo, max_pairs):
     dt = topo[0]
