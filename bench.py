@@ -1013,6 +1013,9 @@ def main() -> None:
                      "split_bf16 = plain's lists with the tcgen05 split-BF16 M2L + Kahan P2P; learned_gears = "
                      "plain's lists with the MLP-selected gears + Kahan P2P"),
             "selection": sel,
+            "streams": ("the graphed steps (the headline) run the near field on the caller's stream while the "
+                        "upward sweep, M2L and L2L run on a high-priority stream, joined before the L2P "
+                        "(Pass.overlap; the same bits as one stream)"),
             "chosen_vs_plain": ms_plain / ms_chosen,
             "eager": {"chosen_ms_per_step": ms["chosen"], "plain_ms_per_step": ms["plain"],
                       "chosen_vs_plain": ms["plain"] / ms["chosen"],

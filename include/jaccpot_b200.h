@@ -58,7 +58,14 @@ enum {
   JB_P2P_KAHAN = 1,     /* compensated per-target sums */
   JB_P2P_POTENTIAL = 2, /* also accumulate the potential (else out.w holds only the far part) */
   JB_P2P_FAR_ONLY = 4,  /* jb_leaf_eval: the far field (L2P) alone, no P2P */
-  JB_P2P_NEAR_ONLY = 8  /* jb_leaf_eval: the near field (P2P) alone, no L2P */
+  JB_P2P_NEAR_ONLY = 8, /* jb_leaf_eval: the near field (P2P) alone, no L2P */
+  /* jb_leaf_eval in two halves, so the near field can run on one stream while
+   * the upward sweep, M2L and L2L run on another: NEAR_FIRST writes the near
+   * field (split leaves' partials left unsummed), FAR_AFTER then adds the L2P
+   * and sums the partials.  The two calls together give the bits of one call
+   * without either flag. */
+  JB_P2P_NEAR_FIRST = 16,
+  JB_P2P_FAR_AFTER = 32
 };
 
 /* Most particles one leaf may hold in the leaf kernels (jb_leaf_eval*,
@@ -254,6 +261,16 @@ JB_API int jb_set_leaf_form(int chunk_major);
  * the compiler may fuse a multiply and an add differently in the two
  * kernels, so results agree to FP32 rounding.  Process-wide setting.       */
 JB_API int jb_set_m2l_fetch(int warp_rows);
+
+/* CUDA-graph plumbing for a captured pass (graph: a cudaGraph_t taken from a
+ * stream capture).  node_priority = 1 instantiates it so that each kernel
+ * node keeps the priority of the stream it was captured on, which lets a
+ * pass whose far-field chain was captured on a high-priority stream and whose
+ * near field on a low-priority one overlap the two as the eager launches do;
+ * 0 runs every node at the priority of the stream it is launched into. */
+JB_API int jb_graph_instantiate(void* graph, int node_priority, void** exec);
+JB_API int jb_graph_launch(void* exec, void* stream);
+JB_API int jb_graph_exec_destroy(void* exec);
 
 /* Row stride (floats) of a coefficient array of order p: (p+1)^2 rounded up
  * to a multiple of 4.  Returns 0 for an unsupported order. */

@@ -27,6 +27,7 @@ ERRORS = {
 JB_MAX_ORDER = 10
 JB_M2L_FP32, JB_M2L_SPLIT_BF16 = 0, 1
 JB_P2P_FP32, JB_P2P_KAHAN, JB_P2P_POTENTIAL, JB_P2P_FAR_ONLY, JB_P2P_NEAR_ONLY = 0, 1, 2, 4, 8
+JB_P2P_NEAR_FIRST, JB_P2P_FAR_AFTER = 16, 32
 JB_LEAF_EVAL_NOALLOC_MAX_SLOTS = 16384
 JB_MAX_LEAF_OCCUPANCY = 64
 JB_MIXED_GEAR_SEGMENTS = 4
@@ -96,6 +97,9 @@ _SIGNATURES = {
     "jb_set_level_split": [_I, _I],
     "jb_set_leaf_form": [_I],
     "jb_set_m2l_fetch": [_I],
+    "jb_graph_instantiate": [_P, _I, ctypes.POINTER(_P)],
+    "jb_graph_launch": [_P, _P],
+    "jb_graph_exec_destroy": [_P],
     "jb_far_reverse_index": [_I, _P, _P, _P, _P],
     "jb_m2l_weighted": [_I, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
     "jb_leaf_eval_weighted": [_I, _I, _P, _P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _F, _F, _P, _P, _I, _P, _P],

@@ -447,6 +447,27 @@ JB_API int jb_set_m2l_fetch(int warp_rows) {
 
 JB_API int jb_coeff_stride(int p) { return (p >= 1 && p <= JB_MAX_ORDER) ? cstride(p) : 0; }
 
+JB_API int jb_graph_instantiate(void* graph, int node_priority, void** exec) {
+  if (!graph || !exec || (node_priority != 0 && node_priority != 1)) return JB_ERR_ARG;
+  cudaGraphExec_t e = nullptr;
+  const cudaError_t rc = cudaGraphInstantiateWithFlags(
+      &e, static_cast<cudaGraph_t>(graph), node_priority ? cudaGraphInstantiateFlagUseNodePriority : 0);
+  if (rc != cudaSuccess) return cuda_status(rc);
+  *exec = e;
+  return JB_OK;
+}
+
+JB_API int jb_graph_launch(void* exec, void* stream) {
+  if (!exec) return JB_ERR_ARG;
+  const cudaError_t rc = cudaGraphLaunch(static_cast<cudaGraphExec_t>(exec), ST(stream));
+  return cuda_status(rc);
+}
+
+JB_API int jb_graph_exec_destroy(void* exec) {
+  if (!exec) return JB_ERR_ARG;
+  return cuda_status(cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(exec)));
+}
+
 JB_API const char* jb_last_cuda_error(void) { return g_err; }
 
 JB_API int jb_gather_sorted(int64_t n, const float* pos, const float* mass, const int64_t* perm, float* out_pos4,
@@ -703,8 +724,9 @@ JB_API int jb_leaf_eval(int p, int p2p_mode, const float* pos4, int num_internal
       (num_units > 0 && (!pos4 || !units || !aux || !runs || !node_ranges || !centers || !locals || !out_acc4)) ||
       (num_split > 0 && (!split || !partials || !out_acc4 || !node_ranges)))
     return JB_ERR_ARG;
-  if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL | JB_P2P_FAR_ONLY | JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
-  if ((p2p_mode & JB_P2P_FAR_ONLY) && (p2p_mode & JB_P2P_NEAR_ONLY)) return JB_ERR_ARG;
+  constexpr int parts = JB_P2P_FAR_ONLY | JB_P2P_NEAR_ONLY | JB_P2P_NEAR_FIRST | JB_P2P_FAR_AFTER;
+  if (p2p_mode & ~(JB_P2P_KAHAN | JB_P2P_POTENTIAL | parts)) return JB_ERR_ARG;
+  if (__builtin_popcount(p2p_mode & parts) > 1) return JB_ERR_ARG;  // at most one of the four
   int* err = nullptr;
   const int rc = leaf_error_word(&err);
   if (rc != JB_OK) return rc;

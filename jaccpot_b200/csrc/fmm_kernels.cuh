@@ -871,6 +871,18 @@ struct SmemF {
   __device__ __forceinline__ float operator()(int k) const { return f[k]; }
 };
 
+// A leaf's near and far parts are each rounded to FP32 on their own, then
+// added with one rounded add.  Written out so the compiler fuses neither the
+// scaling nor the add into an FMA: the sum then has the same bits whichever
+// part is written first (the near field before the far field when the two
+// run on separate streams, JB_P2P_NEAR_FIRST / JB_P2P_FAR_AFTER).
+__device__ __forceinline__ float4 near_scaled(float G, const float* v) {
+  return make_float4(__fmul_rn(-G, v[0]), __fmul_rn(-G, v[1]), __fmul_rn(-G, v[2]), __fmul_rn(-G, v[3]));
+}
+__device__ __forceinline__ float4 add_rn(float4 a, float4 b) {
+  return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
+}
+
 template <bool KAHAN>
 struct NearAcc {
   float s[4] = {0.f, 0.f, 0.f, 0.f};
@@ -1084,11 +1096,11 @@ __device__ __forceinline__ void leaf_unit(const float4* __restrict__ pos4, int2 
     if (G >= 2) v[i] += __shfl_xor_sync(0xffffffffu, v[i], 1);
     if (G >= 4) v[i] += __shfl_xor_sync(0xffffffffu, v[i], 2);
   }
-  const float4 res = make_float4(-G_ * v[0], -G_ * v[1], -G_ * v[2], -G_ * v[3]);
+  const float4 res = near_scaled(G_, v);
   if (active && h == 0) {
     if (aux.x < 0) {
       const float4 f = out[rg.x + tl];  // the far field k_leaf_l2p wrote
-      out[rg.x + tl] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
+      out[rg.x + tl] = add_rn(f, res);
     } else if (aux.x < max_slots) {
       partial[(size_t)aux.x * kMaxLeaf + row + tl] = res;
     } else {
@@ -1373,10 +1385,10 @@ __device__ __forceinline__ void leaf_unit_flat(const float4* __restrict__ pos4, 
     float v[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) v[i] = (POT || i < 3) ? a.value(i) : 0.f;
-    const float4 res = make_float4(-G_ * v[0], -G_ * v[1], -G_ * v[2], -G_ * v[3]);
+    const float4 res = near_scaled(G_, v);
     if (aux.x < 0) {
       const float4 f = out[rg.x + lane];  // the far field k_leaf_l2p wrote
-      out[rg.x + lane] = make_float4(f.x + res.x, f.y + res.y, f.z + res.z, f.w + res.w);
+      out[rg.x + lane] = add_rn(f, res);
     } else if (aux.x < max_slots) {
       partial[(size_t)aux.x * kMaxLeaf + row + lane] = res;
     } else {
@@ -1426,12 +1438,16 @@ static __global__ void __launch_bounds__(32 * kWarpsPerBlock, POT ? 6 : 8) k_lea
 // out = -G (grad phi, phi); runs before k_leaf_units, which adds the near
 // field.  Kept out of the near-field kernel so that kernel's register count
 // is set by the P2P loop alone (about half, and twice the resident warps).
-// zero: write zeros instead (the near field alone, JB_P2P_NEAR_ONLY).
+// mode kL2PZero: write zeros instead (the near field alone, JB_P2P_NEAR_ONLY
+// and JB_P2P_NEAR_FIRST); kL2PAdd: add the far field to what out holds (the
+// near field a JB_P2P_NEAR_FIRST launch wrote), with the rounding of the
+// near-field kernel's own add.
+enum { kL2PWrite = 0, kL2PZero = 1, kL2PAdd = 2 };
 template <int P>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
     const float4* __restrict__ pos4, int num_internal, int num_units, const int4* __restrict__ units,
     const int2* __restrict__ aux, const int2* __restrict__ ranges, const float4* __restrict__ centers,
-    const float* __restrict__ locals, float G, float4* __restrict__ out, bool zero) {
+    const float* __restrict__ locals, float G, float4* __restrict__ out, int mode) {
   constexpr int C = csize(P), CS = cstride(P);
   __shared__ float sF[kWarpsPerBlock][CS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1440,7 +1456,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
   const int node = num_internal + units[u].x;
   const int2 rg = ranges[node];
   if (rg.y - rg.x + 1 > kMaxLeaf) return;  // refused by the near-field kernel, which flags it
-  if (zero) {  // near field alone: the sums start from zero
+  if (mode == kL2PZero) {  // near field alone: the sums start from zero
     for (int i = rg.x + lane; i <= rg.y; i += 32) out[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     return;
   }
@@ -1455,7 +1471,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_leaf_l2p(
     solid_harmonics<P>(c.x - ti.x, c.y - ti.y, c.z - ti.z, U_);
     float phi, g[3];
     l2p_eval<P>(SmemF{sF[warp]}, U_, &phi, g);
-    out[i] = make_float4(-G * g[0], -G * g[1], -G * g[2], -G * phi);
+    const float4 f = make_float4(__fmul_rn(-G, g[0]), __fmul_rn(-G, g[1]), __fmul_rn(-G, g[2]), __fmul_rn(-G, phi));
+    out[i] = mode == kL2PAdd ? add_rn(f, out[i]) : f;
   }
 }
 
@@ -1697,22 +1714,25 @@ struct RunLeafEval {
       auto a4 = reinterpret_cast<const int2*>(ranges);
       auto o = reinterpret_cast<float4*>(out);
       auto pt = reinterpret_cast<float4*>(partial);
-      const bool far_only = (mode & JB_P2P_FAR_ONLY) != 0, near_only = (mode & JB_P2P_NEAR_ONLY) != 0;
+      const bool far_only = (mode & JB_P2P_FAR_ONLY) != 0, far_after = (mode & JB_P2P_FAR_AFTER) != 0;
+      const bool zero = (mode & (JB_P2P_NEAR_ONLY | JB_P2P_NEAR_FIRST)) != 0;
       k_leaf_l2p<P><<<nb, 32 * kWarpsPerBlock, 0, st>>>(a0, num_internal, num_units, a1, a2, a4,
                                                         reinterpret_cast<const float4*>(centers), locals, G, o,
-                                                        near_only);
+                                                        zero ? kL2PZero : far_after ? kL2PAdd : kL2PWrite);
       int rc = launch_status();
       if (rc) return rc;
       if (far_only) return JB_OK;
-      const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
-      if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
-      else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
-      else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
-      else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
-      rc = launch_status();
-      if (rc) return rc;
+      if (!far_after) {  // FAR_AFTER: the near field is already in out (and partials)
+        const bool kahan = (mode & JB_P2P_KAHAN) != 0, pot = (mode & JB_P2P_POTENTIAL) != 0;
+        if (kahan && pot) go<true, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
+        else if (kahan) go<true, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
+        else if (pot) go<false, true>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
+        else go<false, false>(nb, st, a0, num_internal, num_units, a1, a2, a3, a4, G, eps2, o, pt, rung, lw, nlw, flat, max_slots, err);
+        rc = launch_status();
+        if (rc) return rc;
+      }
     }
-    if (num_split > 0) {
+    if (num_split > 0 && !(mode & JB_P2P_NEAR_FIRST)) {  // NEAR_FIRST: summed by the FAR_AFTER call
       k_leaf_reduce<true><<<blocks_for((int64_t)num_split * kMaxLeaf, 256), 256, 0, st>>>(
           num_split, reinterpret_cast<const int4*>(split), num_internal, reinterpret_cast<const int2*>(ranges),
           reinterpret_cast<const float4*>(partial), reinterpret_cast<float4*>(out), max_slots, err);
