@@ -884,6 +884,34 @@ def main() -> None:
             del g
     clocks = cs.summary()
 
+    def overlap_timeline(ps: engine.Pass, steps: int = 3) -> dict:
+        """When each stream's part of the two-stream step ends (events from
+        the step's start; eager, median of `steps`): the near field on the
+        caller's stream, the upward sweep + M2L + L2L on the pass's
+        high-priority stream, and the L2P after the join."""
+        far = ps.far_stream()
+        rows = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ps.load_particles(d_pos, d_mass)
+            ev[0].record(stream)
+            far.wait_stream(stream)
+            ps.evaluate(stream, part="near_first")
+            ev[1].record(stream)
+            ps.upward(far)
+            ps.downward(far)
+            ev[2].record(far)
+            stream.wait_stream(far)
+            ps.evaluate(stream, part="far_after")
+            ev[3].record(stream)
+            torch.cuda.synchronize()
+            rows.append([ev[0].elapsed_time(ev[i]) for i in (1, 2, 3)])
+        med = np.median(np.array(rows), axis=0)
+        return {"near_field_done": float(med[0]), "far_chain_done": float(med[1]), "step_done": float(med[2])}
+
+    timeline = overlap_timeline(passes["chosen"])
+
     def reduce_max(x: float) -> float:
         if world == 1:
             return x
@@ -1016,6 +1044,7 @@ def main() -> None:
             "streams": ("the graphed steps (the headline) run the near field on the caller's stream while the "
                         "upward sweep, M2L and L2L run on a high-priority stream, joined before the L2P "
                         "(Pass.overlap; the same bits as one stream)"),
+            "overlap_timeline_ms_chosen": timeline,
             "chosen_vs_plain": ms_plain / ms_chosen,
             "eager": {"chosen_ms_per_step": ms["chosen"], "plain_ms_per_step": ms["plain"],
                       "chosen_vs_plain": ms["plain"] / ms["chosen"],
