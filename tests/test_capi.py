@@ -47,6 +47,13 @@ def test_argument_errors_without_a_device():
     assert lib.jb_m2l(8, 0, -1, None, None, None, None, None, None, 0, None, None) == 1
     assert lib.jb_m2l(8, 9, 1, 1, 1, 1, 1, 1, 1, 0, None, None) == 8
     assert lib.jb_leaf_eval(8, 64, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1.0, 0.0, 1, 1, 0, None, None) == 1
+    # at most one of the part flags (near / far alone, or one half of the two-stream form)
+    for a, b in ((_lib.JB_P2P_NEAR_FIRST, _lib.JB_P2P_FAR_AFTER), (_lib.JB_P2P_NEAR_ONLY, _lib.JB_P2P_FAR_AFTER),
+                 (_lib.JB_P2P_FAR_ONLY, _lib.JB_P2P_NEAR_FIRST), (_lib.JB_P2P_FAR_ONLY, _lib.JB_P2P_NEAR_ONLY)):
+        assert lib.jb_leaf_eval(8, a | b, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1.0, 0.0, 1, 1, 0, None, None) == 1
+    assert lib.jb_graph_instantiate(None, 1, ctypes.byref(ctypes.c_void_p())) == 1
+    assert lib.jb_graph_instantiate(1, 2, ctypes.byref(ctypes.c_void_p())) == 1
+    assert lib.jb_graph_launch(None, None) == 1 and lib.jb_graph_exec_destroy(None) == 1
     assert lib.jb_m2m_level(8, 5, 4, None, None, None, None, None, None) == 1
     assert lib.jb_gather_sorted(-1, None, None, None, None, None) == 1
     assert lib.jb_direct_f64(0, None, 0, None, 1.0, 0.0, None, None) == 1
